@@ -1,0 +1,209 @@
+"""ctypes binding of libarc.so (include/arc_api.h).
+
+The shared library is the product; this module only declares its C ABI for Python callers
+(tests, benchmark, smoke check).  Loading fails loudly when libarc.so has not been built: there
+is no Python or CPU fallback for any GPU entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libarc.so")
+
+ARC_OK = 0
+ARC_ERR_INVALID_ARG = 1
+ARC_ERR_TOO_FEW_AVPLS = 2
+ARC_ERR_STACK_OVERFLOW = 3
+ARC_ERR_TIMEOUT = 4
+ARC_ERR_CUDA = 5
+ARC_ERR_OUT_OF_MEMORY = 6
+ARC_ERR_DEVICE = 7
+ARC_ERR_UNSUPPORTED = 8
+
+ARC_DEVERR_STACK_OVERFLOW = 0x1
+ARC_DEVERR_TIMEOUT = 0x2
+ARC_DEVERR_BAD_MATERIAL = 0x4
+ARC_DEVERR_BAD_NODE = 0x8
+ARC_DEVERR_CUT_OVERFLOW = 0x10
+
+ARC_MAX_MATERIALS = 64
+ARC_SCENE_MAX_BOXES = 32
+
+ARC_AR_NONE, ARC_AR_DISK, ARC_AR_CONE = 0, 1, 2
+ARC_PREC_KAHAN, ARC_PREC_KAHAN_STRICT, ARC_PREC_NAIVE, ARC_PREC_FP64 = 0, 1, 2, 3
+ARC_BBOX_SCENE, ARC_BBOX_AVPL_REFERENCE = 0, 1
+ARC_CUT_SOLID_ANGLE, ARC_CUT_ERROR_BOUND, ARC_CUT_LEARNED = 0, 1, 2
+ARC_SCENE_ROOM, ARC_SCENE_ROOM_2BOXES, ARC_SCENE_ROOM_RANDOM, ARC_SCENE_TRAIN_VARIANT = 0, 1, 2, 3
+
+
+class ArcFloat3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class ArcAvplHost(C.Structure):
+    _fields_ = [("position", ArcFloat3), ("normal", ArcFloat3), ("incRadiance", ArcFloat3),
+                ("antiradiance", ArcFloat3), ("incDirection", ArcFloat3), ("bounce", C.c_int32),
+                ("materialIndex", C.c_int32)]
+
+
+class ArcAvplsGpuParam(C.Structure):
+    _fields_ = [("position", C.c_void_p), ("normal", C.c_void_p), ("incDirection", C.c_void_p),
+                ("incRadiance", C.c_void_p), ("antiradiance", C.c_void_p), ("materialIndex", C.c_void_p),
+                ("bounce", C.c_void_p), ("numAvpls", C.c_int32)]
+
+
+class ArcMaterial(C.Structure):
+    _fields_ = [("emissive", ArcFloat3), ("diffuse", ArcFloat3), ("specular", ArcFloat3), ("exponent", C.c_float)]
+
+
+class ArcGBufferView(C.Structure):
+    _fields_ = [("position", C.c_void_p), ("normal", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32),
+                ("pitch", C.c_int64)]
+
+
+class ArcOutputView(C.Structure):
+    _fields_ = [("result", C.c_void_p), ("radiance", C.c_void_p), ("antiradiance", C.c_void_p),
+                ("result_fp64", C.c_void_p), ("pitch", C.c_int64)]
+
+
+class ArcGatherParams(C.Structure):
+    _fields_ = [("ar_kind", C.c_int32), ("disk_radius", C.c_float), ("cone_half_angle", C.c_float),
+                ("dist_clamp", C.c_float), ("geo_limit_radiance", C.c_float),
+                ("geo_limit_antiradiance", C.c_float), ("precision", C.c_int32), ("tile_config", C.c_int32)]
+
+
+class ArcLbvhParams(C.Structure):
+    _fields_ = [("consider_normals", C.c_int32), ("bbox_mode", C.c_int32), ("scene_min", ArcFloat3),
+                ("scene_max", ArcFloat3), ("repr_seed", C.c_uint32)]
+
+
+class ArcBvhNode(C.Structure):
+    _fields_ = [("left", C.c_int32), ("right", C.c_int32), ("bbMin", ArcFloat3), ("bbMax", ArcFloat3),
+                ("visited", C.c_int32)]
+
+
+class ArcBvhParam(C.Structure):
+    _fields_ = [("numLeafs", C.c_int32), ("numNodes", C.c_int32), ("nodes", C.c_void_p),
+                ("positions", C.c_void_p), ("normals", C.c_void_p)]
+
+
+class ArcAvplBvhNodeDataParam(C.Structure):
+    _fields_ = [("size", C.c_void_p), ("materialIndex", C.c_void_p), ("randomNumbers", C.c_void_p),
+                ("position", C.c_void_p), ("normal", C.c_void_p), ("incRadiance", C.c_void_p),
+                ("incDirection", C.c_void_p)]
+
+
+class ArcLbvhView(C.Structure):
+    _fields_ = [("num_leaves", C.c_int32), ("num_nodes", C.c_int32), ("morton", C.c_void_p),
+                ("sorted_index", C.c_void_p), ("left", C.c_void_p), ("right", C.c_void_p),
+                ("parents", C.c_void_p), ("range", C.c_void_p), ("bounds", C.c_void_p), ("records", C.c_void_p),
+                ("node_data", ArcAvplBvhNodeDataParam)]
+
+
+class ArcCutParams(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("solid_angle_threshold", C.c_float), ("error_bound", C.c_float),
+                ("ar_uncertain_factor", C.c_float), ("max_cut_nodes", C.c_int32), ("model", C.c_void_p), ("mlp_threshold", C.c_float),
+                ("debug_pixel_x", C.c_int32), ("debug_pixel_y", C.c_int32), ("used_nodes", C.c_void_p)]
+
+
+class ArcRunConfig(C.Structure):
+    _fields_ = [("useLightCuts", C.c_int32), ("cut_kind", C.c_int32), ("clusterRefinementThreshold", C.c_float),
+                ("error_bound", C.c_float), ("photonRadiusScale", C.c_float), ("ar_kind", C.c_int32),
+                ("cone_half_angle", C.c_float), ("dist_clamp", C.c_float), ("precision", C.c_int32),
+                ("considerNormals", C.c_int32), ("model", C.c_void_p), ("profile", C.c_int32)]
+
+
+class ArcBox(C.Structure):
+    _fields_ = [("lo", ArcFloat3), ("hi", ArcFloat3), ("material", C.c_int32)]
+
+
+class ArcSceneDesc(C.Structure):
+    _fields_ = [("num_boxes", C.c_int32), ("boxes", ArcBox * ARC_SCENE_MAX_BOXES), ("num_materials", C.c_int32),
+                ("materials", ArcMaterial * ARC_MAX_MATERIALS), ("light_center", ArcFloat3),
+                ("light_half_size", C.c_float), ("light_radiance", ArcFloat3), ("light_material", C.c_int32),
+                ("camera_position", ArcFloat3), ("camera_target", ArcFloat3), ("camera_fov_deg", C.c_float),
+                ("scene_min", ArcFloat3), ("scene_max", ArcFloat3)]
+
+
+P = C.POINTER
+_vp = C.c_void_p
+_st = C.c_int32
+
+# name -> (restype, argtypes); every entry is a symbol declared in include/arc_api.h
+SIGNATURES = {
+    "arc_api_version": (C.c_int32, []),
+    "arc_status_string": (C.c_char_p, [C.c_int32]),
+    "arc_last_error": (C.c_char_p, []),
+    "arc_gather_params_default": (None, [P(ArcGatherParams)]),
+    "arc_lbvh_params_default": (None, [P(ArcLbvhParams)]),
+    "arc_cut_params_default": (None, [P(ArcCutParams)]),
+    "arc_run_config_default": (None, [P(ArcRunConfig)]),
+    "arc_context_create": (_st, [C.c_int32, _vp, P(_vp)]),
+    "arc_context_destroy": (_st, [_vp]),
+    "arc_context_synchronize": (_st, [_vp, P(C.c_uint32)]),
+    "arc_context_stream": (_vp, [_vp]),
+    "arc_device_alloc": (_st, [_vp, C.c_size_t, P(_vp)]),
+    "arc_device_free": (_st, [_vp, _vp]),
+    "arc_copy_h2d": (_st, [_vp, _vp, _vp, C.c_size_t]),
+    "arc_copy_d2h": (_st, [_vp, _vp, _vp, C.c_size_t]),
+    "arc_materials_upload": (_st, [_vp, P(ArcMaterial), C.c_int32]),
+    "arc_avpls_upload": (_st, [_vp, P(ArcAvplHost), C.c_int32, P(ArcAvplsGpuParam)]),
+    "arc_gather_bruteforce": (_st, [_vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcGatherParams),
+                                    P(ArcOutputView)]),
+    "arc_lbvh_create": (_st, [_vp, P(_vp)]),
+    "arc_lbvh_destroy": (_st, [_vp]),
+    "arc_lbvh_build": (_st, [_vp, P(ArcAvplsGpuParam), P(ArcLbvhParams)]),
+    "arc_lbvh_get_view": (_st, [_vp, P(ArcLbvhView)]),
+    "arc_lbvh_reference_views": (_st, [_vp, P(ArcBvhParam), P(ArcAvplBvhNodeDataParam)]),
+    "arc_gather_cut": (_st, [_vp, _vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcGatherParams),
+                             P(ArcCutParams), P(ArcOutputView)]),
+    "arc_last_cut": (_st, [_vp, P(C.c_int32), P(C.c_int32), P(_vp), P(_vp)]),
+    "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),
+                      P(ArcOutputView)]),
+    "arc_scene_preset_desc": (_st, [C.c_int32, C.c_uint64, C.c_int32, P(ArcSceneDesc)]),
+    "arc_scene_trace_avpls": (_st, [P(ArcSceneDesc), C.c_uint64, C.c_int32, C.c_int32, C.c_int32, P(ArcAvplHost),
+                                    P(C.c_int64)]),
+    "arc_scene_gbuffer": (_st, [P(ArcSceneDesc), C.c_int32, C.c_int32, _vp, _vp]),
+}
+
+_lib = None
+
+
+class ArcError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str = ""):
+        self.status = status
+        super().__init__(f"{where}: status {status} ({status_string(status)}) {msg}")
+
+
+def load() -> C.CDLL:
+    """Load libarc.so (built by antiradiancecuts_b200.build); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m antiradiancecuts_b200.build` "
+                           "(the library has no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def status_string(s: int) -> str:
+    return load().arc_status_string(int(s)).decode()
+
+
+def check(status: int, where: str) -> None:
+    if status != ARC_OK:
+        raise ArcError(status, where, load().arc_last_error().decode())
+
+
+def f3(x, y=None, z=None) -> ArcFloat3:
+    if y is None:
+        x, y, z = x
+    return ArcFloat3(float(x), float(y), float(z))

@@ -1,0 +1,265 @@
+"""Python host interface over libarc's C ABI, named after the reference's classes:
+
+    CudaGather(ctx, gbuffer, materials).run(avpls, camera_position, scene_extent, config)
+        -> CudaGather::run (cudaGather.cu:836-1051)
+    AvplBvh(ctx, avpls, consider_normals)      -> AvplBvh (bvh.cu:746-774)
+    gather_bruteforce / gather_cut             -> the gather kernels
+
+Device buffers are torch CUDA tensors (torch is used for device memory and streams only); every
+computation runs in libarc's sm_100a kernels on the context's stream, which is torch's current
+stream so the two stay ordered.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import weakref
+
+import numpy as np
+
+from . import _lib as L
+from .scene import AVPL_DTYPE
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+class Context:
+    """arc_context on `device`, running on torch's current stream of that device."""
+
+    def __init__(self, device: int = 0):
+        torch = _torch()
+        self.lib = L.load()
+        self.device = device
+        torch.cuda.set_device(device)
+        stream = torch.cuda.current_stream(device).cuda_stream
+        h = C.c_void_p()
+        L.check(self.lib.arc_context_create(device, C.c_void_p(stream), C.byref(h)), "arc_context_create")
+        self.handle = h
+        self._avpl_keep = None
+        self._children = weakref.WeakSet()  # objects whose handles live in this context
+
+    def close(self):
+        if self.handle:
+            for ch in list(self._children):
+                ch.close()
+            self.lib.arc_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self) -> int:
+        w = C.c_uint32(0)
+        L.check(self.lib.arc_context_synchronize(self.handle, C.byref(w)), "arc_context_synchronize")
+        return int(w.value)
+
+    def upload_materials(self, mats) -> None:
+        L.check(self.lib.arc_materials_upload(self.handle, mats, len(mats)), "arc_materials_upload")
+
+    def upload_avpls(self, avpls: np.ndarray) -> L.ArcAvplsGpuParam:
+        """AvplsGpu(avpls): host records -> context-owned device arrays."""
+        avpls = np.ascontiguousarray(avpls, dtype=AVPL_DTYPE)
+        out = L.ArcAvplsGpuParam()
+        L.check(self.lib.arc_avpls_upload(self.handle, avpls.ctypes.data_as(C.POINTER(L.ArcAvplHost)), len(avpls),
+                                          C.byref(out)), "arc_avpls_upload")
+        self._avpl_keep = avpls
+        return out
+
+    def d2h(self, ptr, dtype, count) -> np.ndarray:
+        out = np.empty(count, dtype=dtype)
+        if count:
+            L.check(self.lib.arc_copy_d2h(self.handle, out.ctypes.data, C.c_void_p(ptr), out.nbytes), "arc_copy_d2h")
+        return out
+
+
+class GBuffer:
+    """Device G-buffer planes (float4 position, float4 normal with material in w)."""
+
+    def __init__(self, pos: np.ndarray, nrm: np.ndarray, device: int = 0):
+        torch = _torch()
+        self.height, self.width = pos.shape[:2]
+        self.pos = torch.from_numpy(np.ascontiguousarray(pos)).to(f"cuda:{device}")
+        self.nrm = torch.from_numpy(np.ascontiguousarray(nrm)).to(f"cuda:{device}")
+
+    def view(self) -> L.ArcGBufferView:
+        return L.ArcGBufferView(self.pos.data_ptr(), self.nrm.data_ptr(), self.width, self.height, self.width)
+
+
+class Outputs:
+    """Result / radiance / antiradiance float4 planes and the FP64 result plane."""
+
+    def __init__(self, width: int, height: int, device: int = 0, fp64: bool = True, parts: bool = True):
+        torch = _torch()
+        dev = f"cuda:{device}"
+        self.width, self.height = width, height
+        self.result = torch.zeros((height, width, 4), dtype=torch.float32, device=dev)
+        self.radiance = torch.zeros_like(self.result) if parts else None
+        self.antiradiance = torch.zeros_like(self.result) if parts else None
+        self.result64 = torch.zeros((height, width, 3), dtype=torch.float64, device=dev) if fp64 else None
+
+    def view(self) -> L.ArcOutputView:
+        p = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
+        return L.ArcOutputView(p(self.result), p(self.radiance), p(self.antiradiance), p(self.result64), self.width)
+
+
+def gather_params(ar_kind=L.ARC_AR_CONE, cone_half_angle_deg=30.0, dist_clamp=0.0, disk_radius=0.0,
+                  precision=L.ARC_PREC_KAHAN, tile_config=-1, geo_limit_radiance=0.0,
+                  geo_limit_antiradiance=0.0) -> L.ArcGatherParams:
+    p = L.ArcGatherParams()
+    L.load().arc_gather_params_default(C.byref(p))
+    p.ar_kind = ar_kind
+    p.cone_half_angle = math.radians(cone_half_angle_deg)
+    p.dist_clamp = dist_clamp
+    p.disk_radius = disk_radius
+    p.precision = precision
+    p.tile_config = tile_config
+    p.geo_limit_radiance = geo_limit_radiance
+    p.geo_limit_antiradiance = geo_limit_antiradiance
+    return p
+
+
+def gather_bruteforce(ctx: Context, avpls: L.ArcAvplsGpuParam, gb: GBuffer, cam, params: L.ArcGatherParams,
+                      out: Outputs) -> None:
+    gv, ov = gb.view(), out.view()
+    L.check(ctx.lib.arc_gather_bruteforce(ctx.handle, C.byref(avpls), C.byref(gv), L.f3(cam), C.byref(params),
+                                          C.byref(ov)), "arc_gather_bruteforce")
+
+
+class AvplBvh:
+    """LBVH over uploaded AVPLs (AvplBvh(avpls, considerNormals), bvh.cu:746-774)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = C.c_void_p()
+        L.check(ctx.lib.arc_lbvh_create(ctx.handle, C.byref(h)), "arc_lbvh_create")
+        self.handle = h
+        ctx._children.add(self)
+
+    def build(self, avpls: L.ArcAvplsGpuParam, consider_normals=False, bbox_mode=L.ARC_BBOX_SCENE,
+              scene_min=(0, 0, 0), scene_max=(1, 1, 1), repr_seed=None) -> None:
+        p = L.ArcLbvhParams()
+        self.ctx.lib.arc_lbvh_params_default(C.byref(p))
+        p.consider_normals = int(consider_normals)
+        p.bbox_mode = bbox_mode
+        p.scene_min = L.f3(scene_min)
+        p.scene_max = L.f3(scene_max)
+        if repr_seed is not None:
+            p.repr_seed = repr_seed
+        L.check(self.ctx.lib.arc_lbvh_build(self.handle, C.byref(avpls), C.byref(p)), "arc_lbvh_build")
+
+    def view(self) -> L.ArcLbvhView:
+        v = L.ArcLbvhView()
+        L.check(self.ctx.lib.arc_lbvh_get_view(self.handle, C.byref(v)), "arc_lbvh_get_view")
+        return v
+
+    def host_arrays(self) -> dict:
+        """Copy every tree array to host numpy arrays."""
+        v = self.view()
+        n = v.num_leaves
+        t = 2 * n - 1
+        d = self.ctx.d2h
+        nd = v.node_data
+        return {
+            "morton": d(v.morton, np.uint32, n),
+            "sorted_index": d(v.sorted_index, np.int32, n),
+            "left": d(v.left, np.int32, n - 1),
+            "right": d(v.right, np.int32, n - 1),
+            "parents": d(v.parents, np.int32, t),
+            "range": d(v.range, np.int32, 2 * (n - 1)).reshape(-1, 2),
+            "bounds": d(v.bounds, np.float32, 16 * (n - 1)).reshape(-1, 16),
+            "records": d(v.records, np.float32, 16 * t).reshape(-1, 16),
+            "size": d(nd.size, np.int32, t),
+            "materialIndex": d(nd.materialIndex, np.int32, t),
+            "randomNumbers": d(nd.randomNumbers, np.float32, t),
+            "position": d(nd.position, np.float32, 3 * t).reshape(-1, 3),
+            "normal": d(nd.normal, np.float32, 3 * t).reshape(-1, 3),
+            "incRadiance": d(nd.incRadiance, np.float32, 3 * t).reshape(-1, 3),
+            "incDirection": d(nd.incDirection, np.float32, 3 * t).reshape(-1, 3),
+        }
+
+    def reference_views(self):
+        bp, nd = L.ArcBvhParam(), L.ArcAvplBvhNodeDataParam()
+        L.check(self.ctx.lib.arc_lbvh_reference_views(self.handle, C.byref(bp), C.byref(nd)),
+                "arc_lbvh_reference_views")
+        return bp, nd
+
+    def close(self):
+        if self.handle and self.ctx.handle:
+            self.ctx.lib.arc_lbvh_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cut_params(kind=L.ARC_CUT_ERROR_BOUND, error_bound=0.01, solid_angle_threshold=math.pi / 10,
+               max_cut_nodes=16384, model=None, mlp_threshold=0.5, debug_pixel=(-1, -1), used_nodes=None,
+               ar_uncertain_factor=16.0):
+    p = L.ArcCutParams()
+    L.load().arc_cut_params_default(C.byref(p))
+    p.kind = kind
+    p.error_bound = error_bound
+    p.ar_uncertain_factor = ar_uncertain_factor
+    p.solid_angle_threshold = solid_angle_threshold
+    p.max_cut_nodes = max_cut_nodes
+    p.model = model
+    p.mlp_threshold = mlp_threshold
+    p.debug_pixel_x, p.debug_pixel_y = debug_pixel
+    p.used_nodes = used_nodes
+    return p
+
+
+def gather_cut(ctx: Context, bvh: AvplBvh, avpls: L.ArcAvplsGpuParam | None, gb: GBuffer, cam,
+               params: L.ArcGatherParams, cut: L.ArcCutParams, out: Outputs) -> None:
+    gv, ov = gb.view(), out.view()
+    ap = C.byref(avpls) if avpls is not None else None
+    L.check(ctx.lib.arc_gather_cut(ctx.handle, bvh.handle, ap, C.byref(gv), L.f3(cam), C.byref(params), C.byref(cut),
+                                   C.byref(ov)), "arc_gather_cut")
+
+
+def last_cut(ctx: Context) -> list[np.ndarray]:
+    """Cut node lists of the last tile-cut gather, one sorted array per tile."""
+    nt, stride = C.c_int32(), C.c_int32()
+    cp, np_ = C.c_void_p(), C.c_void_p()
+    L.check(ctx.lib.arc_last_cut(ctx.handle, C.byref(nt), C.byref(stride), C.byref(cp), C.byref(np_)), "arc_last_cut")
+    counts = ctx.d2h(cp.value, np.int32, nt.value)
+    nodes = ctx.d2h(np_.value, np.int32, nt.value * stride.value).reshape(nt.value, stride.value)
+    return [np.sort(nodes[t, :counts[t]]) for t in range(nt.value)]
+
+
+def run_config(**kw) -> L.ArcRunConfig:
+    c = L.ArcRunConfig()
+    L.load().arc_run_config_default(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class CudaGather:
+    """CudaGather (cudaGather.h:25-70) over a device G-buffer and output planes instead of GL
+    textures."""
+
+    def __init__(self, ctx: Context, gbuffer: GBuffer, materials, outputs: Outputs | None = None):
+        self.ctx = ctx
+        self.gbuffer = gbuffer
+        self.outputs = outputs or Outputs(gbuffer.width, gbuffer.height, ctx.device)
+        ctx.upload_materials(materials)
+
+    def run(self, avpls: np.ndarray, camera_position, scene_extent: float, config: L.ArcRunConfig | None = None):
+        config = config or run_config()
+        avpls = np.ascontiguousarray(avpls, dtype=AVPL_DTYPE)
+        gv, ov = self.gbuffer.view(), self.outputs.view()
+        L.check(self.ctx.lib.arc_run(self.ctx.handle, avpls.ctypes.data_as(C.POINTER(L.ArcAvplHost)), len(avpls),
+                                     L.f3(camera_position), float(scene_extent), C.byref(config), C.byref(gv),
+                                     C.byref(ov)), "arc_run")
+        return self.outputs

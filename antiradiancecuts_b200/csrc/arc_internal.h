@@ -1,0 +1,124 @@
+// Internal host-side declarations of libarc: the context, its grow-only device arena, error
+// reporting and the launchers each kernel file provides.
+#ifndef ARC_INTERNAL_H_
+#define ARC_INTERNAL_H_
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "arc_api.h"
+
+namespace arc {
+
+void set_last_error(const std::string& msg);
+
+#define ARC_TRY_CUDA(expr)                                                                    \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess) {                                                              \
+            ::arc::set_last_error(std::string(#expr) + ": " + cudaGetErrorString(_e));         \
+            return _e == cudaErrorMemoryAllocation ? ARC_ERR_OUT_OF_MEMORY : ARC_ERR_CUDA;    \
+        }                                                                                     \
+    } while (0)
+
+#define ARC_CHECK_ARG(cond, msg)                    \
+    do {                                            \
+        if (!(cond)) {                              \
+            ::arc::set_last_error(msg);             \
+            return ARC_ERR_INVALID_ARG;             \
+        }                                           \
+    } while (0)
+
+#define ARC_TRY(expr)                      \
+    do {                                   \
+        arc_status _s = (expr);            \
+        if (_s != ARC_OK) return _s;       \
+    } while (0)
+
+// Per-material data the kernels read: {diffuse.xyz, exponent}, {specular.xyz, has_specular}.
+struct MaterialRecord {
+    float4 diffuse_exp;
+    float4 specular_flag;
+};
+
+// Grow-only named device buffers.  A buffer is reallocated only when a call needs more bytes
+// than it holds, so steady-state frames allocate nothing.
+class Arena {
+  public:
+    ~Arena();
+    arc_status get(const char* name, size_t bytes, void** out);
+    size_t bytes_held() const;
+
+  private:
+    struct Buf {
+        void* ptr = nullptr;
+        size_t bytes = 0;
+    };
+    std::map<std::string, Buf> bufs_;
+};
+
+struct CutState {
+    int32_t num_tiles = 0;
+    int32_t stride = 0;
+    int32_t* counts = nullptr;
+    int32_t* nodes = nullptr;
+};
+
+}  // namespace arc
+
+struct arc_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    arc::Arena arena;
+    uint32_t* d_error = nullptr;  // device error word (ARC_DEVERR_*)
+    // materials
+    arc::MaterialRecord* d_materials = nullptr;
+    int32_t num_materials = 0;
+    bool any_specular = false;
+    std::vector<ArcMaterial> host_materials;
+    // AVPL upload buffers (AvplsGpu)
+    ArcAvplHost* h_staging = nullptr;  // pinned
+    size_t h_staging_bytes = 0;
+    arc::CutState last_cut;
+    int sm_count = 148;
+    arc_lbvh* run_bvh = nullptr;  // tree rebuilt by arc_run every frame
+};
+
+struct arc_lbvh {
+    arc_context* ctx = nullptr;
+    arc::Arena arena;
+    int32_t n = 0;
+    ArcLbvhView view{};
+    bool has_reference_nodes = false;
+    ArcBvhParam ref_param{};
+    ArcAvplBvhNodeDataParam ref_data{};
+    ArcFloat3* sorted_positions = nullptr;
+    ArcFloat3* sorted_normals = nullptr;
+};
+
+namespace arc {
+
+struct GatherLaunch {
+    const ArcAvplsGpuParam* avpls;
+    const ArcGBufferView* gbuffer;
+    float3 cam;
+    const ArcGatherParams* params;
+    const ArcOutputView* out;
+};
+
+arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g);
+arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const ArcLbvhParams* p);
+arc_status launch_lbvh_reference_nodes(arc_lbvh* bvh);
+arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsGpuParam* avpls,
+                             const ArcGBufferView* gb, float3 cam, const ArcGatherParams* gp, const ArcCutParams* cp,
+                             const ArcOutputView* out);
+arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64);
+
+}  // namespace arc
+
+#endif  // ARC_INTERNAL_H_

@@ -1,0 +1,575 @@
+// Brute-force gather: radiance minus antiradiance of every AVPL at every pixel, fused into one
+// kernel.  Replaces kernel_radiance_simple + kernel_antiradiance + kernel_combine
+// (cudaGather.cu:269-314, 446-557, 782-803) and the cone antiradiance of Shaders/Gather.frag:149-188.
+//
+// Fast path (Lambertian materials, which every configured scene uses):
+//   * AVPLs are first packed into 64-byte records {p, n}, {n, w}, {w, L'}, {A, 1/|w|} with
+//     L' = L * (diffuse/pi) of the AVPL's own material (1 for light-source AVPLs), so the AVPL-side
+//     BRDF of getRadiance (cudaGather.cu:84-90) is paid once per AVPL instead of once per pair.
+//   * The receiver's Lambertian BRDF is constant per pixel and is applied once in the epilogue.
+//   * A block owns a 16 x (16*PX) pixel tile; AVPL records are staged chunk by chunk into shared
+//     memory with bulk asynchronous copies (cp.async.bulk, no multicast) on an mbarrier ring and
+//     read back as broadcast 128-bit loads, each reused for PX pixels per thread.
+//   * Radiance and antiradiance go to separate compensated sums (per-chunk FP32 partials folded
+//     into Kahan sums, or per-term Kahan) and are combined in FP64.
+// General path (specular materials or geometry-term limits): one thread per pixel evaluating the
+// full f_r on both sides of every pair.
+#include <cfloat>
+#include <cmath>
+
+#include "arc_internal.h"
+#include "device_common.cuh"
+#include "pair_math.cuh"
+
+namespace arc {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTileW = 16;
+constexpr int kStages = 2;
+
+struct BfArgs {
+    const float4* records;  // 4 float4 per AVPL
+    int32_t n;
+    const float4* gpos;
+    const float4* gnrm;
+    int64_t gpitch;
+    int32_t width, height;
+    const MaterialRecord* mats;
+    int32_t num_mats;
+    float3 cam;
+    PairConsts pc;       // per-pair constants (cone threshold, clamp, disk radius)
+    float cos_thr;       // cone: max(cos(half angle), 0.001)
+    float eps;           // cone: 0.001 (Gather.frag:10)
+    float clamp2;        // dist_clamp^2, or 0
+    float disk_r2;       // disk radius^2
+    float disk_scale;    // 1 / (pi r^2)
+    float lim_rad;       // GeoTermLimitRadiance or +inf
+    float lim_ar;        // GeoTermLimitAntiradiance or +inf
+    int32_t chunk;       // AVPL records per stage
+    float4* out_res;
+    float4* out_rad;
+    float4* out_ar;
+    double* out_res64;
+    double* out_ar64;    // antiradiance in FP64 (3 per pixel), used by the cut path
+    int64_t opitch;
+    uint32_t* err;
+    // general path (raw SoA)
+    ArcAvplsGpuParam soa;
+};
+
+// ---------------------------------------------------------------------------------------
+// pack: SoA -> 64-byte records
+// ---------------------------------------------------------------------------------------
+__global__ void pack_bf_records(ArcAvplsGpuParam a, const MaterialRecord* mats, int32_t num_mats, float4* rec,
+                                uint32_t* err) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.numAvpls) return;
+    const float3 p = ld3(a.position, i), nr = ld3(a.normal, i), w = ld3(a.incDirection, i);
+    const float3 L = ld3(a.incRadiance, i), A = ld3(a.antiradiance, i);
+    int m = a.materialIndex[i];
+    if (m < 0 || m >= num_mats) {
+        set_error(err, ARC_DEVERR_BAD_MATERIAL);
+        m = 0;
+    }
+    const float4 dif = mats[m].diffuse_exp;
+    const float inv_n = rn_div(1.0f, rn_sqrt(rn_dot(nr.x, nr.y, nr.z, nr.x, nr.y, nr.z)));
+    const float3 n = f3(rn_mul(nr.x, inv_n), rn_mul(nr.y, inv_n), rn_mul(nr.z, inv_n));
+    const float ww = rn_dot(w.x, w.y, w.z, w.x, w.y, w.z);
+    const bool light = (ww == 0.0f);
+    float3 Lp;
+    Lp.x = light ? L.x : rn_mul(L.x, rn_mul(kOneOverPi, dif.x));
+    Lp.y = light ? L.y : rn_mul(L.y, rn_mul(kOneOverPi, dif.y));
+    Lp.z = light ? L.z : rn_mul(L.z, rn_mul(kOneOverPi, dif.z));
+    const float inv_w = light ? 0.0f : rn_div(1.0f, rn_sqrt(ww));
+    float4* r = rec + 4 * i;
+    r[0] = make_float4(p.x, p.y, p.z, n.x);
+    r[1] = make_float4(n.y, n.z, w.x, w.y);
+    r[2] = make_float4(w.z, Lp.x, Lp.y, Lp.z);
+    r[3] = make_float4(A.x, A.y, A.z, inv_w);
+}
+
+// PREC: 0 = chunk partials folded into Kahan sums, 1 = per-term Kahan, 2 = naive FP32, 3 = FP64.
+// RAD = false skips the radiance sums (antiradiance-only pass of the solid-angle cut path).
+template <int AR, int PREC, int PX, bool RAD = true>
+__global__ void __launch_bounds__(kThreads) gather_bf_kernel(BfArgs k) {
+    using T = typename std::conditional<PREC == 3, double, float>::type;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float4* stage = reinterpret_cast<float4*>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)kStages * k.chunk * 64);
+
+    const int tid = threadIdx.x;
+    const int tx = tid % kTileW, ty = tid / kTileW;
+    const int x = blockIdx.x * kTileW + tx;
+    const int rows = kThreads / kTileW;  // 16
+    const int ybase = blockIdx.y * rows * PX + ty;
+
+    const int nchunks = (k.n + k.chunk - 1) / k.chunk;
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int c = 0; c < kStages && c < nchunks; ++c) {
+            const int cnt = min(k.chunk, k.n - c * k.chunk);
+            mbar_arrive_expect_tx(&bars[c], (uint32_t)cnt * 64u);
+            bulk_g2s(stage + (size_t)c * k.chunk * 4, k.records + (size_t)c * k.chunk * 4, (uint32_t)cnt * 64u,
+                     &bars[c]);
+        }
+    }
+
+    Pixel<T> pix[PX];
+    float sc[PX][6];  // Kahan compensation (PREC 0/1)
+    float ss[PX][6];  // Kahan running sums (PREC 0)
+    bool valid[PX];
+    int mat[PX];
+#pragma unroll
+    for (int j = 0; j < PX; ++j) {
+        const int y = ybase + j * rows;
+        valid[j] = (x < k.width && y < k.height);
+        mat[j] = 0;
+        float4 gp = make_float4(0, 0, 0, 0), gn = make_float4(0, 0, 0, 0);
+        if (valid[j]) {
+            gp = k.gpos[(int64_t)y * k.gpitch + x];
+            gn = k.gnrm[(int64_t)y * k.gpitch + x];
+            mat[j] = (int)gn.w;
+            if (mat[j] <= 0 || mat[j] >= k.num_mats) {
+                if (mat[j] != 0) set_error(k.err, ARC_DEVERR_BAD_MATERIAL);
+                valid[j] = false;
+            }
+        }
+        T nx = 0, ny = 0, nz = 0;
+        if (valid[j]) {
+            const T l = rsqrt_t<T>((T)gn.x * gn.x + (T)gn.y * gn.y + (T)gn.z * gn.z);
+            nx = gn.x * l;
+            ny = gn.y * l;
+            nz = gn.z * l;
+        }
+        pix[j].px = gp.x;
+        pix[j].py = gp.y;
+        pix[j].pz = gp.z;
+        pix[j].nx = nx;
+        pix[j].ny = ny;
+        pix[j].nz = nz;
+        pix[j].r0 = pix[j].r1 = pix[j].r2 = pix[j].a0 = pix[j].a1 = pix[j].a2 = 0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) sc[j][c] = ss[j][c] = 0.0f;
+    }
+
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c % kStages;
+        const uint32_t parity = (uint32_t)((c / kStages) & 1);
+        if (ok) ok = mbar_wait_bounded(&bars[s], parity, k.err);
+        if (ok) {
+            const int cnt = min(k.chunk, k.n - c * k.chunk);
+            const float4* rec = stage + (size_t)s * k.chunk * 4;
+#pragma unroll 2
+            for (int i = 0; i < cnt; ++i) {
+                const float4 q0 = rec[4 * i + 0], q1 = rec[4 * i + 1], q2 = rec[4 * i + 2], q3 = rec[4 * i + 3];
+#pragma unroll
+                for (int j = 0; j < PX; ++j) {
+                    T g, ga;
+                    pair_terms<AR, T>(q0, q1, q2, q3, pix[j], k.pc, g, ga);
+                    if (PREC == 1) {
+                        if (RAD) {
+                            kahan_add(ss[j][0], sc[j][0], (float)(q2.y * g));
+                            kahan_add(ss[j][1], sc[j][1], (float)(q2.z * g));
+                            kahan_add(ss[j][2], sc[j][2], (float)(q2.w * g));
+                        }
+                        if (AR != ARC_AR_NONE) {
+                            kahan_add(ss[j][3], sc[j][3], (float)(q3.x * ga));
+                            kahan_add(ss[j][4], sc[j][4], (float)(q3.y * ga));
+                            kahan_add(ss[j][5], sc[j][5], (float)(q3.z * ga));
+                        }
+                    } else {
+                        if (RAD) {
+                            pix[j].r0 += (T)q2.y * g;
+                            pix[j].r1 += (T)q2.z * g;
+                            pix[j].r2 += (T)q2.w * g;
+                        }
+                        if (AR != ARC_AR_NONE) {
+                            pix[j].a0 += (T)q3.x * ga;
+                            pix[j].a1 += (T)q3.y * ga;
+                            pix[j].a2 += (T)q3.z * ga;
+                        }
+                    }
+                }
+            }
+            if (PREC == 0) {
+#pragma unroll
+                for (int j = 0; j < PX; ++j) {
+                    kahan_add(ss[j][0], sc[j][0], (float)pix[j].r0);
+                    kahan_add(ss[j][1], sc[j][1], (float)pix[j].r1);
+                    kahan_add(ss[j][2], sc[j][2], (float)pix[j].r2);
+                    kahan_add(ss[j][3], sc[j][3], (float)pix[j].a0);
+                    kahan_add(ss[j][4], sc[j][4], (float)pix[j].a1);
+                    kahan_add(ss[j][5], sc[j][5], (float)pix[j].a2);
+                    pix[j].r0 = pix[j].r1 = pix[j].r2 = pix[j].a0 = pix[j].a1 = pix[j].a2 = 0;
+                }
+            }
+        }
+        __syncthreads();  // every thread is done reading stage s before it is refilled
+        if (tid == 0 && ok && c + kStages < nchunks) {
+            fence_proxy_async_smem();
+            const int cn = c + kStages;
+            const int cnt = min(k.chunk, k.n - cn * k.chunk);
+            mbar_arrive_expect_tx(&bars[s], (uint32_t)cnt * 64u);
+            bulk_g2s(stage + (size_t)s * k.chunk * 4, k.records + (size_t)cn * k.chunk * 4, (uint32_t)cnt * 64u,
+                     &bars[s]);
+        }
+    }
+
+    // epilogue: receiver BRDF, signed combine, stores
+#pragma unroll
+    for (int j = 0; j < PX; ++j) {
+        const int y = ybase + j * rows;
+        if (x >= k.width || y >= k.height) continue;
+        double rad[3] = {0, 0, 0}, ar[3] = {0, 0, 0}, res[3] = {0, 0, 0};
+        float radf[3] = {0, 0, 0}, arf[3] = {0, 0, 0}, resf[3] = {0, 0, 0};
+        if (valid[j]) {
+            const float4 d = k.mats[mat[j]].diffuse_exp;
+            const float kd[3] = {kOneOverPi * d.x, kOneOverPi * d.y, kOneOverPi * d.z};
+            const float arscale = (AR == ARC_AR_DISK) ? k.disk_scale : 1.0f;
+            if (PREC == 2) {
+                const float S[6] = {(float)pix[j].r0, (float)pix[j].r1, (float)pix[j].r2,
+                                    (float)pix[j].a0, (float)pix[j].a1, (float)pix[j].a2};
+                for (int c = 0; c < 3; ++c) {
+                    radf[c] = kd[c] * S[c];
+                    arf[c] = kd[c] * arscale * S[3 + c];
+                    resf[c] = radf[c] - arf[c];
+                    rad[c] = radf[c];
+                    ar[c] = arf[c];
+                    res[c] = resf[c];
+                }
+            } else {
+                double S[6];
+                if (PREC == 3) {
+                    S[0] = (double)pix[j].r0; S[1] = (double)pix[j].r1; S[2] = (double)pix[j].r2;
+                    S[3] = (double)pix[j].a0; S[4] = (double)pix[j].a1; S[5] = (double)pix[j].a2;
+                } else {
+                    for (int c = 0; c < 6; ++c) S[c] = (double)ss[j][c] - (double)sc[j][c];
+                }
+                for (int c = 0; c < 3; ++c) {
+                    rad[c] = (double)kd[c] * S[c];
+                    ar[c] = (double)kd[c] * (double)arscale * S[3 + c];
+                    res[c] = rad[c] - ar[c];
+                    radf[c] = (float)rad[c];
+                    arf[c] = (float)ar[c];
+                    resf[c] = (float)res[c];
+                }
+            }
+        }
+        const int64_t o = (int64_t)y * k.opitch + x;
+        if (k.out_res) k.out_res[o] = make_float4(resf[0], resf[1], resf[2], 1.0f);
+        if (k.out_rad) k.out_rad[o] = make_float4(radf[0], radf[1], radf[2], 1.0f);
+        if (k.out_ar) k.out_ar[o] = make_float4(arf[0], arf[1], arf[2], 1.0f);
+        if (k.out_res64) {
+            k.out_res64[3 * o + 0] = res[0];
+            k.out_res64[3 * o + 1] = res[1];
+            k.out_res64[3 * o + 2] = res[2];
+        }
+        if (k.out_ar64) {
+            k.out_ar64[3 * o + 0] = ar[0];
+            k.out_ar64[3 * o + 1] = ar[1];
+            k.out_ar64[3 * o + 2] = ar[2];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// General path: full f_r on both sides (cudaGather.cu:59-95), geometry-term limits
+// (Gather.frag:182, 190-194); one thread per pixel over the raw SoA arrays.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct V {
+    T x, y, z;
+};
+template <typename T>
+__device__ __forceinline__ V<T> vsub(V<T> a, V<T> b) {
+    return {a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <typename T>
+__device__ __forceinline__ V<T> vs(T s, V<T> a) {
+    return {s * a.x, s * a.y, s * a.z};
+}
+template <typename T>
+__device__ __forceinline__ T vdot(V<T> a, V<T> b) {
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <typename T>
+__device__ __forceinline__ V<T> vnorm(V<T> a) {
+    return vs(rsqrt_t<T>(vdot(a, a)), a);
+}
+
+// f_r(w_i, w_o, n, mat) = diffuse/pi + [|spec| > 0] (e+2)/(2 pi) max(0, reflect(-w_i, n).w_o)^e spec
+template <typename T>
+__device__ __forceinline__ V<T> brdf(V<T> w_i, V<T> w_o, V<T> n, const MaterialRecord& m) {
+    V<T> d = {(T)kOneOverPi * m.diffuse_exp.x, (T)kOneOverPi * m.diffuse_exp.y, (T)kOneOverPi * m.diffuse_exp.z};
+    if (m.specular_flag.w != 0.0f) {
+        const V<T> I = vs((T)-1, w_i);
+        const V<T> r = vsub(I, vs((T)2 * vdot(n, I), n));
+        T c = vdot(r, w_o);
+        c = c > (T)0 ? c : (T)0;
+        const T e = m.diffuse_exp.w;
+        const T f = (T)0.5 * (T)kOneOverPi * (e + (T)2) * (T)pow(c, e);
+        d.x += f * m.specular_flag.x;
+        d.y += f * m.specular_flag.y;
+        d.z += f * m.specular_flag.z;
+    }
+    return d;
+}
+
+template <int AR, typename T>
+__global__ void __launch_bounds__(kThreads) gather_general_kernel(BfArgs k) {
+    __shared__ MaterialRecord smat[ARC_MAX_MATERIALS];
+    for (int i = threadIdx.x; i < k.num_mats; i += blockDim.x) smat[i] = k.mats[i];
+    __syncthreads();
+    const int x = blockIdx.x * kTileW + threadIdx.x % kTileW;
+    const int y = blockIdx.y * (kThreads / kTileW) + threadIdx.x / kTileW;
+    if (x >= k.width || y >= k.height) return;
+    const float4 gp = k.gpos[(int64_t)y * k.gpitch + x];
+    const float4 gn = k.gnrm[(int64_t)y * k.gpitch + x];
+    const int m = (int)gn.w;
+    double rad[3] = {0, 0, 0}, ar[3] = {0, 0, 0};
+    if (m > 0 && m < k.num_mats) {
+        const V<T> p = {(T)gp.x, (T)gp.y, (T)gp.z};
+        const V<T> n = vnorm(V<T>{(T)gn.x, (T)gn.y, (T)gn.z});
+        const V<T> cam = {(T)k.cam.x, (T)k.cam.y, (T)k.cam.z};
+        const V<T> w_o = vnorm(vsub(cam, p));
+        T s[6] = {0, 0, 0, 0, 0, 0};
+        float c[6] = {0, 0, 0, 0, 0, 0};
+        const ArcAvplsGpuParam& a = k.soa;
+        for (int i = 0; i < a.numAvpls; ++i) {
+            const float3 fpa = ld3(a.position, i), fna = ld3(a.normal, i), fwa = ld3(a.incDirection, i);
+            const V<T> pa = {(T)fpa.x, (T)fpa.y, (T)fpa.z};
+            const V<T> na = vnorm(V<T>{(T)fna.x, (T)fna.y, (T)fna.z});
+            const V<T> wa = {(T)fwa.x, (T)fwa.y, (T)fwa.z};
+            int ma = a.materialIndex[i];
+            if (ma < 0 || ma >= k.num_mats) ma = 0;
+            const V<T> v = vsub(pa, p);
+            T l2 = vdot(v, v);
+            if (!(l2 > (T)0)) continue;
+            const V<T> w = vs(rsqrt_t<T>(l2), v);  // pixel -> AVPL
+            const V<T> fr = brdf<T>(w, w_o, n, smat[m]);
+            // radiance
+            V<T> fl = {1, 1, 1};
+            if (vdot(wa, wa) != (T)0) fl = brdf<T>(vs((T)-1, wa), vs((T)-1, w), na, smat[ma]);
+            T c1 = vdot(n, w), c2 = -vdot(na, w);
+            c1 = c1 < (T)0 ? (T)0 : (c1 > (T)1 ? (T)1 : c1);
+            c2 = c2 < (T)0 ? (T)0 : (c2 > (T)1 ? (T)1 : c2);
+            const T l2c = l2 < (T)k.clamp2 ? (T)k.clamp2 : l2;
+            T g = c1 * c2 / l2c;
+            if (g > (T)k.lim_rad) g = (T)k.lim_rad;
+            const float3 L = ld3(a.incRadiance, i), A = ld3(a.antiradiance, i);
+            T term[6];
+            term[0] = (T)L.x * fl.x * fr.x * g;
+            term[1] = (T)L.y * fl.y * fr.y * g;
+            term[2] = (T)L.z * fl.z * fr.z * g;
+            T ga = 0;
+            if (AR == ARC_AR_CONE) {
+                const T cw = -vdot(w, wa);
+                const T cn = vdot(n, w);
+                if (cw > (T)k.eps && cn > (T)k.eps && cw > (T)k.cos_thr) {
+                    ga = cn / l2c;
+                    if (ga > (T)k.lim_ar) ga = (T)k.lim_ar;
+                }
+            } else if (AR == ARC_AR_DISK) {
+                const T wn = vdot(wa, n);
+                if (wn != (T)0) {
+                    const T t = -vdot(v, n) / wn;
+                    const V<T> wu = vnorm(wa);
+                    const V<T> h = {pa.x + t * wu.x, pa.y + t * wu.y, pa.z + t * wu.z};
+                    const V<T> hp = vsub(h, p);
+                    if (t > (T)0 && vdot(hp, hp) < (T)k.disk_r2 && wn < (T)0 && -vdot(w, na) < (T)0) ga = (T)k.disk_scale;
+                }
+            }
+            term[3] = (T)A.x * fr.x * ga;
+            term[4] = (T)A.y * fr.y * ga;
+            term[5] = (T)A.z * fr.z * ga;
+            if (sizeof(T) == 8) {
+                for (int q = 0; q < 6; ++q) s[q] += term[q];
+            } else {
+                for (int q = 0; q < 6; ++q) {
+                    float ssq = (float)s[q];
+                    kahan_add(ssq, c[q], (float)term[q]);
+                    s[q] = (T)ssq;
+                }
+            }
+        }
+        for (int q = 0; q < 3; ++q) {
+            rad[q] = (double)s[q] - (double)c[q];
+            ar[q] = (double)s[3 + q] - (double)c[3 + q];
+        }
+    }
+    const int64_t o = (int64_t)y * k.opitch + x;
+    const double res[3] = {rad[0] - ar[0], rad[1] - ar[1], rad[2] - ar[2]};
+    if (k.out_res) k.out_res[o] = make_float4((float)res[0], (float)res[1], (float)res[2], 1.0f);
+    if (k.out_rad) k.out_rad[o] = make_float4((float)rad[0], (float)rad[1], (float)rad[2], 1.0f);
+    if (k.out_ar) k.out_ar[o] = make_float4((float)ar[0], (float)ar[1], (float)ar[2], 1.0f);
+    if (k.out_res64) {
+        k.out_res64[3 * o + 0] = res[0];
+        k.out_res64[3 * o + 1] = res[1];
+        k.out_res64[3 * o + 2] = res[2];
+    }
+}
+
+// Tile shapes selectable by ArcGatherParams::tile_config: pixels per thread x AVPLs per stage.
+struct TileShape {
+    int px;
+    int chunk;
+};
+constexpr TileShape kTileShapes[] = {{1, 128}, {2, 128}, {2, 256}, {4, 128}, {4, 256}, {1, 256}, {2, 64}, {4, 64}};
+constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
+constexpr int kDefaultTileShape = 2;
+
+template <int AR, int PREC, int PX, bool RAD = true>
+arc_status launch_fast(const BfArgs& a, cudaStream_t st) {
+    const size_t smem = (size_t)kStages * a.chunk * 64 + kStages * sizeof(uint64_t);
+    auto fn = gather_bf_kernel<AR, PREC, PX, RAD>;
+    if (smem > 48 * 1024) ARC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((a.width + kTileW - 1) / kTileW, (a.height + 16 * PX - 1) / (16 * PX));
+    fn<<<grid, kThreads, smem, st>>>(a);
+    ARC_TRY_CUDA(cudaGetLastError());
+    return ARC_OK;
+}
+
+template <int AR, int PREC>
+arc_status launch_fast_px(const BfArgs& a, int px, cudaStream_t st) {
+    if (px == 1) return launch_fast<AR, PREC, 1>(a, st);
+    if (px == 2) return launch_fast<AR, PREC, 2>(a, st);
+    return launch_fast<AR, PREC, 4>(a, st);
+}
+
+template <int AR>
+arc_status launch_fast_prec(const BfArgs& a, int prec, int px, cudaStream_t st) {
+    switch (prec) {
+        case 0: return launch_fast_px<AR, 0>(a, px, st);
+        case 1: return launch_fast_px<AR, 1>(a, px, st);
+        case 2: return launch_fast_px<AR, 2>(a, px, st);
+        default: return launch_fast<AR, 3, 1>(a, st);
+    }
+}
+
+BfArgs make_args(arc_context* ctx, const GatherLaunch& g);
+arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a);
+
+}  // namespace
+
+int bf_num_tile_shapes() { return kNumTileShapes; }
+
+arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g) {
+    const ArcGatherParams& p = *g.params;
+    const ArcGBufferView& gb = *g.gbuffer;
+    const ArcOutputView& out = *g.out;
+    ARC_CHECK_ARG(p.ar_kind >= 0 && p.ar_kind <= 2, "ar_kind out of range");
+    ARC_CHECK_ARG(p.precision >= 0 && p.precision <= 3, "precision out of range");
+    ARC_CHECK_ARG(p.tile_config >= -1 && p.tile_config < kNumTileShapes, "tile_config out of range");
+    ARC_CHECK_ARG(gb.width > 0 && gb.height > 0 && gb.pitch >= gb.width && gb.position && gb.normal,
+                  "bad G-buffer view");
+    ARC_CHECK_ARG(out.pitch >= gb.width && (out.result || out.radiance || out.antiradiance || out.result_fp64),
+                  "bad output view");
+    ARC_CHECK_ARG(g.avpls->numAvpls >= 0, "negative AVPL count");
+    ARC_CHECK_ARG(ctx->num_materials > 0, "materials not uploaded");
+    ARC_CHECK_ARG(p.ar_kind != ARC_AR_DISK || p.disk_radius > 0.0f, "disk radius must be > 0");
+    ARC_CHECK_ARG(reinterpret_cast<uintptr_t>(gb.position) % 16 == 0 && reinterpret_cast<uintptr_t>(gb.normal) % 16 == 0,
+                  "G-buffer planes must be 16-byte aligned");
+
+    BfArgs a = make_args(ctx, g);
+    const bool general = ctx->any_specular || p.geo_limit_radiance > 0.0f || p.geo_limit_antiradiance > 0.0f;
+    cudaStream_t st = ctx->stream;
+    if (general) {
+        dim3 grid((gb.width + kTileW - 1) / kTileW, (gb.height + 15) / 16);
+        if (p.precision == ARC_PREC_FP64) {
+            if (p.ar_kind == 0) gather_general_kernel<0, double><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 1) gather_general_kernel<1, double><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 2) gather_general_kernel<2, double><<<grid, kThreads, 0, st>>>(a);
+        } else {
+            if (p.ar_kind == 0) gather_general_kernel<0, float><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 1) gather_general_kernel<1, float><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 2) gather_general_kernel<2, float><<<grid, kThreads, 0, st>>>(a);
+        }
+        ARC_TRY_CUDA(cudaGetLastError());
+        return ARC_OK;
+    }
+    ARC_TRY(pack_records(ctx, g, a));
+    const TileShape ts = kTileShapes[p.tile_config < 0 ? kDefaultTileShape : p.tile_config];
+    a.chunk = ts.chunk;
+    switch (p.ar_kind) {
+        case 0: return launch_fast_prec<0>(a, p.precision, ts.px, st);
+        case 1: return launch_fast_prec<1>(a, p.precision, ts.px, st);
+        default: return launch_fast_prec<2>(a, p.precision, ts.px, st);
+    }
+}
+
+arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64) {
+    const ArcGatherParams& p = *g.params;
+    BfArgs a = make_args(ctx, g);
+    a.out_res = nullptr;
+    a.out_rad = nullptr;
+    a.out_res64 = nullptr;
+    a.out_ar64 = ar64;
+    cudaStream_t st = ctx->stream;
+    ARC_TRY(pack_records(ctx, g, a));
+    a.chunk = kTileShapes[kDefaultTileShape].chunk;
+    if (p.ar_kind == ARC_AR_DISK) return launch_fast<ARC_AR_DISK, 0, 2, false>(a, st);
+    return launch_fast<ARC_AR_CONE, 0, 2, false>(a, st);
+}
+
+}  // namespace arc
+
+namespace arc {
+namespace {
+
+BfArgs make_args(arc_context* ctx, const GatherLaunch& g) {
+    const ArcGatherParams& p = *g.params;
+    const ArcGBufferView& gb = *g.gbuffer;
+    const ArcOutputView& out = *g.out;
+    BfArgs a{};
+    a.n = g.avpls->numAvpls;
+    a.gpos = reinterpret_cast<const float4*>(gb.position);
+    a.gnrm = reinterpret_cast<const float4*>(gb.normal);
+    a.gpitch = gb.pitch;
+    a.width = gb.width;
+    a.height = gb.height;
+    a.mats = ctx->d_materials;
+    a.num_mats = ctx->num_materials;
+    a.cam = g.cam;
+    a.eps = 0.001f;
+    a.cos_thr = fmaxf(cosf(p.cone_half_angle), a.eps);
+    a.clamp2 = p.dist_clamp > 0.0f ? p.dist_clamp * p.dist_clamp : 0.0f;
+    a.disk_r2 = p.disk_radius * p.disk_radius;
+    a.pc.cos_thr = a.cos_thr;
+    a.pc.eps = a.eps;
+    a.pc.inv_clamp2 = p.dist_clamp > 0.0f ? 1.0f / a.clamp2 : INFINITY;
+    a.pc.disk_r2 = a.disk_r2;
+    a.disk_scale = p.disk_radius > 0.0f ? 1.0f / (kPi * p.disk_radius * p.disk_radius) : 0.0f;
+    a.lim_rad = p.geo_limit_radiance > 0.0f ? p.geo_limit_radiance : INFINITY;
+    a.lim_ar = p.geo_limit_antiradiance > 0.0f ? p.geo_limit_antiradiance : INFINITY;
+    a.out_res = reinterpret_cast<float4*>(out.result);
+    a.out_rad = reinterpret_cast<float4*>(out.radiance);
+    a.out_ar = reinterpret_cast<float4*>(out.antiradiance);
+    a.out_res64 = out.result_fp64;
+    a.opitch = out.pitch;
+    a.err = ctx->d_error;
+    a.soa = *g.avpls;
+    return a;
+}
+
+// Pack the AVPL records into the context arena.
+arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a) {
+    float4* rec = nullptr;
+    ARC_TRY(ctx->arena.get("bf_records", (size_t)(a.n > 0 ? a.n : 1) * 64, reinterpret_cast<void**>(&rec)));
+    if (a.n > 0) {
+        pack_bf_records<<<(a.n + 255) / 256, 256, 0, ctx->stream>>>(*g.avpls, ctx->d_materials, ctx->num_materials,
+                                                                     rec, ctx->d_error);
+        ARC_TRY_CUDA(cudaGetLastError());
+    }
+    a.records = rec;
+    return ARC_OK;
+}
+
+}  // namespace
+}  // namespace arc

@@ -1,0 +1,403 @@
+/*
+ * arc_api.h - C ABI of the B200 (sm_100a) AntiradianceCuts gather + LBVH library (libarc.so).
+ *
+ * Every entry point takes plain pointers and sizes, returns an arc_status, and enqueues its
+ * GPU work on the stream owned by the arc_context it is given.  The library never falls back
+ * to the CPU: when no CUDA device is usable, a call returns ARC_ERR_CUDA.  The only CPU
+ * functions are the synthetic-scene helpers at the end (arc_scene_*), which make inputs.
+ *
+ * Reference interface each group replaces (paths are inside the reference's Framework/ tree):
+ *   - AvplsGpu / AvplsGpuParam         data_gpu.h:14-40, data_gpu.cu:5-52
+ *   - MaterialsGpu / MaterialsGpuParam data_gpu.h:42-62, data_gpu.cu:54-86
+ *   - CudaGather ctor / run()          cudaGather.h:25-70, cudaGather.cu:805-1051
+ *   - kernel_radiance_simple + kernel_antiradiance + kernel_combine
+ *                                      cudaGather.cu:269-314, 446-557, 782-803
+ *   - kernel_bvh (lightcut)            cudaGather.cu:316-444
+ *   - AvplBvh ctor, Bvh::create, getBvhParam/getAvplBvhNodeDataParam
+ *                                      bvh.h:53-148, bvh.cu:325-454, 673-808
+ *   - BvhNode / BvhParam / AvplBvhNodeDataParam layouts
+ *                                      bvh.h:21-51, 104-113
+ */
+#ifndef ARC_API_H_
+#define ARC_API_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARC_API_VERSION 1
+/* The reference caches at most 20 materials in shared memory (cudaGather.cu:18); this
+ * library keeps up to 64 in constant memory and rejects more with ARC_ERR_INVALID_ARG. */
+#define ARC_MAX_MATERIALS 64
+
+typedef enum arc_status {
+    ARC_OK = 0,
+    ARC_ERR_INVALID_ARG = 1,     /* bad pointer, size, enum or parameter value */
+    ARC_ERR_TOO_FEW_AVPLS = 2,   /* LBVH needs >= 2 AVPLs (reference prints and returns, bvh.cu:327-330) */
+    ARC_ERR_STACK_OVERFLOW = 3,  /* cut traversal stack overflowed (reference paints magenta, cudaGather.cu:438-442) */
+    ARC_ERR_TIMEOUT = 4,         /* a bounded device wait gave up (mbarrier / look-back) */
+    ARC_ERR_CUDA = 5,            /* CUDA runtime error (message in arc_last_error) */
+    ARC_ERR_OUT_OF_MEMORY = 6,
+    ARC_ERR_DEVICE = 7,          /* device-side error word set; see ARC_DEVERR_* */
+    ARC_ERR_UNSUPPORTED = 8
+} arc_status;
+
+/* Bits of the device error word returned by arc_context_synchronize. */
+#define ARC_DEVERR_STACK_OVERFLOW 0x1u
+#define ARC_DEVERR_TIMEOUT 0x2u
+#define ARC_DEVERR_BAD_MATERIAL 0x4u
+#define ARC_DEVERR_BAD_NODE 0x8u
+#define ARC_DEVERR_CUT_OVERFLOW 0x10u
+
+typedef struct ArcFloat3 {
+    float x, y, z;
+} ArcFloat3;
+
+/* Host AVPL record.  Mirrors class Avpl (AVPL.h:7-57) without its shadow-map view/projection
+ * matrices, which the CUDA path never reads. */
+typedef struct ArcAvplHost {
+    ArcFloat3 position;
+    ArcFloat3 normal;
+    ArcFloat3 incRadiance;  /* L */
+    ArcFloat3 antiradiance; /* A */
+    ArcFloat3 incDirection; /* w; zero for light-source AVPLs */
+    int32_t bounce;
+    int32_t materialIndex;
+} ArcAvplHost;
+
+/* Device structure-of-arrays view of AVPLs.  Same fields and meaning as AvplsGpuParam
+ * (data_gpu.h:14-23); float3 arrays have a 12-byte stride. */
+typedef struct ArcAvplsGpuParam {
+    ArcFloat3* position;
+    ArcFloat3* normal;
+    ArcFloat3* incDirection;
+    ArcFloat3* incRadiance;
+    ArcFloat3* antiradiance;
+    int32_t* materialIndex;
+    int32_t* bounce;
+    int32_t numAvpls;
+} ArcAvplsGpuParam;
+
+/* MATERIAL (Material.h:6-12).  Index 0 is the "no surface" material (CMaterialBuffer.cpp:5-17). */
+typedef struct ArcMaterial {
+    ArcFloat3 emissive;
+    ArcFloat3 diffuse;
+    ArcFloat3 specular;
+    float exponent;
+} ArcMaterial;
+
+/* G-buffer, replacing the two GL textures read with surf2Dread (cudaGather.cu:285-290).
+ * Pitch-linear float4 planes in device memory:
+ *   position: (x, y, z, 1)          normal: (nx, ny, nz, float(materialIndex))
+ * A pixel whose material index is 0 has no surface and gathers 0. */
+typedef struct ArcGBufferView {
+    const float* position;
+    const float* normal;
+    int32_t width;
+    int32_t height;
+    int64_t pitch; /* row pitch in float4 elements (>= width) */
+} ArcGBufferView;
+
+/* Outputs, replacing the three GL render-target attachments (cudaGather.cu:805-826, where
+ * attachment 0 is the result).  float4 planes with w = 1, like the reference's surf2Dwrite.
+ * radiance / antiradiance / result_fp64 may be NULL.  result_fp64 holds 3 doubles per pixel
+ * (the FP64 signed combine before it is rounded to float). */
+typedef struct ArcOutputView {
+    float* result;
+    float* radiance;
+    float* antiradiance;
+    double* result_fp64;
+    int64_t pitch; /* row pitch in pixels, shared by all planes */
+} ArcOutputView;
+
+typedef enum arc_ar_kind {
+    ARC_AR_NONE = 0,
+    ARC_AR_DISK = 1, /* CUDA getAntiradiance (cudaGather.cu:97-144) */
+    ARC_AR_CONE = 2  /* GLSL GetAntiradiance (Shaders/Gather.frag:149-188) */
+} arc_ar_kind;
+
+typedef enum arc_precision {
+    ARC_PREC_KAHAN = 0,        /* FP32 terms, per-chunk FP32 partials folded into Kahan sums, FP64 combine (default) */
+    ARC_PREC_KAHAN_STRICT = 1, /* FP32 terms, every term Kahan-added, FP64 combine */
+    ARC_PREC_NAIVE = 2,        /* FP32 terms, plain FP32 sums, FP32 combine (the reference's arithmetic) */
+    ARC_PREC_FP64 = 3          /* every operation in FP64 */
+} arc_precision;
+
+typedef struct ArcGatherParams {
+    int32_t ar_kind;              /* arc_ar_kind */
+    float disk_radius;            /* DISK: photonRadius = photonRadiusScale * sceneExtent / 100 (cudaGather.cu:949) */
+    float cone_half_angle;        /* CONE: radians; the reference's pi / coneFactor (Gather.frag:166) */
+    float dist_clamp;             /* geometry-term distance clamp: dist^2 -> max(dist^2, clamp^2); 0 = off */
+    float geo_limit_radiance;     /* clamp(G, 0, limit) as GeoTermLimitRadiance (Gather.frag:190-194); 0 = off */
+    float geo_limit_antiradiance; /* clamp(G_A, 0, limit) as GeoTermLimitAntiradiance (Gather.frag:182); 0 = off */
+    int32_t precision;            /* arc_precision */
+    int32_t tile_config;          /* brute-force tile shape index, -1 = autotuned choice */
+} ArcGatherParams;
+
+/* Fill *p with the library defaults: cone 30 deg, no clamp, ARC_PREC_KAHAN, tile_config -1. */
+void arc_gather_params_default(ArcGatherParams* p);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Context, errors, memory                                                                  */
+/* ---------------------------------------------------------------------------------------- */
+
+typedef struct arc_context arc_context;
+
+int32_t arc_api_version(void);
+const char* arc_status_string(int32_t status);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* arc_last_error(void);
+
+/* cuda_stream: a cudaStream_t to run on, or NULL to let the context create its own. */
+arc_status arc_context_create(int32_t device, void* cuda_stream, arc_context** out);
+arc_status arc_context_destroy(arc_context* ctx);
+/* Waits for the context's stream; returns and clears the device error word. */
+arc_status arc_context_synchronize(arc_context* ctx, uint32_t* device_error_word);
+/* The context's stream (cudaStream_t). */
+void* arc_context_stream(arc_context* ctx);
+
+/* Device memory helpers for hosts without their own CUDA binding. */
+arc_status arc_device_alloc(arc_context* ctx, size_t bytes, void** out);
+arc_status arc_device_free(arc_context* ctx, void* ptr);
+arc_status arc_copy_h2d(arc_context* ctx, void* dst, const void* src, size_t bytes);
+arc_status arc_copy_d2h(arc_context* ctx, void* dst, const void* src, size_t bytes);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Scene data uploads (MaterialsGpu / AvplsGpu constructors)                                */
+/* ---------------------------------------------------------------------------------------- */
+
+/* MaterialsGpu(materials) (data_gpu.cu:54-86).  num <= ARC_MAX_MATERIALS. */
+arc_status arc_materials_upload(arc_context* ctx, const ArcMaterial* materials, int32_t num);
+
+/* AvplsGpu(avpls) (data_gpu.cu:5-52): AoS -> SoA, host -> device, into context-owned buffers
+ * that stay valid until the next upload on this context.  *out receives the device view. */
+arc_status arc_avpls_upload(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcAvplsGpuParam* out);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Brute-force gather (kernel_radiance_simple + kernel_antiradiance + kernel_combine)        */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Radiance minus antiradiance over every AVPL for every pixel, in one fused kernel. */
+arc_status arc_gather_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avpls, const ArcGBufferView* gbuffer,
+                                 ArcFloat3 camera_position, const ArcGatherParams* params,
+                                 const ArcOutputView* out);
+
+/* ---------------------------------------------------------------------------------------- */
+/* LBVH (AvplBvh)                                                                            */
+/* ---------------------------------------------------------------------------------------- */
+
+typedef enum arc_bbox_mode {
+    ARC_BBOX_SCENE = 0,         /* normalise positions over the given scene box */
+    ARC_BBOX_AVPL_REFERENCE = 1 /* normalise over the AVPL box, max seeded with FLT_MIN as bvh.cu:346-353 */
+} arc_bbox_mode;
+
+typedef struct ArcLbvhParams {
+    int32_t consider_normals; /* 6D codes truncated to 32 bits (morton.h:94-107 into MC_SIZE uint32, bvh.h:17) */
+    int32_t bbox_mode;        /* arc_bbox_mode */
+    ArcFloat3 scene_min;
+    ArcFloat3 scene_max;
+    uint32_t repr_seed; /* seed of the counter-based hash that replaces the host mt19937 of bvh.cu:694-697 */
+} ArcLbvhParams;
+
+void arc_lbvh_params_default(ArcLbvhParams* p);
+
+/* BvhNode (bvh.h:21-28): 36-byte record; left/right >= 0 are leaves, -(k+1) is inner node k. */
+typedef struct ArcBvhNode {
+    int32_t left;
+    int32_t right;
+    ArcFloat3 bbMin;
+    ArcFloat3 bbMax;
+    int32_t visited;
+} ArcBvhNode;
+
+/* BvhParam (bvh.h:44-51). */
+typedef struct ArcBvhParam {
+    int32_t numLeafs;
+    int32_t numNodes;
+    ArcBvhNode* nodes;
+    ArcFloat3* positions;
+    ArcFloat3* normals;
+} ArcBvhParam;
+
+/* AvplBvhNodeDataParam (bvh.h:104-113): 2N-1 elements, inner node k at index N+k. */
+typedef struct ArcAvplBvhNodeDataParam {
+    int32_t* size;
+    int32_t* materialIndex;
+    float* randomNumbers;
+    ArcFloat3* position;
+    ArcFloat3* normal;
+    ArcFloat3* incRadiance;
+    ArcFloat3* incDirection;
+} ArcAvplBvhNodeDataParam;
+
+/* Device views of the library's own tree layout (all device pointers, valid until the next
+ * build on the same arc_lbvh).  Node index space: leaf i -> i, inner node k -> N + k.
+ *   morton[N]          sorted Morton codes
+ *   sorted_index[N]    original AVPL index of sorted leaf i
+ *   left/right[N-1]    children of inner node k (reference encoding: leaf >= 0, inner -(k+1))
+ *   parents[2N-1]      leaves first, then inner nodes; the root's parent is -1 (bvh.cu:192-265)
+ *   range[2(N-1)]      first and last sorted leaf under inner node k
+ *   bounds[16(N-1)]    per inner node {bbMin.xyz, left}, {bbMax.xyz, right},
+ *                      {normal-cone axis.xyz, cos half-angle}, {direction-cone axis.xyz, cos half-angle}
+ *                      (left/right stored as int32 bit patterns)
+ *   records[16(2N-1)]  per node the packed gather record {p.xyz, n.x}, {n.y, n.z, w.x, w.y},
+ *                      {w.z, L'.rgb}, {A.rgb, count}: representative position/normal/direction,
+ *                      summed L' (L times the AVPL-side Lambertian BRDF) and summed A
+ *   node_data          reference AvplBvhNodeDataParam arrays (raw summed L, representative) */
+typedef struct ArcLbvhView {
+    int32_t num_leaves;
+    int32_t num_nodes;
+    const uint32_t* morton;
+    const int32_t* sorted_index;
+    const int32_t* left;
+    const int32_t* right;
+    const int32_t* parents;
+    const int32_t* range;
+    const float* bounds;
+    const float* records;
+    ArcAvplBvhNodeDataParam node_data;
+} ArcLbvhView;
+
+typedef struct arc_lbvh arc_lbvh;
+
+arc_status arc_lbvh_create(arc_context* ctx, arc_lbvh** out);
+arc_status arc_lbvh_destroy(arc_lbvh* bvh);
+/* AvplBvh(avpls, considerNormals) (bvh.cu:746-774): Morton codes, stable radix sort,
+ * Karras radix tree, bottom-up bounds and cluster data.  Every AVPL passed is a leaf (the
+ * reference's caller passes only bounce >= 1 AVPLs, Render.cpp:289-298).  num < 2 gives
+ * ARC_ERR_TOO_FEW_AVPLS. */
+arc_status arc_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const ArcLbvhParams* params);
+arc_status arc_lbvh_get_view(const arc_lbvh* bvh, ArcLbvhView* out);
+/* getBvhParam() / getAvplBvhNodeDataParam() (bvh.h:72, 141): writes host structs whose
+ * pointers address device arrays in the reference layouts (materialised on first request
+ * after each build). */
+arc_status arc_lbvh_reference_views(arc_lbvh* bvh, ArcBvhParam* bvh_param, ArcAvplBvhNodeDataParam* node_data);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Cut gather (kernel_bvh and its tile-level successors)                                    */
+/* ---------------------------------------------------------------------------------------- */
+
+typedef enum arc_cut_kind {
+    ARC_CUT_SOLID_ANGLE = 0, /* per-pixel DFS with the solid-angle test of kernel_bvh (cudaGather.cu:316-444) */
+    ARC_CUT_ERROR_BOUND = 1, /* per 8x8 tile cut: refine while the node's error bound > eps * tile estimate */
+    ARC_CUT_LEARNED = 2      /* per 8x8 tile cut: refine decision from the MLP, error bound as fallback */
+} arc_cut_kind;
+
+typedef struct arc_mlp arc_mlp;
+
+typedef struct ArcCutParams {
+    int32_t kind;                /* arc_cut_kind */
+    float solid_angle_threshold; /* ClusterRefinementThreshold, default pi/10 (CConfigManager.cpp:37) */
+    float error_bound;           /* relative error bound, default 0.01 */
+    float ar_uncertain_factor;   /* antiradiance bound multiplier for nodes whose cone test may differ
+                                    between pairs (default 16); 1 treats them like certain nodes */
+    int32_t max_cut_nodes;       /* per-tile cut capacity (ARC_DEVERR_CUT_OVERFLOW beyond it) */
+    const arc_mlp* model;        /* LEARNED only */
+    float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this */
+    int32_t debug_pixel_x;       /* SOLID_ANGLE scene probe (cudaGather.cu:338, 392-396); -1 = off */
+    int32_t debug_pixel_y;
+    int32_t* used_nodes;         /* optional device array[2N-1]: set to 1 for nodes the probe pixel used */
+} ArcCutParams;
+
+void arc_cut_params_default(ArcCutParams* p);
+
+/* avpls: the AVPL arrays the tree was built from; needed only by ARC_CUT_SOLID_ANGLE with an
+ * antiradiance mode (its antiradiance is the brute-force pass, as in run()), else may be NULL. */
+arc_status arc_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsGpuParam* avpls,
+                          const ArcGBufferView* gbuffer, ArcFloat3 camera_position, const ArcGatherParams* params,
+                          const ArcCutParams* cut, const ArcOutputView* out);
+
+/* Per-tile cut lists of the last ERROR_BOUND / LEARNED gather on this context (device pointers):
+ * tile t (row-major 8x8 tiles) uses cut_nodes[t * stride .. t * stride + counts[t]) in the
+ * node-record index space (leaf i -> i, inner k -> N + k). */
+arc_status arc_last_cut(arc_context* ctx, int32_t* num_tiles, int32_t* stride, const int32_t** counts,
+                        const int32_t** cut_nodes);
+
+/* ---------------------------------------------------------------------------------------- */
+/* CudaGather::run                                                                           */
+/* ---------------------------------------------------------------------------------------- */
+
+/* The CONF_VARS flags that select hot-path variants (CConfigManager.h:6-52). */
+typedef struct ArcRunConfig {
+    int32_t useLightCuts;             /* 1: LBVH + cut gather for radiance; 0: brute force */
+    int32_t cut_kind;                 /* arc_cut_kind used when useLightCuts */
+    float clusterRefinementThreshold; /* solid-angle threshold (pi/10) */
+    float error_bound;                /* for ERROR_BOUND / LEARNED */
+    float photonRadiusScale;          /* DISK radius = scale * sceneExtent / 100 (cudaGather.cu:949) */
+    int32_t ar_kind;                  /* arc_ar_kind */
+    float cone_half_angle;
+    float dist_clamp;
+    int32_t precision;
+    int32_t considerNormals;
+    const arc_mlp* model;
+    int32_t profile; /* print per-stage CUDA-event timings, as run(..., profile) */
+} ArcRunConfig;
+
+void arc_run_config_default(ArcRunConfig* c);
+
+/* CudaGather::run(avpls, cameraPosition, sceneProbe, sceneExtent, profile) (cudaGather.cu:836-1051):
+ * uploads the AVPLs, gathers radiance (brute force or cut) and antiradiance and writes
+ * result = radiance - antiradiance. */
+arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcFloat3 camera_position,
+                   float scene_extent, const ArcRunConfig* config, const ArcGBufferView* gbuffer,
+                   const ArcOutputView* out);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Synthetic scenes (CPU): inputs for tests and benchmarks                                   */
+/* ---------------------------------------------------------------------------------------- */
+
+#define ARC_SCENE_MAX_BOXES 32
+
+typedef struct ArcBox {
+    ArcFloat3 lo;
+    ArcFloat3 hi;
+    int32_t material;
+} ArcBox;
+
+typedef struct ArcSceneDesc {
+    int32_t num_boxes;
+    ArcBox boxes[ARC_SCENE_MAX_BOXES];
+    int32_t num_materials;
+    ArcMaterial materials[ARC_MAX_MATERIALS];
+    ArcFloat3 light_center;   /* area light quad centre (faces -y) */
+    float light_half_size;    /* half edge length of the square light */
+    ArcFloat3 light_radiance; /* emitted radiance */
+    int32_t light_material;
+    ArcFloat3 camera_position;
+    ArcFloat3 camera_target;
+    float camera_fov_deg; /* vertical field of view */
+    ArcFloat3 scene_min;
+    ArcFloat3 scene_max;
+} ArcSceneDesc;
+
+typedef enum arc_scene_preset {
+    ARC_SCENE_ROOM = 0,         /* open-front room, red/green side walls, gray 0.7 elsewhere */
+    ARC_SCENE_ROOM_2BOXES = 1,  /* room + two boxes */
+    ARC_SCENE_ROOM_RANDOM = 2,  /* room + `num_boxes` random boxes (seeded) */
+    ARC_SCENE_TRAIN_VARIANT = 3 /* room + 0..16 random boxes, random albedo and light position (seeded) */
+} arc_scene_preset;
+
+arc_status arc_scene_preset_desc(int32_t preset, uint64_t seed, int32_t num_boxes, ArcSceneDesc* out);
+
+/* Light tracer with the AVPL semantics of AvplShooter::createPath (AvplShooter.h:77-142):
+ * PCG32 stream per path, cosine-weighted bounces, Russian roulette 0.8, at most max_bounces
+ * bounces.  Writes exactly num_avpls indirect (bounce >= 1) AVPLs; *num_paths receives the
+ * number of light paths they came from. */
+arc_status arc_scene_trace_avpls(const ArcSceneDesc* scene, uint64_t seed, int32_t max_bounces,
+                                 int32_t explicit_direct_illum, int32_t num_avpls, ArcAvplHost* out,
+                                 int64_t* num_paths);
+
+/* One primary ray per pixel centre from the scene's pinhole camera.  Writes float4 planes
+ * (position (x,y,z,1), normal (n, float(material))); misses are all zero (material 0).
+ * Row 0 is the top of the image. */
+arc_status arc_scene_gbuffer(const ArcSceneDesc* scene, int32_t width, int32_t height, float* position,
+                             float* normal);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARC_API_H_ */

@@ -1,0 +1,39 @@
+"""CudaGather::run through the C ABI (arc_run): upload, optional LBVH + cut, antiradiance, combine."""
+import math
+
+import numpy as np
+import pytest
+
+import helpers as H
+from antiradiancecuts_b200 import _lib as L
+from antiradiancecuts_b200 import api, scene
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("use_cuts", [0, 1])
+def test_run_matches_oracle(ctx, use_cuts):
+    d = H.workload("room_256_4k", 128, 128, 4096)
+    gb = api.GBuffer(d["pos"], d["nrm"])
+    g = api.CudaGather(ctx, gb, d["mats"])
+    ext = scene.scene_extent(d["desc"])
+    cfg = api.run_config(useLightCuts=use_cuts, ar_kind=L.ARC_AR_DISK, dist_clamp=0.01)
+    out = g.run(d["avpls"], d["cam"], ext, cfg)
+    got = out.result64.cpu().numpy().reshape(-1, 3)
+    px = np.arange(128 * 128)
+    r = 2.0 * ext / 100.0  # photonRadiusScale * sceneExtent / 100
+    rad, ar, res = O.gather_fp64(d["pos"], d["nrm"], px, d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"],
+                                 O.params(1, 30.0, 0.01, r))
+    if use_cuts == 0:
+        assert H.rel_rmse(got, res) < 2e-5
+    else:
+        # radiance through the solid-angle lightcut (threshold pi/10), antiradiance brute force
+        ctx.upload_materials(d["mats"])
+        dv = ctx.upload_avpls(d["avpls"])
+        bvh = api.AvplBvh(ctx)
+        bvh.build(dv)
+        tree = bvh.host_arrays()
+        crad, err = O.cut_solid_angle(d["pos"], d["nrm"], px, tree, d["dif"], d["spe"], d["ex"], d["cam"],
+                                      math.pi / 10, 0.01)
+        assert H.rel_rmse(got, crad - ar) < 1e-5
