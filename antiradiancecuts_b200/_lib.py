@@ -144,6 +144,10 @@ SIGNATURES = {
     "arc_context_destroy": (_st, [_vp]),
     "arc_context_synchronize": (_st, [_vp, P(C.c_uint32)]),
     "arc_context_stream": (_vp, [_vp]),
+    "arc_context_profile": (_st, [_vp, C.c_int32]),
+    "arc_context_stage_times": (_st, [_vp, C.c_char_p, C.c_size_t, P(C.c_float), C.c_int32, P(C.c_int32)]),
+    "arc_context_launch_count": (C.c_uint64, [_vp]),
+    "arc_measure_fp32_peak": (_st, [_vp, P(C.c_double), P(C.c_double)]),
     "arc_device_alloc": (_st, [_vp, C.c_size_t, P(_vp)]),
     "arc_device_free": (_st, [_vp, _vp]),
     "arc_copy_h2d": (_st, [_vp, _vp, _vp, C.c_size_t]),

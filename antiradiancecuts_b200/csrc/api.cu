@@ -36,6 +36,32 @@ arc_status Arena::get(const char* name, size_t bytes, void** out) {
     return ARC_OK;
 }
 
+void stage_begin(arc_context* ctx, const char* name) {
+    StageTimer& t = ctx->timer;
+    if (!t.enabled) return;
+    if (t.used == t.begin.size()) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess) return;
+        if (cudaEventCreate(&b) != cudaSuccess) {
+            cudaEventDestroy(a);
+            return;
+        }
+        t.begin.push_back(a);
+        t.end.push_back(b);
+        t.names.emplace_back();
+    }
+    t.names[t.used] = name;
+    cudaEventRecord(t.begin[t.used], ctx->stream);
+}
+
+void stage_end(arc_context* ctx, int kernels_launched) {
+    ctx->launches += (uint64_t)kernels_launched;
+    StageTimer& t = ctx->timer;
+    if (!t.enabled || t.used >= t.begin.size()) return;
+    cudaEventRecord(t.end[t.used], ctx->stream);
+    ++t.used;
+}
+
 size_t Arena::bytes_held() const {
     size_t s = 0;
     for (const auto& kv : bufs_) s += kv.second.bytes;
@@ -167,6 +193,8 @@ arc_status arc_context_destroy(arc_context* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->run_bvh) arc_lbvh_destroy(ctx->run_bvh);
+    for (auto e : ctx->timer.begin) cudaEventDestroy(e);
+    for (auto e : ctx->timer.end) cudaEventDestroy(e);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_materials) cudaFree(ctx->d_materials);
     if (ctx->h_staging) cudaFreeHost(ctx->h_staging);
@@ -186,6 +214,35 @@ arc_status arc_context_synchronize(arc_context* ctx, uint32_t* device_error_word
 }
 
 void* arc_context_stream(arc_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+arc_status arc_context_profile(arc_context* ctx, int32_t enable) {
+    ARC_CHECK_ARG(ctx != nullptr, "ctx is NULL");
+    ctx->timer.enabled = enable != 0;
+    ctx->timer.used = 0;
+    return ARC_OK;
+}
+
+arc_status arc_context_stage_times(arc_context* ctx, char* names, size_t names_len, float* ms, int32_t max_stages,
+                                   int32_t* num_stages) {
+    ARC_CHECK_ARG(ctx && names && ms && num_stages && names_len > 0, "NULL argument");
+    StageTimer& t = ctx->timer;
+    ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::string joined;
+    int32_t n = 0;
+    for (size_t i = 0; i < t.used && n < max_stages; ++i, ++n) {
+        float v = 0.0f;
+        ARC_TRY_CUDA(cudaEventElapsedTime(&v, t.begin[i], t.end[i]));
+        ms[n] = v;
+        if (i) joined += ",";
+        joined += t.names[i];
+    }
+    std::snprintf(names, names_len, "%s", joined.c_str());
+    *num_stages = n;
+    t.used = 0;
+    return ARC_OK;
+}
+
+uint64_t arc_context_launch_count(arc_context* ctx) { return ctx ? ctx->launches : 0; }
 
 arc_status arc_device_alloc(arc_context* ctx, size_t bytes, void** out) {
     ARC_CHECK_ARG(ctx && out, "NULL argument");

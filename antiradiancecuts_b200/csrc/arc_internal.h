@@ -61,6 +61,15 @@ class Arena {
     std::map<std::string, Buf> bufs_;
 };
 
+// Optional per-stage CUDA-event timing (the reference's CudaTimer around each stage of run(),
+// cudaGather.cu:845-1049) and a count of the library's kernel launches.
+struct StageTimer {
+    bool enabled = false;
+    std::vector<std::string> names;
+    std::vector<cudaEvent_t> begin, end;
+    size_t used = 0;
+};
+
 struct CutState {
     int32_t num_tiles = 0;
     int32_t stride = 0;
@@ -87,6 +96,8 @@ struct arc_context {
     arc::CutState last_cut;
     int sm_count = 148;
     arc_lbvh* run_bvh = nullptr;  // tree rebuilt by arc_run every frame
+    arc::StageTimer timer;
+    uint64_t launches = 0;  // kernels launched by this context
 };
 
 struct arc_lbvh {
@@ -102,6 +113,10 @@ struct arc_lbvh {
 };
 
 namespace arc {
+
+// Stage timing and launch counting around a group of kernel launches on ctx->stream.
+void stage_begin(arc_context* ctx, const char* name);
+void stage_end(arc_context* ctx, int kernels_launched);
 
 struct GatherLaunch {
     const ArcAvplsGpuParam* avpls;

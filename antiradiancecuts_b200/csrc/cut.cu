@@ -644,7 +644,9 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
         a.used = cp->used_nodes;
         a.err = ctx->d_error;
         dim3 grid((W + 15) / 16, (H + 15) / 16);
+        stage_begin(ctx, "cut_solid_angle");
         cut_solid_angle_kernel<<<grid, 256, 0, st>>>(a);
+        stage_end(ctx, 1);
         ARC_TRY_CUDA(cudaGetLastError());
         if (gp->ar_kind != ARC_AR_NONE) {
             ARC_CHECK_ARG(avpls != nullptr, "ARC_CUT_SOLID_ANGLE with antiradiance needs the AVPL arrays");
@@ -653,9 +655,11 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
             ARC_TRY(launch_antiradiance_only(ctx, g, ar64));
         }
         dim3 cg((W + 31) / 32, (H + 7) / 8);
+        stage_begin(ctx, "combine");
         combine_kernel<<<cg, dim3(32, 8), 0, st>>>(rad64, ar64, W, H, reinterpret_cast<float4*>(out->result),
                                                   reinterpret_cast<float4*>(out->antiradiance), out->result_fp64,
                                                   out->pitch);
+        stage_end(ctx, 1);
         ARC_TRY_CUDA(cudaGetLastError());
         return ARC_OK;
     }
@@ -684,7 +688,9 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ta.tiles_x = tiles_x;
     ta.tiles_y = tiles_y;
     ta.info = info;
+    stage_begin(ctx, "cut_setup");
     cut_tile_setup<<<(tiles + kSelWarps - 1) / kSelWarps, 32 * kSelWarps, 0, st>>>(ta);
+    stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
 
     if (cp->kind == ARC_CUT_ERROR_BOUND) {
@@ -706,7 +712,9 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
         sa.err = ctx->d_error;
         const size_t smem = (size_t)kSelWarps * kSelStack * sizeof(int);
         ARC_TRY_CUDA(cudaFuncSetAttribute(cut_select_bound, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        stage_begin(ctx, "cut_select");
         cut_select_bound<<<(tiles + kSelWarps - 1) / kSelWarps, 32 * kSelWarps, smem, st>>>(sa);
+        stage_end(ctx, 1);
         ARC_TRY_CUDA(cudaGetLastError());
     } else {
         ARC_CHECK_ARG(cp->model != nullptr, "ARC_CUT_LEARNED needs a model");
@@ -736,9 +744,11 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ea.out_ar = reinterpret_cast<float4*>(out->antiradiance);
     ea.out_res64 = out->result_fp64;
     ea.opitch = out->pitch;
+    stage_begin(ctx, "cut_eval");
     if (gp->ar_kind == 0) cut_eval_kernel<0><<<tiles, 64, 0, st>>>(ea);
     if (gp->ar_kind == 1) cut_eval_kernel<1><<<tiles, 64, 0, st>>>(ea);
     if (gp->ar_kind == 2) cut_eval_kernel<2><<<tiles, 64, 0, st>>>(ea);
+    stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
     ctx->last_cut.num_tiles = tiles;
     ctx->last_cut.counts = cut_counts;

@@ -482,6 +482,7 @@ arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g) {
     cudaStream_t st = ctx->stream;
     if (general) {
         dim3 grid((gb.width + kTileW - 1) / kTileW, (gb.height + 15) / 16);
+        stage_begin(ctx, "bf_general");
         if (p.precision == ARC_PREC_FP64) {
             if (p.ar_kind == 0) gather_general_kernel<0, double><<<grid, kThreads, 0, st>>>(a);
             if (p.ar_kind == 1) gather_general_kernel<1, double><<<grid, kThreads, 0, st>>>(a);
@@ -491,17 +492,22 @@ arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g) {
             if (p.ar_kind == 1) gather_general_kernel<1, float><<<grid, kThreads, 0, st>>>(a);
             if (p.ar_kind == 2) gather_general_kernel<2, float><<<grid, kThreads, 0, st>>>(a);
         }
+        stage_end(ctx, 1);
         ARC_TRY_CUDA(cudaGetLastError());
         return ARC_OK;
     }
     ARC_TRY(pack_records(ctx, g, a));
     const TileShape ts = kTileShapes[p.tile_config < 0 ? kDefaultTileShape : p.tile_config];
     a.chunk = ts.chunk;
+    stage_begin(ctx, "bf_gather");
+    arc_status s;
     switch (p.ar_kind) {
-        case 0: return launch_fast_prec<0>(a, p.precision, ts.px, st);
-        case 1: return launch_fast_prec<1>(a, p.precision, ts.px, st);
-        default: return launch_fast_prec<2>(a, p.precision, ts.px, st);
+        case 0: s = launch_fast_prec<0>(a, p.precision, ts.px, st); break;
+        case 1: s = launch_fast_prec<1>(a, p.precision, ts.px, st); break;
+        default: s = launch_fast_prec<2>(a, p.precision, ts.px, st); break;
     }
+    stage_end(ctx, 1);
+    return s;
 }
 
 arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64) {
@@ -514,8 +520,11 @@ arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, dou
     cudaStream_t st = ctx->stream;
     ARC_TRY(pack_records(ctx, g, a));
     a.chunk = kTileShapes[kDefaultTileShape].chunk;
-    if (p.ar_kind == ARC_AR_DISK) return launch_fast<ARC_AR_DISK, 0, 2, false>(a, st);
-    return launch_fast<ARC_AR_CONE, 0, 2, false>(a, st);
+    stage_begin(ctx, "bf_antiradiance");
+    const arc_status s = p.ar_kind == ARC_AR_DISK ? launch_fast<ARC_AR_DISK, 0, 2, false>(a, st)
+                                                  : launch_fast<ARC_AR_CONE, 0, 2, false>(a, st);
+    stage_end(ctx, 1);
+    return s;
 }
 
 }  // namespace arc
@@ -563,8 +572,10 @@ arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a) {
     float4* rec = nullptr;
     ARC_TRY(ctx->arena.get("bf_records", (size_t)(a.n > 0 ? a.n : 1) * 64, reinterpret_cast<void**>(&rec)));
     if (a.n > 0) {
+        stage_begin(ctx, "bf_pack");
         pack_bf_records<<<(a.n + 255) / 256, 256, 0, ctx->stream>>>(*g.avpls, ctx->d_materials, ctx->num_materials,
                                                                      rec, ctx->d_error);
+        stage_end(ctx, 1);
         ARC_TRY_CUDA(cudaGetLastError());
     }
     a.records = rec;

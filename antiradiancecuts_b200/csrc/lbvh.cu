@@ -597,6 +597,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     ARC_TRY_CUDA(cudaMemsetAsync(visit, 0, sizeof(int32_t) * (size_t)(n - 1), st));
 
     const int grid_stride_blocks = ctx->sm_count * 4;
+    stage_begin(ctx, "lbvh_morton");
     const bool need_box = p->bbox_mode == ARC_BBOX_AVPL_REFERENCE || p->consider_normals;
     if (need_box) {
         lbvh_bbox_init<<<1, 32, 0, st>>>(bb);
@@ -615,7 +616,9 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     m.hist = hist;
     lbvh_morton<<<grid_stride_blocks, 256, 0, st>>>(m);
     lbvh_scan_hist<<<1, 256, 0, st>>>(hist);
+    stage_end(ctx, need_box ? 4 : 2);
     ARC_TRY_CUDA(cudaGetLastError());
+    stage_begin(ctx, "lbvh_sort");
 
     uint32_t* kin = keys0;
     uint32_t* kout = keys1;
@@ -639,6 +642,8 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
         std::swap(vin, vout);
     }
     // after 4 passes the sorted data is back in keys0 / vals0
+    stage_end(ctx, 4);
+    stage_begin(ctx, "lbvh_karras");
 
     KarrasArgs k;
     k.morton = kin;
@@ -660,6 +665,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     k.sorted_nrm = bvh->sorted_normals;
     k.err = ctx->d_error;
     lbvh_karras<<<(n + 255) / 256, 256, 0, st>>>(k);
+    stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
 
     BottomUpArgs bu;
@@ -675,7 +681,9 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     bu.bounds = bounds;
     bu.nd = nd;
     bu.err = ctx->d_error;
+    stage_begin(ctx, "lbvh_bottom_up");
     lbvh_bottom_up<<<(n + 255) / 256, 256, 0, st>>>(bu);
+    stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
 
     bvh->n = n;
@@ -699,8 +707,10 @@ arc_status launch_lbvh_reference_nodes(arc_lbvh* bvh) {
     const int32_t n = bvh->n;
     ArcBvhNode* nodes = nullptr;
     ARC_TRY(bvh->arena.get("ref_nodes", sizeof(ArcBvhNode) * (size_t)(n - 1), reinterpret_cast<void**>(&nodes)));
+    stage_begin(bvh->ctx, "lbvh_reference_nodes");
     lbvh_reference_nodes<<<(n - 1 + 255) / 256, 256, 0, bvh->ctx->stream>>>(
         n - 1, reinterpret_cast<const float4*>(bvh->view.bounds), nodes);
+    stage_end(bvh->ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
     bvh->ref_param.numLeafs = n;
     bvh->ref_param.numNodes = n - 1;

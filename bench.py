@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""ms/frame at 1920x1080 with 1,048,576 AVPLs: the cut gather (LBVH build + cut selection + cut
+evaluation) against the exact brute-force gather, with the cut image's RMSE against an FP64 image.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--method learned|error_bound]
+    python bench.py --impl reference      # the CPU gather (scalar FP32 restatement), same metric
+
+One step = one frame rendered from device-resident inputs (AVPL arrays, G-buffer): LBVH build +
+cut gather into HBM output planes.  Inputs (AVPLs 71 MB, G-buffer 66 MB) and the tree
+(~0.9 GB) exceed the 126 MB L2, so no flush is needed between steps.  Under torchrun (N > 1)
+every rank renders its own replica of the frame (the path does not shard across GPUs: replicas
+only); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms/frame 1080p, 1M AVPLs: learned-cut vs exact gather at ≤1% RMSE (FP64)"
+UNIT = "ms/frame"
+
+# Algorithmic FLOPs of one (pixel, record) pair of the fast gather, Lambertian, counting FFMA = 2,
+# FADD/FMUL/MUFU = 1, compares/selects = 0, per-pixel invariants hoisted:
+#   radiance: d (3) + |d|^2 (5) + rsqrt (1) + n.d (5) + n_a.d (5) + 2 cosines (2) + r^2 (1)
+#             + G (2) + 3 FFMA accumulate (6)                                        = 30
+#   cone antiradiance: w.d (5) + cos (1) + G_A (1) + 3 FFMA accumulate (6)           = 13
+#   disk antiradiance: w.n (5) + t (2) + hit (6) + |h - p|^2 (5) + 3 FFMA (6)         = 24
+FLOP_PER_PAIR = {0: 30, 1: 54, 2: 43}
+
+
+def lbvh_bytes_per_avpl() -> dict:
+    """Compulsory DRAM bytes per AVPL of each LBVH kernel (reads + writes of its inputs and
+    outputs once, N leaves and N - 1 inner nodes)."""
+    return {
+        "lbvh_morton": 12 + 8,                     # positions in; key + index out
+        "lbvh_sort": 4 * (8 + 8),                  # 4 passes: (key, index) in and out
+        "lbvh_karras": (4 + 4 + 64) + (16 + 4 + 64 + 32 + 24 + 60 + 24),  # codes, index, AVPL in; tree out
+        "lbvh_bottom_up": 2 * (24 + 12 + 4 + 64 + 32) + (24 + 60 + 64 + 32 + 64),
+    }
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=None)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        dist.barrier(device_ids=[torch.cuda.current_device()])
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, threads: int) -> dict:
+    """The scalar FP32 CPU gather (oracle restatement of the reference's formulas) on a seeded
+    pixel sample over all AVPLs, extrapolated to the full frame."""
+    from oracle import oracle as O
+
+    prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
+    H, W = pos.shape[:2]
+    valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
+    rng = np.random.default_rng(7)
+    t0 = time.perf_counter()
+    probe = rng.choice(valid, size=min(len(valid), 4 * threads), replace=False)
+    O.gather_fp32(pos, nrm, probe, avpls, dif, spe, ex, cam, prm, threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    k = int(min(len(valid), max(4 * threads, len(probe) * target_s / dt)))
+    sample = rng.choice(valid, size=k, replace=False)
+    t0 = time.perf_counter()
+    O.gather_fp32(pos, nrm, sample, avpls, dif, spe, ex, cam, prm, threads=threads)
+    dt = time.perf_counter() - t0
+    # every pixel costs the same (all AVPLs); background pixels cost nothing, so extrapolate over
+    # the valid pixels
+    ms_frame = dt * 1e3 * len(valid) / k
+    return {"value": ms_frame, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{k} random surface pixels x {len(avpls)} AVPLs (scalar FP32 C, -O2, {threads} threads), "
+                      f"{dt:.1f} s, extrapolated to {len(valid)} surface pixels"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU gather on the host cores (rank 0 only)."""
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from antiradiancecuts_b200 import scene
+
+    wl = scene.WORKLOADS[args.workload]
+    desc, avpls, paths, pos, nrm = wl.build()
+    _, dif, spe, ex = scene.materials(desc)
+    cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
+    threads = os.cpu_count() or 1
+    per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, per, threads)
+        if i >= args.warmup:
+            vals.append(b["value"])
+    v = float(np.median(vals))
+    b["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "resolution": [wl.width, wl.height], "avpls": wl.num_avpls,
+                       "method": "exact brute-force gather on the CPU (the reference has no CPU gather: scalar "
+                                 "FP32 restatement of cudaGather.cu / Gather.frag formulas)"},
+            "cpu_baseline": b, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="variant500_1080p_1m")
+    ap.add_argument("--method", default="auto", choices=["auto", "learned", "error_bound"])
+    ap.add_argument("--error-bound", type=float, default=0.01)
+    ap.add_argument("--small", action="store_true", help="640x360 / 262,144 AVPLs, no extras (profiling)")
+    ap.add_argument("--no-extras", action="store_true", help="skip exact / FP64 / CPU legs")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    from antiradiancecuts_b200 import _lib as L
+    from antiradiancecuts_b200 import api, scene
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    ctx = api.Context(local)
+    lib = ctx.lib
+    wl = scene.WORKLOADS[args.workload]
+    if args.small:
+        W, H, N = 640, 360, 262144
+        args.no_extras = True
+    else:
+        W, H, N = wl.width, wl.height, wl.num_avpls
+    desc, avpls, paths, pos, nrm = wl.build(W, H, N)
+    mats, dif, spe, ex = scene.materials(desc)
+    cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
+    ctx.upload_materials(mats)
+    dv = ctx.upload_avpls(avpls)
+    gb = api.GBuffer(pos, nrm)
+    out = api.Outputs(W, H)
+    bvh = api.AvplBvh(ctx)
+    prm = api.gather_params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
+
+    method = args.method
+    model = None
+    if method in ("auto", "learned"):
+        try:
+            from antiradiancecuts_b200 import learned
+
+            model = learned.load_default_model(ctx)
+            method = "learned"
+        except Exception as e:  # no trained model available
+            if args.method == "learned":
+                raise
+            method = "error_bound"
+            model_error = str(e)
+    kind = L.ARC_CUT_LEARNED if method == "learned" else L.ARC_CUT_ERROR_BOUND
+    cut = api.cut_params(kind, error_bound=args.error_bound, model=model.handle.value if model else None)
+
+    stream = torch.cuda.current_stream()
+
+    def frame():
+        bvh.build(dv)
+        api.gather_cut(ctx, bvh, None, gb, cam, prm, cut, out)
+
+    for _ in range(args.warmup):
+        frame()
+    assert ctx.synchronize() == 0, "device error during warm-up"
+    barrier(world)
+    torch.cuda.synchronize()
+    lib.arc_context_profile(ctx.handle, 1)
+    launches0 = lib.arc_context_launch_count(ctx.handle)
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        frame()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = lib.arc_context_launch_count(ctx.handle) - launches0
+    names = C.create_string_buffer(4096)
+    st_ms = (C.c_float * 256)()
+    nst = C.c_int32()
+    lib.arc_context_stage_times(ctx.handle, names, 4096, st_ms, 256, C.byref(nst))
+    lib.arc_context_profile(ctx.handle, 0)
+    stage_names = names.value.decode().split(",") if nst.value else []
+    per_stage = {}
+    for nme, v in zip(stage_names, list(st_ms)[: nst.value]):
+        per_stage[nme] = per_stage.get(nme, 0.0) + v / args.steps
+    assert ctx.synchronize() == 0, "device error during the timed frames"
+    barrier(world)
+    ms = max_over_ranks(world, ms)
+
+    # ---- roofline of the dominant kernel ----
+    cuts = api.last_cut(ctx)
+    valid_px = (nrm[..., 3] > 0)
+    tiles_x = (W + 7) // 8
+    pairs = 0
+    for t, c in enumerate(cuts):
+        ty, tx = divmod(t, tiles_x)
+        pairs += len(c) * int(valid_px[ty * 8:(ty + 1) * 8, tx * 8:(tx + 1) * 8].sum())
+    sc, pk = C.c_double(), C.c_double()
+    L.check(lib.arc_measure_fp32_peak(ctx.handle, C.byref(sc), C.byref(pk)), "arc_measure_fp32_peak")
+    fp32_peak = max(sc.value, pk.value)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0, "fallback": True}
+    dom = max(per_stage, key=per_stage.get) if per_stage else "cut_eval"
+    if dom == "cut_eval":
+        flops = pairs * FLOP_PER_PAIR[wl.ar_kind]
+        ach = flops / (per_stage[dom] * 1e-3) / 1e12
+        roof = {"kernel": "cut_eval", "bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": ach / fp32_peak, "traffic": None,
+                "peak_source": "measured FFMA microbenchmark (arc_measure_fp32_peak), max of scalar/packed"}
+    elif dom.startswith("lbvh"):
+        b = lbvh_bytes_per_avpl()[dom] * N
+        ach = b / (per_stage[dom] * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": ach / peaks["hbm_gbs"], "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+    else:
+        roof = {"kernel": dom, "bound": "latency", "achieved": None, "peak": None, "unit": None, "frac": None,
+                "traffic": None}
+    lb_ms = sum(v for k, v in per_stage.items() if k.startswith("lbvh"))
+    lb_bytes = sum(lbvh_bytes_per_avpl().values()) * N
+    lbvh_roof = {"achieved": lb_bytes / (lb_ms * 1e-3) / 1e9 if lb_ms else None, "peak": peaks["hbm_gbs"],
+                 "unit": "GB/s", "frac": (lb_bytes / (lb_ms * 1e-3) / 1e9) / peaks["hbm_gbs"] if lb_ms else None,
+                 "ms": lb_ms, "bytes_per_avpl": sum(lbvh_bytes_per_avpl().values())}
+
+    result = {}
+    cut_img = out.result64.cpu().numpy().reshape(-1, 3).copy()
+    if not args.no_extras:
+        # ---- exact brute-force gather (same GPU) ----
+        prm_bf = api.gather_params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
+        out_bf = api.Outputs(W, H)
+        api.gather_bruteforce(ctx, dv, gb, cam, prm_bf, out_bf)  # warm-up
+        torch.cuda.synchronize()
+        lib.arc_context_profile(ctx.handle, 1)
+        e0.record(stream)
+        for _ in range(2):
+            api.gather_bruteforce(ctx, dv, gb, cam, prm_bf, out_bf)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        exact_ms = e0.elapsed_time(e1) / 2
+        lib.arc_context_stage_times(ctx.handle, names, 4096, st_ms, 256, C.byref(nst))
+        lib.arc_context_profile(ctx.handle, 0)
+        bf_stage = {}
+        for nme, v in zip(names.value.decode().split(","), list(st_ms)[: nst.value]):
+            bf_stage[nme] = bf_stage.get(nme, 0.0) + v / 2
+        bf_pairs = int(valid_px.sum()) * N
+        bf_ach = bf_pairs * FLOP_PER_PAIR[wl.ar_kind] / (bf_stage.get("bf_gather", exact_ms) * 1e-3) / 1e12
+        # ---- FP64 image (all-FP64 GPU gather), checked against the CPU FP64 oracle on a sample ----
+        prm64 = api.gather_params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp, precision=L.ARC_PREC_FP64)
+        out64 = api.Outputs(W, H)
+        api.gather_bruteforce(ctx, dv, gb, cam, prm64, out64)
+        assert ctx.synchronize() == 0
+        ref64 = out64.result64.cpu().numpy().reshape(-1, 3)
+        exact_img = out_bf.result64.cpu().numpy().reshape(-1, 3)
+
+        def rel_rmse(a, b):
+            return float(np.max(np.sqrt(np.mean((a - b) ** 2, 0)) / (np.sqrt(np.mean(b ** 2, 0)) + 1e-300)))
+
+        from oracle import oracle as O
+
+        rng = np.random.default_rng(11)
+        sample = rng.choice(np.nonzero(valid_px.ravel())[0], size=64, replace=False)
+        _, _, o64 = O.gather_fp64(pos, nrm, sample, avpls, dif, spe, ex, cam,
+                                  O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp))
+        result = {
+            "exact_ms_per_frame": exact_ms,
+            "speedup_vs_exact": exact_ms / ms,
+            "rel_rmse_vs_fp64": rel_rmse(cut_img, ref64),
+            "exact_rel_rmse_vs_fp64": rel_rmse(exact_img, ref64),
+            "fp64_image_vs_cpu_oracle_rel_rmse": rel_rmse(ref64[sample], o64),
+            "exact_roofline": {"kernel": "bf_gather", "bound": "fp32", "achieved": bf_ach, "peak": fp32_peak,
+                               "unit": "TFLOP/s", "frac": bf_ach / fp32_peak},
+        }
+
+    # ---- e2e through the public API: CudaGather::run with host AVPLs, result read back ----
+    g = api.CudaGather(ctx, gb, mats, outputs=api.Outputs(W, H, fp64=False, parts=False))
+    rcfg = api.run_config(useLightCuts=1, cut_kind=kind, error_bound=args.error_bound, ar_kind=wl.ar_kind,
+                          cone_half_angle=math.radians(wl.cone_half_angle_deg), dist_clamp=wl.dist_clamp,
+                          model=model.handle.value if model else None)
+    host_out = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
+    for _ in range(args.warmup):
+        g.run(avpls, cam, scene.scene_extent(desc), rcfg)
+        host_out.copy_(g.outputs.result, non_blocking=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.run(avpls, cam, scene.scene_extent(desc), rcfg)
+        host_out.copy_(g.outputs.result, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(world, e0.elapsed_time(e1) / args.steps)
+
+    cpu = None
+    if rank == 0 and not args.no_extras:
+        cpu = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, args.cpu_seconds, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload if not args.small else args.workload + "_small",
+                       "resolution": [W, H], "avpls": N, "light_paths": paths, "method": method,
+                       "error_bound": args.error_bound, "antiradiance": "cone", "cone_half_angle_deg":
+                           wl.cone_half_angle_deg, "dist_clamp": wl.dist_clamp,
+                       "l2": "inputs larger than L2 (AVPLs 71 MB, G-buffer 66 MB, tree ~0.9 GB); no flush",
+                       "parallelism": f"replicas x{world}", "frames_per_s_all_gpus": world * 1000.0 / ms},
+            "stage_ms": per_stage, "gpu_launches": int(launches), "launches_per_frame": launches / args.steps,
+            "roofline": roof, "lbvh_roofline": lbvh_roof, **result,
+            "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
+                    "d2h_bytes_per_step": int(W * H * 16)},
+            "cpu_baseline": cpu, "clocks": clk,
+        }
+        if method != "learned" and args.method == "auto":
+            line["config"]["learned_unavailable"] = model_error[:200]
+        print(json.dumps(line))
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,6 +159,19 @@ arc_status arc_context_synchronize(arc_context* ctx, uint32_t* device_error_word
 /* The context's stream (cudaStream_t). */
 void* arc_context_stream(arc_context* ctx);
 
+/* Per-stage CUDA-event timing, as the reference's CudaTimer around each stage of run()
+ * (cudaGather.cu:845-1049).  While enabled, every library stage records an event pair on the
+ * context's stream; arc_context_stage_times waits for the stream and returns the recorded
+ * stages (comma-separated names, elapsed ms) since the last call, then clears them. */
+arc_status arc_context_profile(arc_context* ctx, int32_t enable);
+arc_status arc_context_stage_times(arc_context* ctx, char* names, size_t names_len, float* ms, int32_t max_stages,
+                                   int32_t* num_stages);
+/* Number of kernels this context has launched so far. */
+uint64_t arc_context_launch_count(arc_context* ctx);
+/* FP32 FMA throughput of the device with scalar FFMA and packed fma.rn.f32x2 chains (TFLOP/s),
+ * the roofline denominator of the gather kernels.  No reference counterpart. */
+arc_status arc_measure_fp32_peak(arc_context* ctx, double* scalar_tflops, double* packed_tflops);
+
 /* Device memory helpers for hosts without their own CUDA binding. */
 arc_status arc_device_alloc(arc_context* ctx, size_t bytes, void** out);
 arc_status arc_device_free(arc_context* ctx, void* ptr);
