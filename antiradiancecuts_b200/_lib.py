@@ -104,8 +104,14 @@ class ArcLbvhView(C.Structure):
 
 class ArcCutParams(C.Structure):
     _fields_ = [("kind", C.c_int32), ("solid_angle_threshold", C.c_float), ("error_bound", C.c_float),
-                ("ar_uncertain_factor", C.c_float), ("max_cut_nodes", C.c_int32), ("model", C.c_void_p), ("mlp_threshold", C.c_float),
+                ("ar_uncertain_factor", C.c_float), ("max_cut_nodes", C.c_int32), ("cut_pool_entries", C.c_int64),
+                ("model", C.c_void_p), ("mlp_threshold", C.c_float),
                 ("debug_pixel_x", C.c_int32), ("debug_pixel_y", C.c_int32), ("used_nodes", C.c_void_p)]
+
+
+class ArcCutLists(C.Structure):
+    _fields_ = [("num_tiles", C.c_int32), ("chunk_size", C.c_int32), ("max_chunks", C.c_int32),
+                ("pool_chunks_used", C.c_int32), ("counts", C.c_void_p), ("tables", C.c_void_p), ("pool", C.c_void_p)]
 
 
 class ArcRunConfig(C.Structure):
@@ -163,7 +169,7 @@ SIGNATURES = {
     "arc_lbvh_reference_views": (_st, [_vp, P(ArcBvhParam), P(ArcAvplBvhNodeDataParam)]),
     "arc_gather_cut": (_st, [_vp, _vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcGatherParams),
                              P(ArcCutParams), P(ArcOutputView)]),
-    "arc_last_cut": (_st, [_vp, P(C.c_int32), P(C.c_int32), P(_vp), P(_vp)]),
+    "arc_last_cut": (_st, [_vp, P(ArcCutLists)]),
     "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),
                       P(ArcOutputView)]),
     "arc_scene_preset_desc": (_st, [C.c_int32, C.c_uint64, C.c_int32, P(ArcSceneDesc)]),

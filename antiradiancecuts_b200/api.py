@@ -203,8 +203,8 @@ class AvplBvh:
 
 
 def cut_params(kind=L.ARC_CUT_ERROR_BOUND, error_bound=0.01, solid_angle_threshold=math.pi / 10,
-               max_cut_nodes=16384, model=None, mlp_threshold=0.5, debug_pixel=(-1, -1), used_nodes=None,
-               ar_uncertain_factor=16.0):
+               max_cut_nodes=262144, model=None, mlp_threshold=0.5, debug_pixel=(-1, -1), used_nodes=None,
+               ar_uncertain_factor=16.0, cut_pool_entries=0):
     p = L.ArcCutParams()
     L.load().arc_cut_params_default(C.byref(p))
     p.kind = kind
@@ -212,6 +212,7 @@ def cut_params(kind=L.ARC_CUT_ERROR_BOUND, error_bound=0.01, solid_angle_thresho
     p.ar_uncertain_factor = ar_uncertain_factor
     p.solid_angle_threshold = solid_angle_threshold
     p.max_cut_nodes = max_cut_nodes
+    p.cut_pool_entries = cut_pool_entries
     p.model = model
     p.mlp_threshold = mlp_threshold
     p.debug_pixel_x, p.debug_pixel_y = debug_pixel
@@ -229,12 +230,24 @@ def gather_cut(ctx: Context, bvh: AvplBvh, avpls: L.ArcAvplsGpuParam | None, gb:
 
 def last_cut(ctx: Context) -> list[np.ndarray]:
     """Cut node lists of the last tile-cut gather, one sorted array per tile."""
-    nt, stride = C.c_int32(), C.c_int32()
-    cp, np_ = C.c_void_p(), C.c_void_p()
-    L.check(ctx.lib.arc_last_cut(ctx.handle, C.byref(nt), C.byref(stride), C.byref(cp), C.byref(np_)), "arc_last_cut")
-    counts = ctx.d2h(cp.value, np.int32, nt.value)
-    nodes = ctx.d2h(np_.value, np.int32, nt.value * stride.value).reshape(nt.value, stride.value)
-    return [np.sort(nodes[t, :counts[t]]) for t in range(nt.value)]
+    cl = L.ArcCutLists()
+    L.check(ctx.lib.arc_last_cut(ctx.handle, C.byref(cl)), "arc_last_cut")
+    counts = ctx.d2h(cl.counts, np.int32, cl.num_tiles)
+    tables = ctx.d2h(cl.tables, np.int32, cl.num_tiles * cl.max_chunks).reshape(cl.num_tiles, cl.max_chunks)
+    pool = ctx.d2h(cl.pool, np.int32, cl.pool_chunks_used * cl.chunk_size).reshape(-1, cl.chunk_size)
+    out = []
+    for t in range(cl.num_tiles):
+        k = int(counts[t])
+        nch = (k + cl.chunk_size - 1) // cl.chunk_size
+        ent = pool[tables[t, :nch]].ravel()[:k] if nch else np.zeros(0, np.int32)
+        out.append(np.sort(ent))
+    return out
+
+
+def cut_counts(ctx: Context) -> np.ndarray:
+    cl = L.ArcCutLists()
+    L.check(ctx.lib.arc_last_cut(ctx.handle, C.byref(cl)), "arc_last_cut")
+    return ctx.d2h(cl.counts, np.int32, cl.num_tiles)
 
 
 def run_config(**kw) -> L.ArcRunConfig:

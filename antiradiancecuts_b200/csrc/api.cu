@@ -140,7 +140,8 @@ void arc_cut_params_default(ArcCutParams* p) {
     p->solid_angle_threshold = 3.14159265f / 10.0f;  // ClusterRefinementThreshold (CConfigManager.cpp:37)
     p->error_bound = 0.01f;
     p->ar_uncertain_factor = 16.0f;
-    p->max_cut_nodes = 16384;
+    p->max_cut_nodes = 262144;
+    p->cut_pool_entries = 0;
     p->mlp_threshold = 0.5f;
     p->debug_pixel_x = -1;
     p->debug_pixel_y = -1;
@@ -397,13 +398,21 @@ arc_status arc_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsG
     return launch_gather_cut(ctx, bvh, avpls, gbuffer, to_f3(camera_position), params, cut, out);
 }
 
-arc_status arc_last_cut(arc_context* ctx, int32_t* num_tiles, int32_t* stride, const int32_t** counts,
-                        const int32_t** cut_nodes) {
-    ARC_CHECK_ARG(ctx && num_tiles && stride && counts && cut_nodes, "NULL argument");
-    *num_tiles = ctx->last_cut.num_tiles;
-    *stride = ctx->last_cut.stride;
-    *counts = ctx->last_cut.counts;
-    *cut_nodes = ctx->last_cut.nodes;
+arc_status arc_last_cut(arc_context* ctx, ArcCutLists* out) {
+    ARC_CHECK_ARG(ctx && out, "NULL argument");
+    const CutPool& p = ctx->last_cut.pool;
+    int32_t used = 0;
+    if (p.next) {
+        ARC_TRY_CUDA(cudaMemcpyAsync(&used, p.next, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    out->num_tiles = ctx->last_cut.num_tiles;
+    out->chunk_size = 1024;
+    out->max_chunks = p.max_chunks;
+    out->pool_chunks_used = used < p.num_chunks ? used : p.num_chunks;
+    out->counts = p.counts;
+    out->tables = p.tables;
+    out->pool = p.entries;
     return ARC_OK;
 }
 

@@ -70,11 +70,20 @@ struct StageTimer {
     size_t used = 0;
 };
 
+// Per-tile cut lists: each tile's nodes live in 1024-entry chunks of one device pool, listed in
+// the tile's row of `tables` (max_chunks per tile); `next` is the pool's allocation counter.
+struct CutPool {
+    int32_t* entries = nullptr;
+    int32_t* tables = nullptr;
+    int32_t* counts = nullptr;
+    int32_t* next = nullptr;
+    int32_t num_chunks = 0;
+    int32_t max_chunks = 0;
+};
+
 struct CutState {
     int32_t num_tiles = 0;
-    int32_t stride = 0;
-    int32_t* counts = nullptr;
-    int32_t* nodes = nullptr;
+    CutPool pool;
 };
 
 }  // namespace arc

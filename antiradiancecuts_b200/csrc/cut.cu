@@ -13,7 +13,9 @@
 //   children to push).  A node is refined while an upper bound of its contribution to any pixel
 //   of the tile exceeds eps times the tile's coarse radiance estimate.  Every pixel of the tile
 //   then evaluates the same node list, so the evaluation is fully coherent.
+#include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 #include "arc_internal.h"
@@ -24,14 +26,15 @@
 namespace arc {
 
 arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64);
-arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, const ArcCutParams* cp,
-                                     const float4* tiles_info, int tiles_x, int tiles_y, int32_t* cut_nodes,
-                                     int32_t* cut_counts, int max_cut);
+arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, const ArcGatherParams* gp,
+                                     const ArcCutParams* cp, const float4* tiles_info, int tiles_x, int tiles_y,
+                                     const CutPool& pool);
 
 namespace {
 
 constexpr int kTile = 8;
 constexpr int kSolidStack = 64;
+constexpr int kChunkSize = 1024;  // cut entries per pool chunk
 constexpr int kSelWarps = 4;
 constexpr int kSelStack = 4096;
 constexpr int kCoarseDepth = 5;
@@ -380,9 +383,7 @@ struct SelArgs {
     const float4* info;
     BoundParams bp;
     int tiles;
-    int max_cut;
-    int32_t* cut_nodes;
-    int32_t* cut_counts;
+    CutPool pool;
     uint32_t* err;
 };
 
@@ -393,16 +394,15 @@ __global__ void __launch_bounds__(32 * kSelWarps) cut_select_bound(SelArgs a) {
     if (tile >= a.tiles) return;
     int* stack = sstack + warp * kSelStack;
     const TileInfo t = load_tile(a.info, tile);
-    int32_t* out = a.cut_nodes + (size_t)tile * a.max_cut;
+    CutWriter cw(a.pool, tile);
     if (t.valid == 0) {
-        if (lane == 0) a.cut_counts[tile] = 0;
+        if (lane == 0) a.pool.counts[tile] = 0;
         return;
     }
     const unsigned lt = (1u << lane) - 1u;
     int sp = 1;
     if (lane == 0) stack[0] = a.n;  // root
     __syncwarp();
-    int count = 0;
     bool overflow = false;
     int budget = 2 * a.n;  // node visits of a valid tree
     while (sp > 0) {
@@ -449,11 +449,7 @@ __global__ void __launch_bounds__(32 * kSelWarps) cut_select_bound(SelArgs a) {
             overflow = true;
         }
         const unsigned amask = __ballot_sync(0xffffffffu, accept);
-        if (accept) {
-            const int pos = count + __popc(amask & lt);
-            if (pos < a.max_cut) out[pos] = node;
-        }
-        count += __popc(amask);
+        cw.append(amask, accept, node, lane);
         if (refine) {
             const int q = sp + 2 * __popc(rmask & lt);
             stack[q] = rc;
@@ -463,12 +459,8 @@ __global__ void __launch_bounds__(32 * kSelWarps) cut_select_bound(SelArgs a) {
         __syncwarp();
     }
     if (lane == 0) {
-        if (count > a.max_cut) {
-            set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
-            count = a.max_cut;
-        }
-        if (overflow) set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
-        a.cut_counts[tile] = count;
+        if (cw.overflow || overflow) set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
+        a.pool.counts[tile] = cw.count;
     }
 }
 
@@ -484,9 +476,7 @@ struct EvalArgs {
     int num_mats;
     const float4* records;
     int tiles_x;
-    int max_cut;
-    const int32_t* cut_nodes;
-    const int32_t* cut_counts;
+    CutPool pool;
     PairConsts pc;
     float disk_scale;
     float4* out_res;
@@ -526,13 +516,15 @@ __global__ void __launch_bounds__(64) cut_eval_kernel(EvalArgs a) {
     }
     px.r0 = px.r1 = px.r2 = px.a0 = px.a1 = px.a2 = 0.0f;
     float ss[6] = {0, 0, 0, 0, 0, 0}, sc[6] = {0, 0, 0, 0, 0, 0};
-    const int count = a.cut_counts[tile];
-    const int32_t* nodes = a.cut_nodes + (size_t)tile * a.max_cut;
+    const int count = a.pool.counts[tile];
     for (int base = 0; base < count; base += kChunk) {
         const int cnt = min(kChunk, count - base);
+        // kChunk divides kChunkSize: a sub-chunk never straddles two pool chunks
+        const int32_t* nodes = a.pool.entries + (size_t)a.pool.tables[(size_t)tile * a.pool.max_chunks + base / kChunkSize] *
+                                                    kChunkSize + base % kChunkSize;
         __syncthreads();
         for (int j = i; j < cnt * 4; j += 64) {
-            const int node = nodes[base + j / 4];
+            const int node = nodes[j / 4];
             float4 q = a.records[4 * (size_t)node + (j & 3)];
             if (AR == ARC_AR_DISK && (j & 3) == 3) {
                 const float4 q1 = a.records[4 * (size_t)node + 1], q2 = a.records[4 * (size_t)node + 2];
@@ -666,12 +658,20 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
 
     // tile cuts
     const int tiles_x = (W + kTile - 1) / kTile, tiles_y = (H + kTile - 1) / kTile, tiles = tiles_x * tiles_y;
-    const int max_cut = cp->max_cut_nodes > 0 ? cp->max_cut_nodes : 4096;
+    const int max_cut = cp->max_cut_nodes > 0 ? cp->max_cut_nodes : 262144;
+    CutPool pool;
+    pool.max_chunks = (max_cut + kChunkSize - 1) / kChunkSize;
+    const int64_t pool_entries = cp->cut_pool_entries > 0 ? cp->cut_pool_entries : (int64_t)tiles * 65536;
+    pool.num_chunks = (int32_t)std::min<int64_t>((pool_entries + kChunkSize - 1) / kChunkSize, INT32_MAX / kChunkSize);
     float4* info = nullptr;
-    int32_t *cut_nodes = nullptr, *cut_counts = nullptr;
     ARC_TRY(ctx->arena.get("tile_info", (size_t)tiles * 4 * sizeof(float4), reinterpret_cast<void**>(&info)));
-    ARC_TRY(ctx->arena.get("cut_nodes", (size_t)tiles * max_cut * sizeof(int32_t), reinterpret_cast<void**>(&cut_nodes)));
-    ARC_TRY(ctx->arena.get("cut_counts", (size_t)tiles * sizeof(int32_t), reinterpret_cast<void**>(&cut_counts)));
+    ARC_TRY(ctx->arena.get("cut_pool", (size_t)pool.num_chunks * kChunkSize * sizeof(int32_t),
+                           reinterpret_cast<void**>(&pool.entries)));
+    ARC_TRY(ctx->arena.get("cut_tables", (size_t)tiles * pool.max_chunks * sizeof(int32_t),
+                           reinterpret_cast<void**>(&pool.tables)));
+    ARC_TRY(ctx->arena.get("cut_counts", (size_t)tiles * sizeof(int32_t), reinterpret_cast<void**>(&pool.counts)));
+    ARC_TRY(ctx->arena.get("cut_pool_next", sizeof(int32_t), reinterpret_cast<void**>(&pool.next)));
+    ARC_TRY_CUDA(cudaMemsetAsync(pool.next, 0, sizeof(int32_t), st));
     TileArgs ta;
     ta.gpos = reinterpret_cast<const float4*>(gb->position);
     ta.gnrm = reinterpret_cast<const float4*>(gb->normal);
@@ -706,9 +706,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
         sa.bp.disk_scale = gp->disk_radius > 0.0f ? 1.0f / (kPi * gp->disk_radius * gp->disk_radius) : 0.0f;
         sa.bp.ar_uncertain = cp->ar_uncertain_factor;
         sa.tiles = tiles;
-        sa.max_cut = max_cut;
-        sa.cut_nodes = cut_nodes;
-        sa.cut_counts = cut_counts;
+        sa.pool = pool;
         sa.err = ctx->d_error;
         const size_t smem = (size_t)kSelWarps * kSelStack * sizeof(int);
         ARC_TRY_CUDA(cudaFuncSetAttribute(cut_select_bound, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -718,7 +716,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
         ARC_TRY_CUDA(cudaGetLastError());
     } else {
         ARC_CHECK_ARG(cp->model != nullptr, "ARC_CUT_LEARNED needs a model");
-        ARC_TRY(launch_cut_select_learned(ctx, bvh, cp, info, tiles_x, tiles_y, cut_nodes, cut_counts, max_cut));
+        ARC_TRY(launch_cut_select_learned(ctx, bvh, gp, cp, info, tiles_x, tiles_y, pool));
     }
 
     EvalArgs ea;
@@ -731,9 +729,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ea.num_mats = ctx->num_materials;
     ea.records = ta.records;
     ea.tiles_x = tiles_x;
-    ea.max_cut = max_cut;
-    ea.cut_nodes = cut_nodes;
-    ea.cut_counts = cut_counts;
+    ea.pool = pool;
     ea.pc.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
     ea.pc.eps = 0.001f;
     ea.pc.inv_clamp2 = clamp2 > 0.0f ? 1.0f / clamp2 : INFINITY;
@@ -751,9 +747,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
     ctx->last_cut.num_tiles = tiles;
-    ctx->last_cut.counts = cut_counts;
-    ctx->last_cut.nodes = cut_nodes;
-    ctx->last_cut.stride = max_cut;
+    ctx->last_cut.pool = pool;
     return ARC_OK;
 }
 

@@ -4,6 +4,7 @@
 #ifndef ARC_CUT_BOUNDS_CUH_
 #define ARC_CUT_BOUNDS_CUH_
 
+#include "arc_internal.h"
 #include "device_common.cuh"
 
 namespace arc {
@@ -143,6 +144,46 @@ __device__ __forceinline__ float node_bound(const TileInfo& t, const NodeGeom& g
     }
     return rn_mul(t.kdl, m);
 }
+
+// Appends one warp's accepted nodes to its tile's chunked list in the cut pool.  Warp-uniform
+// state; every lane of the warp calls append() with the same `mask`.
+struct CutWriter {
+    static constexpr int kChunk = 1024;
+    CutPool pool;
+    int32_t* table;
+    int count = 0;
+    int chunk_id = -1;  // pool chunk holding entry count - 1
+    bool overflow = false;
+
+    __device__ CutWriter(const CutPool& p, int tile) : pool(p), table(p.tables + (size_t)tile * p.max_chunks) {}
+
+    __device__ __forceinline__ void append(unsigned mask, bool mine, int node, int lane) {
+        const int n = __popc(mask);
+        if (n == 0) return;
+        const int first_new = count % kChunk == 0 ? count / kChunk : count / kChunk + 1;
+        const int last = (count + n - 1) / kChunk;
+        int new_id = -1;
+        if (last >= first_new) {  // the batch starts a new chunk (at most one: n <= 32 < kChunk)
+            if (lane == 0) {
+                new_id = last < pool.max_chunks ? atomicAdd(pool.next, 1) : pool.num_chunks;
+                if (new_id < pool.num_chunks) table[last] = new_id;
+            }
+            new_id = __shfl_sync(0xffffffffu, new_id, 0);
+            if (new_id >= pool.num_chunks) overflow = true;
+        }
+        if (mine) {
+            const int pos = count + __popc(mask & ((1u << lane) - 1u));
+            const int id = pos / kChunk == last && last >= first_new ? new_id : chunk_id;
+            if (id >= 0 && id < pool.num_chunks) pool.entries[(size_t)id * kChunk + pos % kChunk] = node;
+        }
+        if (last >= first_new) chunk_id = new_id;
+        if (overflow) {
+            count = min(count + n, last * kChunk);  // keep only entries that landed in a chunk
+        } else {
+            count += n;
+        }
+    }
+};
 
 }  // namespace arc
 

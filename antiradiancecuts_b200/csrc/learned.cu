@@ -3,8 +3,8 @@
 
 namespace arc {
 
-arc_status launch_cut_select_learned(arc_context*, const arc_lbvh*, const ArcCutParams*, const float4*, int, int,
-                                     int32_t*, int32_t*, int) {
+arc_status launch_cut_select_learned(arc_context*, const arc_lbvh*, const ArcGatherParams*, const ArcCutParams*,
+                                     const float4*, int, int, const CutPool&) {
     set_last_error("learned cut not available");
     return ARC_ERR_UNSUPPORTED;
 }

@@ -307,7 +307,8 @@ typedef struct ArcCutParams {
     float error_bound;           /* relative error bound, default 0.01 */
     float ar_uncertain_factor;   /* antiradiance bound multiplier for nodes whose cone test may differ
                                     between pairs (default 16); 1 treats them like certain nodes */
-    int32_t max_cut_nodes;       /* per-tile cut capacity (ARC_DEVERR_CUT_OVERFLOW beyond it) */
+    int32_t max_cut_nodes;       /* per-tile cut capacity, default 262144 (ARC_DEVERR_CUT_OVERFLOW beyond it) */
+    int64_t cut_pool_entries;    /* total cut entries over all tiles; 0 = 65536 per tile */
     const arc_mlp* model;        /* LEARNED only */
     float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this */
     int32_t debug_pixel_x;       /* SOLID_ANGLE scene probe (cudaGather.cu:338, 392-396); -1 = off */
@@ -323,11 +324,20 @@ arc_status arc_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsG
                           const ArcGBufferView* gbuffer, ArcFloat3 camera_position, const ArcGatherParams* params,
                           const ArcCutParams* cut, const ArcOutputView* out);
 
-/* Per-tile cut lists of the last ERROR_BOUND / LEARNED gather on this context (device pointers):
- * tile t (row-major 8x8 tiles) uses cut_nodes[t * stride .. t * stride + counts[t]) in the
- * node-record index space (leaf i -> i, inner k -> N + k). */
-arc_status arc_last_cut(arc_context* ctx, int32_t* num_tiles, int32_t* stride, const int32_t** counts,
-                        const int32_t** cut_nodes);
+/* Per-tile cut lists of the last ERROR_BOUND / LEARNED gather on this context (device pointers).
+ * Tile t (row-major 8x8 tiles) holds counts[t] nodes in the node-record index space (leaf i -> i,
+ * inner k -> N + k); entry j of tile t is pool[tables[t * max_chunks + j / chunk_size] *
+ * chunk_size + j % chunk_size]. */
+typedef struct ArcCutLists {
+    int32_t num_tiles;
+    int32_t chunk_size;
+    int32_t max_chunks;
+    int32_t pool_chunks_used;
+    const int32_t* counts;
+    const int32_t* tables;
+    const int32_t* pool;
+} ArcCutLists;
+arc_status arc_last_cut(arc_context* ctx, ArcCutLists* out);
 
 /* ---------------------------------------------------------------------------------------- */
 /* CudaGather::run                                                                           */

@@ -75,7 +75,7 @@ def test_error_bound_cut_lists_identical(ctx, boxes, eps):
     d, dv, bvh, tree, gb = boxes
     w = d["w"]
     prm = api.gather_params(L.ARC_AR_CONE, w.cone_half_angle_deg, w.dist_clamp)
-    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=eps, max_cut_nodes=65536)
+    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=eps)
     out = api.Outputs(W, HGT)
     api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, cut, out)
     assert ctx.synchronize() == 0
@@ -100,7 +100,16 @@ def test_error_bound_cut_lists_identical(ctx, boxes, eps):
 def test_cut_overflow_is_reported(ctx, boxes):
     d, dv, bvh, tree, gb = boxes
     prm = api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
-    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.001, max_cut_nodes=64)
     out = api.Outputs(W, HGT)
+    # per-tile capacity
+    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.001, max_cut_nodes=2048)
     api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, cut, out)
     assert ctx.synchronize() & L.ARC_DEVERR_CUT_OVERFLOW
+    counts = api.cut_counts(ctx)
+    assert counts.max() <= 2048
+    # pool capacity
+    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.001, cut_pool_entries=100 * 1024)
+    api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, cut, out)
+    assert ctx.synchronize() & L.ARC_DEVERR_CUT_OVERFLOW
+    cl = api.last_cut(ctx)
+    assert sum(len(c) for c in cl) <= 100 * 1024
