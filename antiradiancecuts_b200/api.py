@@ -28,16 +28,20 @@ def _torch():
 
 
 class Context:
-    """arc_context on `device`, running on torch's current stream of that device."""
+    """arc_context on `device`.  It owns a torch CUDA stream and makes it torch's current stream,
+    so tensor allocations, fills and copies are ordered with the library's kernels (the legacy
+    default stream would not be: the library's streams are non-blocking)."""
 
     def __init__(self, device: int = 0):
         torch = _torch()
         self.lib = L.load()
         self.device = device
         torch.cuda.set_device(device)
-        stream = torch.cuda.current_stream(device).cuda_stream
+        self.stream = torch.cuda.Stream(device)
+        torch.cuda.set_stream(self.stream)
         h = C.c_void_p()
-        L.check(self.lib.arc_context_create(device, C.c_void_p(stream), C.byref(h)), "arc_context_create")
+        L.check(self.lib.arc_context_create(device, C.c_void_p(self.stream.cuda_stream), C.byref(h)),
+                "arc_context_create")
         self.handle = h
         self._avpl_keep = None
         self._children = weakref.WeakSet()  # objects whose handles live in this context
@@ -203,7 +207,7 @@ class AvplBvh:
 
 
 def cut_params(kind=L.ARC_CUT_ERROR_BOUND, error_bound=0.01, solid_angle_threshold=math.pi / 10,
-               max_cut_nodes=262144, model=None, mlp_threshold=0.5, debug_pixel=(-1, -1), used_nodes=None,
+               max_cut_nodes=1 << 20, model=None, mlp_threshold=0.5, debug_pixel=(-1, -1), used_nodes=None,
                ar_uncertain_factor=16.0, cut_pool_entries=0):
     p = L.ArcCutParams()
     L.load().arc_cut_params_default(C.byref(p))

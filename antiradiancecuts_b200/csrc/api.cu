@@ -140,7 +140,7 @@ void arc_cut_params_default(ArcCutParams* p) {
     p->solid_angle_threshold = 3.14159265f / 10.0f;  // ClusterRefinementThreshold (CConfigManager.cpp:37)
     p->error_bound = 0.01f;
     p->ar_uncertain_factor = 16.0f;
-    p->max_cut_nodes = 262144;
+    p->max_cut_nodes = 1 << 20;
     p->cut_pool_entries = 0;
     p->mlp_threshold = 0.5f;
     p->debug_pixel_x = -1;

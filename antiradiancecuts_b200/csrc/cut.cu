@@ -658,7 +658,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
 
     // tile cuts
     const int tiles_x = (W + kTile - 1) / kTile, tiles_y = (H + kTile - 1) / kTile, tiles = tiles_x * tiles_y;
-    const int max_cut = cp->max_cut_nodes > 0 ? cp->max_cut_nodes : 262144;
+    const int max_cut = cp->max_cut_nodes > 0 ? cp->max_cut_nodes : (1 << 20);
     CutPool pool;
     pool.max_chunks = (max_cut + kChunkSize - 1) / kChunkSize;
     const int64_t pool_entries = cp->cut_pool_entries > 0 ? cp->cut_pool_entries : (int64_t)tiles * 65536;

@@ -247,7 +247,7 @@ def main():
     cut = api.cut_params(kind, error_bound=args.error_bound, model=model.handle.value if model else None,
                          cut_pool_entries=tiles * 65536)
 
-    stream = torch.cuda.current_stream()
+    stream = ctx.stream  # the context's stream (also torch's current stream)
 
     def frame():
         bvh.build(dv)
@@ -255,7 +255,8 @@ def main():
 
     for _ in range(args.warmup):
         frame()
-    assert ctx.synchronize() == 0, "device error during warm-up"
+    word = ctx.synchronize()
+    assert word == 0, f"device error word 0x{word:x} during warm-up"
     barrier(world)
     torch.cuda.synchronize()
     lib.arc_context_profile(ctx.handle, 1)

@@ -307,7 +307,7 @@ typedef struct ArcCutParams {
     float error_bound;           /* relative error bound, default 0.01 */
     float ar_uncertain_factor;   /* antiradiance bound multiplier for nodes whose cone test may differ
                                     between pairs (default 16); 1 treats them like certain nodes */
-    int32_t max_cut_nodes;       /* per-tile cut capacity, default 262144 (ARC_DEVERR_CUT_OVERFLOW beyond it) */
+    int32_t max_cut_nodes;       /* per-tile cut capacity, default 2^20 (ARC_DEVERR_CUT_OVERFLOW beyond it) */
     int64_t cut_pool_entries;    /* total cut entries over all tiles; 0 = 65536 per tile */
     const arc_mlp* model;        /* LEARNED only */
     float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this */
