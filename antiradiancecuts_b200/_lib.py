@@ -162,6 +162,8 @@ SIGNATURES = {
     "arc_avpls_upload": (_st, [_vp, P(ArcAvplHost), C.c_int32, P(ArcAvplsGpuParam)]),
     "arc_gather_bruteforce": (_st, [_vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcGatherParams),
                                     P(ArcOutputView)]),
+    "arc_gather_bruteforce_noalloc": (_st, [_vp, P(ArcMaterial), C.c_int32, P(ArcAvplsGpuParam), P(ArcGBufferView),
+                                            ArcFloat3, P(ArcGatherParams), P(ArcOutputView), P(C.c_uint32)]),
     "arc_lbvh_create": (_st, [_vp, P(_vp)]),
     "arc_lbvh_destroy": (_st, [_vp]),
     "arc_lbvh_build": (_st, [_vp, P(ArcAvplsGpuParam), P(ArcLbvhParams)]),

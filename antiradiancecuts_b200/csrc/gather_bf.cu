@@ -584,3 +584,169 @@ arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a) {
 
 }  // namespace
 }  // namespace arc
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free brute-force gather (arc_gather_bruteforce_noalloc).
+//
+// For hosts that own every byte of device memory themselves and forbid the library from
+// allocating: renderer plugins whose host pre-allocates a fixed device budget at start-up, and
+// real-time frame loops that must not call cudaMalloc/cudaFree mid-frame (both can synchronise
+// the device and stall the frame).  Such a caller cannot create an arc_context (which
+// allocates), so this entry point takes a stream instead and keeps its only scratch -- the
+// packed AVPL records, the material table and the device error word -- in one file-scope
+// __device__ array of fixed size, which every GPU that loads libarc holds until the process
+// exits.
+// ---------------------------------------------------------------------------------------
+#include <mutex>
+
+static constexpr int kNoAllocMaxAvpls = 65536;  // AVPL records the static scratch holds
+static constexpr size_t kNoAllocRecordBytes = (size_t)kNoAllocMaxAvpls * 64;
+static constexpr size_t kNoAllocMaterialBytes = ARC_MAX_MATERIALS * sizeof(arc::MaterialRecord);
+// [records: 64 B x kNoAllocMaxAvpls][materials: 32 B x 64][error word: 256 B]  (4.2 MB)
+static constexpr size_t kNoAllocBytes = kNoAllocRecordBytes + kNoAllocMaterialBytes + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace arc {
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device with that
+// device current.  The host-side name g_noalloc_scratch is only a stand-in for the symbol and
+// must never be handed to a kernel.
+arc_status noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    ARC_TRY_CUDA(cudaGetDevice(&dev));
+    ARC_CHECK_ARG(dev >= 0 && dev < kNoAllocMaxDevices, "device index beyond the allocation-free path's table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        ARC_TRY_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return ARC_OK;
+}
+
+}  // namespace
+}  // namespace arc
+
+extern "C" arc_status arc_gather_bruteforce_noalloc(void* cuda_stream, const ArcMaterial* materials,
+                                                    int32_t num_materials, const ArcAvplsGpuParam* avpls,
+                                                    const ArcGBufferView* gbuffer, ArcFloat3 camera_position,
+                                                    const ArcGatherParams* params, const ArcOutputView* out,
+                                                    uint32_t* device_error_word) {
+    using namespace arc;
+    ARC_CHECK_ARG(materials && avpls && gbuffer && params && out, "NULL argument");
+    const ArcGatherParams& p = *params;
+    const ArcGBufferView& gb = *gbuffer;
+    ARC_CHECK_ARG(num_materials > 0 && num_materials <= ARC_MAX_MATERIALS,
+                  "material count must be in [1, ARC_MAX_MATERIALS]");
+    ARC_CHECK_ARG(avpls->numAvpls >= 0, "negative AVPL count");
+    if (avpls->numAvpls > kNoAllocMaxAvpls) {
+        set_last_error("arc_gather_bruteforce_noalloc: " + std::to_string(avpls->numAvpls) +
+                       " AVPLs exceed the allocation-free path's maximum of " + std::to_string(kNoAllocMaxAvpls) +
+                       " (use arc_gather_bruteforce)");
+        return ARC_ERR_INVALID_ARG;
+    }
+    ARC_CHECK_ARG(p.ar_kind >= 0 && p.ar_kind <= 2, "ar_kind out of range");
+    ARC_CHECK_ARG(p.precision >= 0 && p.precision <= 3, "precision out of range");
+    ARC_CHECK_ARG(p.tile_config >= -1 && p.tile_config < kNumTileShapes, "tile_config out of range");
+    ARC_CHECK_ARG(gb.width > 0 && gb.height > 0 && gb.pitch >= gb.width && gb.position && gb.normal,
+                  "bad G-buffer view");
+    ARC_CHECK_ARG(reinterpret_cast<uintptr_t>(gb.position) % 16 == 0 && reinterpret_cast<uintptr_t>(gb.normal) % 16 == 0,
+                  "G-buffer planes must be 16-byte aligned");
+    ARC_CHECK_ARG(out->pitch >= gb.width && (out->result || out->radiance || out->antiradiance || out->result_fp64),
+                  "bad output view");
+    ARC_CHECK_ARG(p.ar_kind != ARC_AR_DISK || p.disk_radius > 0.0f, "disk radius must be > 0");
+
+    unsigned char* scratch = nullptr;
+    ARC_TRY(noalloc_scratch(&scratch));
+    float4* records = reinterpret_cast<float4*>(scratch);
+    MaterialRecord* mats = reinterpret_cast<MaterialRecord*>(scratch + kNoAllocRecordBytes);
+    uint32_t* err = reinterpret_cast<uint32_t*>(scratch + kNoAllocRecordBytes + kNoAllocMaterialBytes);
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+
+    // material table and error word: the scratch keeps the previous call's contents, so both are
+    // rewritten here (the records are rewritten by the pack kernel for every AVPL used)
+    MaterialRecord recs[ARC_MAX_MATERIALS];
+    bool spec = false;
+    for (int i = 0; i < num_materials; ++i) {
+        const ArcMaterial& m = materials[i];
+        const float sl = sqrtf(m.specular.x * m.specular.x + m.specular.y * m.specular.y + m.specular.z * m.specular.z);
+        recs[i].diffuse_exp = make_float4(m.diffuse.x, m.diffuse.y, m.diffuse.z, m.exponent);
+        recs[i].specular_flag = make_float4(m.specular.x, m.specular.y, m.specular.z, sl > 0.0f ? 1.0f : 0.0f);
+        spec = spec || sl > 0.0f;
+    }
+    ARC_TRY_CUDA(cudaMemcpyAsync(mats, recs, sizeof(MaterialRecord) * num_materials, cudaMemcpyHostToDevice, st));
+    ARC_TRY_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+
+    BfArgs a{};
+    a.n = avpls->numAvpls;
+    a.gpos = reinterpret_cast<const float4*>(gb.position);
+    a.gnrm = reinterpret_cast<const float4*>(gb.normal);
+    a.gpitch = gb.pitch;
+    a.width = gb.width;
+    a.height = gb.height;
+    a.mats = mats;
+    a.num_mats = num_materials;
+    a.cam = make_float3(camera_position.x, camera_position.y, camera_position.z);
+    a.eps = 0.001f;
+    a.cos_thr = fmaxf(cosf(p.cone_half_angle), a.eps);
+    a.clamp2 = p.dist_clamp > 0.0f ? p.dist_clamp * p.dist_clamp : 0.0f;
+    a.disk_r2 = p.disk_radius * p.disk_radius;
+    a.pc.cos_thr = a.cos_thr;
+    a.pc.eps = a.eps;
+    a.pc.inv_clamp2 = p.dist_clamp > 0.0f ? 1.0f / a.clamp2 : INFINITY;
+    a.pc.disk_r2 = a.disk_r2;
+    a.disk_scale = p.disk_radius > 0.0f ? 1.0f / (kPi * p.disk_radius * p.disk_radius) : 0.0f;
+    a.lim_rad = p.geo_limit_radiance > 0.0f ? p.geo_limit_radiance : INFINITY;
+    a.lim_ar = p.geo_limit_antiradiance > 0.0f ? p.geo_limit_antiradiance : INFINITY;
+    a.out_res = reinterpret_cast<float4*>(out->result);
+    a.out_rad = reinterpret_cast<float4*>(out->radiance);
+    a.out_ar = reinterpret_cast<float4*>(out->antiradiance);
+    a.out_res64 = out->result_fp64;
+    a.out_ar64 = nullptr;
+    a.opitch = out->pitch;
+    a.err = err;
+    a.soa = *avpls;
+    a.records = records;
+
+    if (spec || p.geo_limit_radiance > 0.0f || p.geo_limit_antiradiance > 0.0f) {
+        dim3 grid((gb.width + kTileW - 1) / kTileW, (gb.height + 15) / 16);
+        if (p.precision == ARC_PREC_FP64) {
+            if (p.ar_kind == 0) gather_general_kernel<0, double><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 1) gather_general_kernel<1, double><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 2) gather_general_kernel<2, double><<<grid, kThreads, 0, st>>>(a);
+        } else {
+            if (p.ar_kind == 0) gather_general_kernel<0, float><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 1) gather_general_kernel<1, float><<<grid, kThreads, 0, st>>>(a);
+            if (p.ar_kind == 2) gather_general_kernel<2, float><<<grid, kThreads, 0, st>>>(a);
+        }
+        ARC_TRY_CUDA(cudaGetLastError());
+    } else {
+        if (a.n > 0) {
+            pack_bf_records<<<(a.n + 255) / 256, 256, 0, st>>>(*avpls, mats, num_materials, records, err);
+            ARC_TRY_CUDA(cudaGetLastError());
+        }
+        const TileShape ts = kTileShapes[p.tile_config < 0 ? kDefaultTileShape : p.tile_config];
+        a.chunk = ts.chunk;
+        arc_status s;
+        switch (p.ar_kind) {
+            case 0: s = launch_fast_prec<0>(a, p.precision, ts.px, st); break;
+            case 1: s = launch_fast_prec<1>(a, p.precision, ts.px, st); break;
+            default: s = launch_fast_prec<2>(a, p.precision, ts.px, st); break;
+        }
+        ARC_TRY(s);
+    }
+    if (device_error_word) {
+        uint32_t w = 0;
+        ARC_TRY_CUDA(cudaMemcpyAsync(&w, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        ARC_TRY_CUDA(cudaStreamSynchronize(st));
+        *device_error_word = w;
+    }
+    return ARC_OK;
+}

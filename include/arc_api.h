@@ -198,6 +198,25 @@ arc_status arc_gather_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avpls
                                  ArcFloat3 camera_position, const ArcGatherParams* params,
                                  const ArcOutputView* out);
 
+/* Allocation-free variant of arc_gather_bruteforce, for callers that may not allocate device
+ * memory through the library: hosts that pre-allocate a fixed device budget and forbid
+ * cudaMalloc/cudaFree after start-up (an allocation can synchronise the device and stall a
+ * frame), or plugin hosts that own every device allocation themselves.  No counterpart in the
+ * reference.  It needs no arc_context: work is enqueued on `cuda_stream` (NULL = the legacy
+ * default stream) of the current device, materials come from the host array, and the caller
+ * passes the AVPL arrays, the G-buffer and the outputs.  Its scratch (packed AVPL records, the
+ * material table, the device error word) is one fixed file-scope device array that every GPU
+ * loading libarc holds until process exit; it is sized for at most 65,536 AVPLs, and larger
+ * inputs are rejected with ARC_ERR_INVALID_ARG.  The first call on a device looks up that
+ * array's device address; make it before any stream capture.  All calls share the array:
+ * calls whose GPU work overlaps (on different streams or devices sharing a process) race on it.
+ * If device_error_word is non-NULL the call waits for the stream and returns the error word
+ * (ARC_DEVERR_*) of this call. */
+arc_status arc_gather_bruteforce_noalloc(void* cuda_stream, const ArcMaterial* materials, int32_t num_materials,
+                                         const ArcAvplsGpuParam* avpls, const ArcGBufferView* gbuffer,
+                                         ArcFloat3 camera_position, const ArcGatherParams* params,
+                                         const ArcOutputView* out, uint32_t* device_error_word);
+
 /* ---------------------------------------------------------------------------------------- */
 /* LBVH (AvplBvh)                                                                            */
 /* ---------------------------------------------------------------------------------------- */
