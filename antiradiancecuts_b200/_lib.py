@@ -172,6 +172,14 @@ SIGNATURES = {
     "arc_gather_cut": (_st, [_vp, _vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcGatherParams),
                              P(ArcCutParams), P(ArcOutputView)]),
     "arc_last_cut": (_st, [_vp, P(ArcCutLists)]),
+    "arc_mlp_num_params": (C.c_int32, []),
+    "arc_mlp_create": (_st, [_vp, C.c_uint64, P(_vp)]),
+    "arc_mlp_destroy": (_st, [_vp]),
+    "arc_mlp_set_params": (_st, [_vp, P(C.c_float), C.c_int32]),
+    "arc_mlp_get_params": (_st, [_vp, P(C.c_float), C.c_int32]),
+    "arc_mlp_forward": (_st, [_vp, _vp, C.c_int64, _vp]),
+    "arc_mlp_gradients": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, P(C.c_float), P(C.c_float)]),
+    "arc_mlp_train_step": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float, _vp]),
     "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),
                       P(ArcOutputView)]),
     "arc_scene_preset_desc": (_st, [C.c_int32, C.c_uint64, C.c_int32, P(ArcSceneDesc)]),

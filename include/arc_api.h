@@ -359,6 +359,31 @@ typedef struct ArcCutLists {
 arc_status arc_last_cut(arc_context* ctx, ArcCutLists* out);
 
 /* ---------------------------------------------------------------------------------------- */
+/* Cut-refinement MLP (no counterpart in the reference)                                      */
+/* ---------------------------------------------------------------------------------------- */
+
+/* 16 -> 64 -> 64 -> 64 -> 1 multilayer perceptron with GELU activations: BF16 weights and
+ * activations on the tensor cores (tcgen05), FP32 accumulation, FP32 master parameters
+ * (layout: W1[64][16], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4).  Features
+ * are BF16 rows of 16 values (16-byte aligned); the output is the logit of "refine this node". */
+int32_t arc_mlp_num_params(void);
+arc_status arc_mlp_create(arc_context* ctx, uint64_t seed, arc_mlp** out);
+arc_status arc_mlp_destroy(arc_mlp* mlp);
+arc_status arc_mlp_set_params(arc_mlp* mlp, const float* host_params, int32_t num);
+arc_status arc_mlp_get_params(arc_mlp* mlp, float* host_params, int32_t num);
+/* logits[rows] = MLP(features[rows][16]) (device pointers, enqueued on the context's stream). */
+arc_status arc_mlp_forward(arc_mlp* mlp, const void* features_bf16, int64_t rows, float* logits);
+/* Weighted binary cross-entropy gradient of the whole batch (sum(w * bce) / weight_sum) into
+ * host_grads[num params] and host_loss; waits for the stream.  labels / weights: device arrays
+ * (weights may be NULL = 1). */
+arc_status arc_mlp_gradients(arc_mlp* mlp, const void* features_bf16, const float* labels, const float* weights,
+                             int64_t rows, float weight_sum, float* host_grads, float* host_loss);
+/* One Adam step (beta 0.9 / 0.999) on the batch's gradient; device_loss_accum (optional, device
+ * float) accumulates the batch loss.  Enqueued only. */
+arc_status arc_mlp_train_step(arc_mlp* mlp, const void* features_bf16, const float* labels, const float* weights,
+                              int64_t rows, float weight_sum, float lr, float* device_loss_accum);
+
+/* ---------------------------------------------------------------------------------------- */
 /* CudaGather::run                                                                           */
 /* ---------------------------------------------------------------------------------------- */
 

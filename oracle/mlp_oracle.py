@@ -1,0 +1,72 @@
+"""FP64 NumPy restatement of the cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, exact GELU) with
+its weighted binary-cross-entropy gradient.  TEST INFRASTRUCTURE ONLY: the checker for the
+tensor-core kernels in antiradiancecuts_b200/csrc/mlp.cu; the product never imports it.
+
+Parameter layout (FP32 master copy of the library): W1[64][16], b1[64], W2[64][64], b2[64],
+W3[64][64], b3[64], w4[64], b4.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+SIZES = [("W1", (64, 16)), ("b1", (64,)), ("W2", (64, 64)), ("b2", (64,)), ("W3", (64, 64)), ("b3", (64,)),
+         ("w4", (64,)), ("b4", (1,))]
+NUM_PARAMS = sum(int(np.prod(s)) for _, s in SIZES)
+
+
+def unpack(p):
+    out, o = {}, 0
+    for name, shape in SIZES:
+        n = int(np.prod(shape))
+        out[name] = np.asarray(p[o:o + n], np.float64).reshape(shape)
+        o += n
+    return out
+
+
+def pack(d):
+    return np.concatenate([np.asarray(d[name], np.float64).ravel() for name, _ in SIZES])
+
+
+_erf = np.vectorize(math.erf)
+
+
+def gelu(x):
+    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+
+
+def gelu_grad(x):
+    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+
+
+def forward(p, x):
+    P = unpack(p)
+    x = np.asarray(x, np.float64)
+    z1 = x @ P["W1"].T + P["b1"]
+    h1 = gelu(z1)
+    z2 = h1 @ P["W2"].T + P["b2"]
+    h2 = gelu(z2)
+    z3 = h2 @ P["W3"].T + P["b3"]
+    h3 = gelu(z3)
+    y = h3 @ P["w4"] + P["b4"][0]
+    return y, (x, z1, h1, z2, h2, z3, h3)
+
+
+def loss_and_grad(p, x, labels, weights=None):
+    """sum(w * bce(y, label)) / sum(w) and its gradient w.r.t. the parameters."""
+    y, (x, z1, h1, z2, h2, z3, h3) = forward(p, x)
+    lab = np.asarray(labels, np.float64)
+    w = np.ones_like(lab) if weights is None else np.asarray(weights, np.float64)
+    ws = w.sum()
+    loss = float(np.sum(w * (np.maximum(y, 0) - y * lab + np.log1p(np.exp(-np.abs(y))))) / ws)
+    P = unpack(p)
+    dy = w * (1.0 / (1.0 + np.exp(-y)) - lab) / ws
+    g = {"w4": h3.T @ dy, "b4": np.array([dy.sum()])}
+    dz3 = np.outer(dy, P["w4"]) * gelu_grad(z3)
+    g["W3"], g["b3"] = dz3.T @ h2, dz3.sum(0)
+    dz2 = (dz3 @ P["W3"]) * gelu_grad(z2)
+    g["W2"], g["b2"] = dz2.T @ h1, dz2.sum(0)
+    dz1 = (dz2 @ P["W2"]) * gelu_grad(z1)
+    g["W1"], g["b1"] = dz1.T @ x, dz1.sum(0)
+    return loss, pack(g)

@@ -1,0 +1,129 @@
+"""Tensor-core MLP kernels (forward and training gradients) against a torch FP32 reference with the
+kernel's BF16 rounding points, and against the FP64 oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from antiradiancecuts_b200 import _lib as L
+from antiradiancecuts_b200 import api
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(t):
+    import torch
+
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def _torch_forward(p, x):
+    """FP32 reference rounding weights, inputs and the hidden activations to BF16 where the kernel does."""
+    import torch
+
+    P = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in M.unpack(p).items()}
+    gelu = lambda z: 0.5 * z * (1 + torch.erf(z / np.sqrt(2.0)))  # noqa: E731
+    h = _bf16(x)
+    z1 = h @ _bf16(P["W1"]).T + P["b1"]
+    h1 = _bf16(gelu(z1))
+    z2 = h1 @ _bf16(P["W2"]).T + P["b2"]
+    h2 = _bf16(gelu(z2))
+    z3 = h2 @ _bf16(P["W3"]).T + P["b3"]
+    h3 = gelu(z3)
+    return h3 @ P["w4"] + P["b4"][0]
+
+
+@pytest.fixture(scope="module")
+def mlp(ctx):
+    h = C.c_void_p()
+    L.check(ctx.lib.arc_mlp_create(ctx.handle, 7, C.byref(h)), "arc_mlp_create")
+    yield h
+    ctx.lib.arc_mlp_destroy(h)
+
+
+def _params(ctx, h):
+    p = np.zeros(M.NUM_PARAMS, np.float32)
+    L.check(ctx.lib.arc_mlp_get_params(h, p.ctypes.data_as(C.POINTER(C.c_float)), M.NUM_PARAMS), "get")
+    return p
+
+
+@pytest.mark.parametrize("rows", [1, 127, 128, 1000, 70000])
+def test_forward_matches_torch_and_oracle(ctx, mlp, rows):
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(rows)
+    x = torch.randn(rows, 16, device="cuda", generator=g).to(torch.bfloat16).contiguous()
+    out = torch.empty(rows, device="cuda")
+    L.check(ctx.lib.arc_mlp_forward(mlp, C.c_void_p(x.data_ptr()), rows, C.c_void_p(out.data_ptr())), "forward")
+    assert ctx.synchronize() == 0
+    p = _params(ctx, mlp)
+    ref = _torch_forward(p, x.float())
+    err = (out - ref).abs().max().item()
+    assert err <= 2e-3 * max(1.0, ref.abs().max().item()), err
+    if rows <= 1000:
+        y64, _ = M.forward(p.astype(np.float64), x.float().cpu().numpy())
+        assert np.max(np.abs(out.cpu().numpy() - y64)) <= 3e-2 * max(1.0, np.abs(y64).max())
+
+
+def test_gradients_match_torch_and_oracle(ctx, mlp):
+    import torch
+
+    rows = 1000
+    g = torch.Generator(device="cuda").manual_seed(11)
+    x = torch.randn(rows, 16, device="cuda", generator=g).to(torch.bfloat16).contiguous()
+    lab = (torch.rand(rows, device="cuda", generator=g) > 0.5).float()
+    wts = torch.rand(rows, device="cuda", generator=g) + 0.5
+    grads = np.zeros(M.NUM_PARAMS, np.float32)
+    loss = C.c_float()
+    L.check(ctx.lib.arc_mlp_gradients(mlp, C.c_void_p(x.data_ptr()), C.c_void_p(lab.data_ptr()),
+                                      C.c_void_p(wts.data_ptr()), rows, float(wts.sum().item()),
+                                      grads.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)), "gradients")
+    p = _params(ctx, mlp)
+    l64, g64 = M.loss_and_grad(p.astype(np.float64), x.float().cpu().numpy(), lab.cpu().numpy(), wts.cpu().numpy())
+    assert abs(loss.value - l64) <= 1e-2 * abs(l64)
+    # torch autograd with the kernel's rounding points (straight-through in the backward)
+    P = {k: torch.tensor(v, dtype=torch.float32, device="cuda", requires_grad=True) for k, v in M.unpack(p).items()}
+    gelu = lambda z: 0.5 * z * (1 + torch.erf(z / np.sqrt(2.0)))  # noqa: E731
+    st = lambda t: t + (_bf16(t) - t).detach()  # noqa: E731
+    z1 = st(x.float()) @ st(P["W1"]).T + P["b1"]
+    h1 = st(gelu(z1))
+    z2 = h1 @ st(P["W2"]).T + P["b2"]
+    h2 = st(gelu(z2))
+    z3 = h2 @ st(P["W3"]).T + P["b3"]
+    y = gelu(z3) @ P["w4"] + P["b4"][0]
+    ref_loss = (wts * torch.nn.functional.binary_cross_entropy_with_logits(y, lab, reduction="none")).sum() / wts.sum()
+    ref_loss.backward()
+    gt = np.concatenate([P[k].grad.detach().cpu().numpy().ravel() for k, _ in M.SIZES])
+    for ref, tol in ((gt, 0.03), (g64, 0.05)):
+        rel = np.linalg.norm(grads - ref) / np.linalg.norm(ref)
+        assert rel < tol, rel
+        cos = grads @ ref / (np.linalg.norm(grads) * np.linalg.norm(ref))
+        assert cos > 0.998
+
+
+def test_training_learns_a_separable_rule(ctx):
+    import torch
+
+    h = C.c_void_p()
+    L.check(ctx.lib.arc_mlp_create(ctx.handle, 1, C.byref(h)), "create")
+    g = torch.Generator(device="cuda").manual_seed(5)
+    n = 65536
+    x = torch.randn(n, 16, device="cuda", generator=g)
+    lab = ((x[:, 0] + 0.5 * x[:, 1] - 0.25 * x[:, 2]) > 0.1).float()
+    xb = x.to(torch.bfloat16).contiguous()
+    losses = []
+    for step in range(300):
+        i = (step * 4096) % n
+        acc = torch.zeros(1, device="cuda")
+        L.check(ctx.lib.arc_mlp_train_step(h, C.c_void_p(xb[i:i + 4096].data_ptr()), C.c_void_p(lab[i:i + 4096].data_ptr()),
+                                           None, 4096, 4096.0, 3e-3, C.c_void_p(acc.data_ptr())), "train")
+        losses.append(acc)
+    out = torch.empty(n, device="cuda")
+    L.check(ctx.lib.arc_mlp_forward(h, C.c_void_p(xb.data_ptr()), n, C.c_void_p(out.data_ptr())), "forward")
+    assert ctx.synchronize() == 0
+    acc = ((out > 0).float() == lab).float().mean().item()
+    first = sum(l.item() for l in losses[:10]) / 10
+    last = sum(l.item() for l in losses[-10:]) / 10
+    ctx.lib.arc_mlp_destroy(h)
+    assert last < 0.3 * first and acc > 0.97, (first, last, acc)
