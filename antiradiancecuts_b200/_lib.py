@@ -180,6 +180,8 @@ SIGNATURES = {
     "arc_mlp_forward": (_st, [_vp, _vp, C.c_int64, _vp]),
     "arc_mlp_gradients": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, P(C.c_float), P(C.c_float)]),
     "arc_mlp_train_step": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float, _vp]),
+    "arc_cut_training_samples": (_st, [_vp, _vp, P(ArcGBufferView), ArcFloat3, P(ArcGatherParams), P(ArcCutParams),
+                                       C.c_float, _vp, _vp, _vp, C.c_int32, P(C.c_int32)]),
     "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),
                       P(ArcOutputView)]),
     "arc_scene_preset_desc": (_st, [C.c_int32, C.c_uint64, C.c_int32, P(ArcSceneDesc)]),

@@ -596,6 +596,36 @@ __global__ void combine_kernel(const double* rad64, const double* ar64, int widt
 
 }  // namespace
 
+arc_status launch_tile_setup(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gb, const ArcGatherParams* gp,
+                             const ArcCutParams* cp, float4** info_out) {
+    const int W = gb->width, H = gb->height;
+    const int tiles_x = (W + kTile - 1) / kTile, tiles_y = (H + kTile - 1) / kTile, tiles = tiles_x * tiles_y;
+    float4* info = nullptr;
+    ARC_TRY(ctx->arena.get("tile_info", (size_t)tiles * 4 * sizeof(float4), reinterpret_cast<void**>(&info)));
+    TileArgs ta;
+    ta.gpos = reinterpret_cast<const float4*>(gb->position);
+    ta.gnrm = reinterpret_cast<const float4*>(gb->normal);
+    ta.gpitch = gb->pitch;
+    ta.width = W;
+    ta.height = H;
+    ta.mats = ctx->d_materials;
+    ta.num_mats = ctx->num_materials;
+    ta.n = bvh->n;
+    ta.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
+    ta.records = reinterpret_cast<const float4*>(bvh->view.records);
+    ta.eps_bound = cp->error_bound;
+    ta.clamp2 = gp->dist_clamp > 0.0f ? gp->dist_clamp * gp->dist_clamp : 0.0f;
+    ta.tiles_x = tiles_x;
+    ta.tiles_y = tiles_y;
+    ta.info = info;
+    stage_begin(ctx, "cut_setup");
+    cut_tile_setup<<<(tiles + kSelWarps - 1) / kSelWarps, 32 * kSelWarps, 0, ctx->stream>>>(ta);
+    stage_end(ctx, 1);
+    ARC_TRY_CUDA(cudaGetLastError());
+    *info_out = info;
+    return ARC_OK;
+}
+
 arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsGpuParam* avpls,
                              const ArcGBufferView* gb, float3 cam, const ArcGatherParams* gp, const ArcCutParams* cp,
                              const ArcOutputView* out) {
@@ -663,8 +693,6 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     pool.max_chunks = (max_cut + kChunkSize - 1) / kChunkSize;
     const int64_t pool_entries = cp->cut_pool_entries > 0 ? cp->cut_pool_entries : (int64_t)tiles * 65536;
     pool.num_chunks = (int32_t)std::min<int64_t>((pool_entries + kChunkSize - 1) / kChunkSize, INT32_MAX / kChunkSize);
-    float4* info = nullptr;
-    ARC_TRY(ctx->arena.get("tile_info", (size_t)tiles * 4 * sizeof(float4), reinterpret_cast<void**>(&info)));
     ARC_TRY(ctx->arena.get("cut_pool", (size_t)pool.num_chunks * kChunkSize * sizeof(int32_t),
                            reinterpret_cast<void**>(&pool.entries)));
     ARC_TRY(ctx->arena.get("cut_tables", (size_t)tiles * pool.max_chunks * sizeof(int32_t),
@@ -672,26 +700,13 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ARC_TRY(ctx->arena.get("cut_counts", (size_t)tiles * sizeof(int32_t), reinterpret_cast<void**>(&pool.counts)));
     ARC_TRY(ctx->arena.get("cut_pool_next", sizeof(int32_t), reinterpret_cast<void**>(&pool.next)));
     ARC_TRY_CUDA(cudaMemsetAsync(pool.next, 0, sizeof(int32_t), st));
+    float4* info = nullptr;
+    ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info));
     TileArgs ta;
     ta.gpos = reinterpret_cast<const float4*>(gb->position);
     ta.gnrm = reinterpret_cast<const float4*>(gb->normal);
-    ta.gpitch = gb->pitch;
-    ta.width = W;
-    ta.height = H;
-    ta.mats = ctx->d_materials;
-    ta.num_mats = ctx->num_materials;
-    ta.n = bvh->n;
     ta.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
     ta.records = reinterpret_cast<const float4*>(bvh->view.records);
-    ta.eps_bound = cp->error_bound;
-    ta.clamp2 = clamp2;
-    ta.tiles_x = tiles_x;
-    ta.tiles_y = tiles_y;
-    ta.info = info;
-    stage_begin(ctx, "cut_setup");
-    cut_tile_setup<<<(tiles + kSelWarps - 1) / kSelWarps, 32 * kSelWarps, 0, st>>>(ta);
-    stage_end(ctx, 1);
-    ARC_TRY_CUDA(cudaGetLastError());
 
     if (cp->kind == ARC_CUT_ERROR_BOUND) {
         SelArgs sa;

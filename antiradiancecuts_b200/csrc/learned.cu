@@ -1,12 +1,668 @@
-// Learned cut selection (placeholder until the MLP kernels land).
+// Learned cut selection and its training data.
+//
+// Selection (ARC_CUT_LEARNED): a level-synchronous walk over all tiles at once.  Level l holds
+// the (tile, node) pairs at depth l.  For each pair, learned_level:
+//   * accepts leaves, and inner nodes whose analytic bound is already within the tile's threshold
+//     (the learned cut is never finer than the analytic one);
+//   * otherwise writes the pair's 16 features (BF16) as one row for the MLP.
+// The tensor-core MLP (mlp.cu) scores every row of the level in one launch, and learned_expand
+// refines the rows whose logit reaches the threshold (children go to level l + 1) and accepts the
+// rest.  Accepted pairs are finally grouped by tile into the chunked cut pool (count, scan,
+// scatter), which the shared cut evaluation reads.
+//
+// Training data (arc_cut_training_samples): for a batch of tiles, label_prefix computes, per
+// pixel, the FP64 prefix sums over the sorted leaves of the luminance of each leaf's signed
+// contribution; a node's exact contribution is then a difference of two prefixes (its leaves form
+// one contiguous range).  label_traverse walks each tile's tree with the exact decision: refine iff
+// max over the tile's pixels |exact - node estimate| > delta * mean |exact tile value|, and emits
+// (features, label, error) for every visited node the analytic bound cannot accept (plus one level
+// below accepted nodes, so the model also sees the children it would skip).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
 #include "arc_internal.h"
+#include "cut_bounds.cuh"
+#include "device_common.cuh"
+#include "pair_math.cuh"
 
 namespace arc {
 
-arc_status launch_cut_select_learned(arc_context*, const arc_lbvh*, const ArcGatherParams*, const ArcCutParams*,
-                                     const float4*, int, int, const CutPool&) {
-    set_last_error("learned cut not available");
-    return ARC_ERR_UNSUPPORTED;
+const float* mlp_params(const arc_mlp* m);
+arc_status mlp_forward_device(arc_mlp* m, const void* x, int64_t rows, float* logits);
+
+namespace {
+
+constexpr int kTile = 8;
+constexpr int kFeat = 16;
+constexpr int kChunk = 1024;
+
+__device__ __forceinline__ TileInfo load_tile_info(const float4* info, int tile, float* mean) {
+    const float4 i0 = info[4 * (size_t)tile], i1 = info[4 * (size_t)tile + 1], i2 = info[4 * (size_t)tile + 2],
+                 i3 = info[4 * (size_t)tile + 3];
+    TileInfo t;
+    t.tmin[0] = i0.x; t.tmin[1] = i0.y; t.tmin[2] = i0.z; t.kdl = i0.w;
+    t.tmax[0] = i1.x; t.tmax[1] = i1.y; t.tmax[2] = i1.z; t.tau = i1.w;
+    t.ncone = i2;
+    t.valid = __float_as_int(i3.x);
+    *mean = i3.y;
+    return t;
+}
+
+__device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+
+__device__ __forceinline__ float safe_log2(float v) { return log2f(fmaxf(v, 1e-30f)); }
+
+// The 16 features of (tile, inner node).  Every input is known at selection time: the tile's
+// geometry and coarse estimate (mean), the node's bounds / cones / record, its depth, and the
+// analytic bound M against tau.
+__device__ __forceinline__ void node_features(const TileInfo& t, float mean, const NodeGeom& g, float M, float4 nc,
+                                              float4 wc, float4 q0, float4 q1, float4 q2, float4 q3, int depth,
+                                              float* f) {
+    const float E = fmaxf(mean, 1e-30f);
+    const float Ls = lum3(q2.y, q2.z, q2.w), As = lum3(q3.x, q3.y, q3.z);
+    const float inv_dc = 1.0f / fmaxf(g.dc, 1e-6f);
+    const float rt = g.rs - g.rn;
+    // representative's radiance at the tile centre, facing the tile normal-cone axis
+    const float cx = 0.5f * (t.tmin[0] + t.tmax[0]), cy = 0.5f * (t.tmin[1] + t.tmax[1]),
+                cz = 0.5f * (t.tmin[2] + t.tmax[2]);
+    const float dx = q0.x - cx, dy = q0.y - cy, dz = q0.z - cz;
+    const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
+    const float r = rsqrtf(l2);
+    const float c1 = fmaxf(0.0f, (t.ncone.x * dx + t.ncone.y * dy + t.ncone.z * dz) * r);
+    const float c2 = fmaxf(0.0f, -(q0.w * dx + q1.x * dy + q1.y * dz) * r);
+    const float grep = c1 * c2 / fmaxf(l2, 1e-4f);
+    f[0] = clampf((M > 0.0f ? safe_log2(M / fmaxf(t.tau, 1e-30f)) : -32.0f) * 0.125f, -4.0f, 4.0f);
+    f[1] = clampf(safe_log2(Ls * t.kdl / E) * 0.125f, -4.0f, 4.0f);
+    f[2] = clampf(safe_log2(As * t.kdl / E + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[3] = clampf(g.rn * inv_dc, 0.0f, 4.0f);
+    f[4] = clampf(rt * inv_dc, 0.0f, 4.0f);
+    f[5] = clampf(sqrtf(g.d2c) * inv_dc, 0.0f, 4.0f);
+    f[6] = g.cos1;
+    f[7] = g.cos2;
+    f[8] = g.ar_ok == 1.0f ? 1.0f : 0.0f;
+    f[9] = g.ar_ok > 0.0f ? 1.0f : 0.0f;
+    f[10] = nc.w;
+    f[11] = wc.w;
+    f[12] = t.ncone.w;
+    f[13] = log2f(fmaxf(q3.w, 1.0f)) * 0.05f;
+    f[14] = depth * (1.0f / 32.0f);
+    f[15] = clampf(safe_log2(Ls * t.kdl * grep / E + 1e-20f) * 0.125f, -4.0f, 4.0f);
+}
+
+__device__ __forceinline__ void store_features(__nv_bfloat16* row, const float* f) {
+    uint4 q0, q1;
+    uint32_t* u0 = reinterpret_cast<uint32_t*>(&q0);
+    uint32_t* u1 = reinterpret_cast<uint32_t*>(&q1);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+        const __nv_bfloat162 b = __floats2bfloat162_rn(f[8 + 2 * i], f[8 + 2 * i + 1]);
+        u0[i] = *reinterpret_cast<const uint32_t*>(&a);
+        u1[i] = *reinterpret_cast<const uint32_t*>(&b);
+    }
+    reinterpret_cast<uint4*>(row)[0] = q0;
+    reinterpret_cast<uint4*>(row)[1] = q1;
+}
+
+__device__ __forceinline__ int child_index(int c, int n) { return c >= 0 ? c : n - (c + 1); }
+
+// ---------------------------------------------------------------------------------------
+// learned selection
+// ---------------------------------------------------------------------------------------
+struct LevelArgs {
+    int n;
+    const float4* bounds;
+    const float4* records;
+    const float4* info;
+    BoundParams bp;
+    const int4* in;         // {tile, node, depth, 0}
+    const int* in_count;
+    int4* out;              // next level
+    int* out_count;
+    int capacity;           // entries per frontier / row buffer
+    __nv_bfloat16* feats;   // [capacity][16]
+    int* row_entry;         // row -> index into `in`
+    int* row_count;
+    int2* accepted;         // {tile, node}
+    int* acc_count;
+    int acc_capacity;
+    int* tile_counts;
+    uint32_t* err;
+};
+
+__device__ __forceinline__ void accept_pair(const LevelArgs& a, int tile, int node) {
+    const int pos = atomicAdd(a.acc_count, 1);
+    if (pos < a.acc_capacity) {
+        a.accepted[pos] = make_int2(tile, node);
+        atomicAdd(&a.tile_counts[tile], 1);
+    } else {
+        set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
+    }
+}
+
+__device__ __forceinline__ void push_children(const LevelArgs& a, int tile, int k, int depth, float4 b0, float4 b1) {
+    const int pos = atomicAdd(a.out_count, 2);
+    if (pos + 1 < a.capacity) {
+        a.out[pos] = make_int4(tile, child_index(__float_as_int(b0.w), a.n), depth + 1, 0);
+        a.out[pos + 1] = make_int4(tile, child_index(__float_as_int(b1.w), a.n), depth + 1, 0);
+    } else {
+        set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
+    }
+}
+
+__global__ void __launch_bounds__(256) learned_level(LevelArgs a) {
+    const int count = min(*a.in_count, a.capacity);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const int4 en = a.in[e];
+        const int tile = en.x, node = en.y, depth = en.z;
+        if (node < a.n) {
+            accept_pair(a, tile, node);
+            continue;
+        }
+        const int k = node - a.n;
+        float mean;
+        const TileInfo t = load_tile_info(a.info, tile, &mean);
+        const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
+        const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
+        const float4 q0 = a.records[4 * (size_t)node], q1 = a.records[4 * (size_t)node + 1];
+        const float4 q2 = a.records[4 * (size_t)node + 2], q3 = a.records[4 * (size_t)node + 3];
+        const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
+        const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
+        if (!(M > t.tau)) {
+            accept_pair(a, tile, node);
+            continue;
+        }
+        const int r = atomicAdd(a.row_count, 1);
+        if (r >= a.capacity) {  // no room to score it: refine, the safe choice
+            set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
+            push_children(a, tile, k, depth, b0, b1);
+            continue;
+        }
+        float f[kFeat];
+        node_features(t, mean, g, M, nc, wc, q0, q1, q2, q3, depth, f);
+        store_features(a.feats + (size_t)r * kFeat, f);
+        a.row_entry[r] = e;
+    }
+}
+
+__global__ void __launch_bounds__(256) learned_expand(LevelArgs a, const float* logits, float thr_logit) {
+    const int rows = min(*a.row_count, a.capacity);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        const int4 en = a.in[a.row_entry[r]];
+        const int k = en.y - a.n;
+        if (logits[r] >= thr_logit) {
+            push_children(a, en.x, k, en.z, a.bounds[4 * (size_t)k], a.bounds[4 * (size_t)k + 1]);
+        } else {
+            accept_pair(a, en.x, en.y);
+        }
+    }
+}
+
+__global__ void init_frontier(int4* fr, int* count, const float4* info, int tiles, int root) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tiles) return;
+    if (__float_as_int(info[4 * (size_t)t + 3].x) == 0) return;  // no valid pixel
+    const int pos = atomicAdd(count, 1);
+    fr[pos] = make_int4(t, root, 0, 0);
+}
+
+// exclusive scan of per-tile chunk counts (single block) -> chunk base per tile, total chunks
+__global__ void tile_chunk_scan(const int* counts, int tiles, int* base, int* total, int max_chunks, uint32_t* err) {
+    __shared__ int carry;
+    __shared__ int warp_sums[32];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int start = 0; start < tiles; start += blockDim.x) {
+        const int t = start + threadIdx.x;
+        int c = 0;
+        if (t < tiles) {
+            c = (counts[t] + kChunk - 1) / kChunk;
+            if (c > max_chunks) {
+                set_error(err, ARC_DEVERR_CUT_OVERFLOW);
+                c = max_chunks;
+            }
+        }
+        // block exclusive scan
+        int v = c;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        if (lane == 31) warp_sums[w] = v;
+        __syncthreads();
+        if (w == 0) {
+            int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += u;
+            }
+            warp_sums[lane] = s;
+        }
+        __syncthreads();
+        const int excl = carry + (w > 0 ? warp_sums[w - 1] : 0) + v - c;
+        if (t < tiles) base[t] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + c;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+struct ScatterArgs {
+    const int2* accepted;
+    const int* acc_count;
+    int acc_capacity;
+    const int* tile_counts;
+    const int* chunk_base;
+    int* fill;
+    CutPool pool;
+    const int* total_chunks;
+    uint32_t* err;
+};
+
+__global__ void scatter_tables(ScatterArgs s, int tiles) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tiles) return;
+    const int total = *s.total_chunks;
+    int c = (s.tile_counts[t] + kChunk - 1) / kChunk;
+    c = min(c, s.pool.max_chunks);
+    int cnt = min(s.tile_counts[t], c * kChunk);
+    for (int j = 0; j < c; ++j) {
+        const int id = s.chunk_base[t] + j;
+        if (id < s.pool.num_chunks && id < total) s.pool.tables[(size_t)t * s.pool.max_chunks + j] = id;
+        if (id >= s.pool.num_chunks) {
+            set_error(s.err, ARC_DEVERR_CUT_OVERFLOW);
+            cnt = min(cnt, j * kChunk);
+        }
+    }
+    s.pool.counts[t] = cnt;
+}
+
+__global__ void scatter_nodes(ScatterArgs s) {
+    const int count = min(*s.acc_count, s.acc_capacity);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const int2 p = s.accepted[e];
+        const int pos = atomicAdd(&s.fill[p.x], 1);
+        const int id = s.chunk_base[p.x] + pos / kChunk;
+        if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p.x])
+            s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p.y;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// training samples
+// ---------------------------------------------------------------------------------------
+struct LabelArgs {
+    const float4* gpos;
+    const float4* gnrm;
+    int64_t gpitch;
+    int width, height;
+    const MaterialRecord* mats;
+    int num_mats;
+    int n;
+    const float4* bounds;
+    const float4* records;
+    const float4* info;
+    BoundParams bp;
+    PairConsts pc;
+    float disk_scale;
+    int ar_kind;
+    int tiles_x;
+    int tile0, batch;
+    double* prefix;  // [batch][n + 1][64]
+    float delta;
+    __nv_bfloat16* feats;
+    float* labels;
+    float* errs;
+    int* count;
+    int capacity;
+    uint32_t* err;
+};
+
+__device__ __forceinline__ void pixel_of(const LabelArgs& a, int tile, int p, int& x, int& y) {
+    x = (tile % a.tiles_x) * kTile + p % kTile;
+    y = (tile / a.tiles_x) * kTile + p / kTile;
+}
+
+// luminance of one record's signed contribution at a pixel (receiver albedo applied)
+template <int AR>
+__device__ __forceinline__ float record_lum(const float4* rec, const Pixel<float>& px, const float* kd,
+                                            const PairConsts& pc, float disk_scale) {
+    float4 q3 = rec[3];
+    if (AR == ARC_AR_DISK) {
+        const float ww = rec[1].z * rec[1].z + rec[1].w * rec[1].w + rec[2].x * rec[2].x;
+        q3.w = ww > 0.0f ? rsqrtf(ww) : 0.0f;
+    }
+    float g, ga;
+    pair_terms<AR, float>(rec[0], rec[1], rec[2], q3, px, pc, g, ga);
+    const float as = AR == ARC_AR_DISK ? disk_scale : 1.0f;
+    const float c0 = kd[0] * (rec[2].y * g - as * q3.x * ga), c1 = kd[1] * (rec[2].z * g - as * q3.y * ga),
+                c2 = kd[2] * (rec[2].w * g - as * q3.z * ga);
+    return 0.2126f * c0 + 0.7152f * c1 + 0.0722f * c2;
+}
+
+__device__ __forceinline__ bool load_pixel(const LabelArgs& a, int tile, int p, Pixel<float>& px, float* kd) {
+    int x, y;
+    pixel_of(a, tile, p, x, y);
+    px.px = px.py = px.pz = px.nx = px.ny = px.nz = 0.0f;
+    kd[0] = kd[1] = kd[2] = 0.0f;
+    if (x >= a.width || y >= a.height) return false;
+    const float4 gp = a.gpos[(int64_t)y * a.gpitch + x], gn = a.gnrm[(int64_t)y * a.gpitch + x];
+    const int m = (int)gn.w;
+    if (m <= 0 || m >= a.num_mats) return false;
+    const float l = rsqrtf(gn.x * gn.x + gn.y * gn.y + gn.z * gn.z);
+    px.px = gp.x;
+    px.py = gp.y;
+    px.pz = gp.z;
+    px.nx = gn.x * l;
+    px.ny = gn.y * l;
+    px.nz = gn.z * l;
+    const float4 d = a.mats[m].diffuse_exp;
+    kd[0] = kOneOverPi * d.x;
+    kd[1] = kOneOverPi * d.y;
+    kd[2] = kOneOverPi * d.z;
+    return true;
+}
+
+template <int AR>
+__global__ void __launch_bounds__(64) label_prefix(LabelArgs a) {
+    const int b = blockIdx.x, p = threadIdx.x;
+    const int tile = a.tile0 + b;
+    Pixel<float> px;
+    float kd[3];
+    const bool valid = load_pixel(a, tile, p, px, kd);
+    double* P = a.prefix + (size_t)b * (a.n + 1) * 64;
+    double run = 0.0;
+    P[p] = 0.0;
+    for (int i = 0; i < a.n; ++i) {
+        if (valid) run += (double)record_lum<AR>(a.records + 4 * (size_t)i, px, kd, a.pc, a.disk_scale);
+        P[(size_t)(i + 1) * 64 + p] = run;
+    }
+}
+
+template <int AR>
+__global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ranges) {
+    const int b = blockIdx.x, lane = threadIdx.x;
+    const int tile = a.tile0 + b;
+    float mean;
+    const TileInfo t = load_tile_info(a.info, tile, &mean);
+    if (t.valid == 0) return;
+    const double* P = a.prefix + (size_t)b * (a.n + 1) * 64;
+    Pixel<float> px[2];
+    float kd[2][3];
+    bool valid[2];
+    for (int h = 0; h < 2; ++h) valid[h] = load_pixel(a, tile, lane + 32 * h, px[h], kd[h]);
+    // exact tile scale: mean |T_p| over the valid pixels
+    float s = 0.0f, nv = 0.0f;
+    for (int h = 0; h < 2; ++h)
+        if (valid[h]) {
+            s += fabsf((float)P[(size_t)a.n * 64 + lane + 32 * h]);
+            nv += 1.0f;
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        nv += __shfl_xor_sync(0xffffffffu, nv, o);
+    }
+    const float Eexact = nv > 0.0f ? s / nv : 0.0f;
+    const float thr = a.delta * Eexact;
+    // DFS with one node per step: stack entries node | (depth << 24) with bit 31 = "extra"
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = a.n;
+    int budget = 4 * a.n;
+    while (sp > 0 && --budget > 0) {
+        const int e = stack[--sp];
+        const bool extra = e < 0;
+        const int node = (e & 0x7fffffff) & 0x00ffffff;
+        const int depth = ((e & 0x7fffffff) >> 24) & 0x7f;
+        if (node < a.n) continue;
+        const int k = node - a.n;
+        const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
+        const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
+        const float4* rec = a.records + 4 * (size_t)node;
+        const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+        const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
+        const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
+        if (!(M > t.tau)) continue;  // the analytic bound accepts it: no decision to learn
+        const int f0 = ranges[2 * k], l0 = ranges[2 * k + 1];
+        float emax = 0.0f;
+        for (int h = 0; h < 2; ++h) {
+            if (!valid[h]) continue;
+            const int p = lane + 32 * h;
+            const float exact = (float)(P[(size_t)(l0 + 1) * 64 + p] - P[(size_t)f0 * 64 + p]);
+            const float approx = record_lum<AR>(rec, px[h], kd[h], a.pc, a.disk_scale);
+            emax = fmaxf(emax, fabsf(exact - approx));
+        }
+        for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        const bool refine = emax > thr;
+        if (lane == 0) {
+            const int r = atomicAdd(a.count, 1);
+            if (r < a.capacity) {
+                float f[kFeat];
+                node_features(t, mean, g, M, nc, wc, q0, q1, q2, q3, depth, f);
+                store_features(a.feats + (size_t)r * kFeat, f);
+                a.labels[r] = refine ? 1.0f : 0.0f;
+                a.errs[r] = Eexact > 0.0f ? emax / Eexact : 0.0f;
+            }
+        }
+        if (extra) continue;
+        if (sp + 2 > 128) {
+            set_error(a.err, ARC_DEVERR_STACK_OVERFLOW);
+            break;
+        }
+        const int c0 = child_index(__float_as_int(b0.w), a.n), c1 = child_index(__float_as_int(b1.w), a.n);
+        const int d1 = min(depth + 1, 127) << 24;
+        const int flag = refine ? 0 : (int)0x80000000;  // below an accepted node: one level only
+        stack[sp++] = (c1 | d1) | flag;
+        stack[sp++] = (c0 | d1) | flag;
+    }
+}
+
+template <typename T>
+arc_status arena_get(arc_context* ctx, const char* name, size_t count, T** out) {
+    return ctx->arena.get(name, sizeof(T) * (count > 0 ? count : 1), reinterpret_cast<void**>(out));
+}
+
+BoundParams bound_params(const ArcGatherParams* gp, const ArcCutParams* cp) {
+    BoundParams bp;
+    bp.clamp2 = gp->dist_clamp > 0.0f ? gp->dist_clamp * gp->dist_clamp : 0.0f;
+    bp.ar_kind = gp->ar_kind;
+    bp.eps_cone = 0.001f;
+    bp.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
+    bp.disk_scale = gp->disk_radius > 0.0f ? 1.0f / (kPi * gp->disk_radius * gp->disk_radius) : 0.0f;
+    bp.ar_uncertain = cp->ar_uncertain_factor;
+    return bp;
+}
+
+}  // namespace
+
+arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, const ArcGatherParams* gp,
+                                     const ArcCutParams* cp, const float4* info, int tiles_x, int tiles_y,
+                                     const CutPool& pool) {
+    cudaStream_t st = ctx->stream;
+    const int tiles = tiles_x * tiles_y;
+    const int n = bvh->n;
+    // capacities: frontier / rows per level and accepted pairs over the whole walk
+    const int cap = (int)std::min<int64_t>((int64_t)tiles * 2048 + 1024, 1 << 30);
+    const int acc_cap = (int)std::min<int64_t>((int64_t)pool.num_chunks * kChunk, (int64_t)INT32_MAX);
+    int4 *fa, *fb;
+    int2* accepted;
+    __nv_bfloat16* feats;
+    int *row_entry, *counters, *tile_counts, *chunk_base, *fill;
+    float* logits;
+    ARC_TRY(arena_get(ctx, "lc_front_a", cap, &fa));
+    ARC_TRY(arena_get(ctx, "lc_front_b", cap, &fb));
+    ARC_TRY(arena_get(ctx, "lc_feats", (size_t)cap * kFeat, &feats));
+    ARC_TRY(arena_get(ctx, "lc_row_entry", cap, &row_entry));
+    ARC_TRY(arena_get(ctx, "lc_logits", cap, &logits));
+    ARC_TRY(arena_get(ctx, "lc_accepted", acc_cap, &accepted));
+    // counters: [0] in count, [1] out count, [2] rows, [3] accepted, [4] total chunks, then one
+    // (in, out, rows) triple per level
+    constexpr int kMaxLevels = 96;
+    ARC_TRY(arena_get(ctx, "lc_counters", 8 + 4 * kMaxLevels, &counters));
+    ARC_TRY(arena_get(ctx, "lc_tile_counts", tiles, &tile_counts));
+    ARC_TRY(arena_get(ctx, "lc_chunk_base", tiles, &chunk_base));
+    ARC_TRY(arena_get(ctx, "lc_fill", tiles, &fill));
+    ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * (8 + 4 * kMaxLevels), st));
+    ARC_TRY_CUDA(cudaMemsetAsync(tile_counts, 0, sizeof(int) * tiles, st));
+    ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * tiles, st));
+
+    const float p = cp->mlp_threshold;
+    const float thr_logit = p <= 0.0f ? -INFINITY : (p >= 1.0f ? INFINITY : logf(p / (1.0f - p)));
+    LevelArgs la{};
+    la.n = n;
+    la.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
+    la.records = reinterpret_cast<const float4*>(bvh->view.records);
+    la.info = info;
+    la.bp = bound_params(gp, cp);
+    la.capacity = cap;
+    la.feats = feats;
+    la.row_entry = row_entry;
+    la.accepted = accepted;
+    la.acc_count = counters + 3;
+    la.acc_capacity = acc_cap;
+    la.tile_counts = tile_counts;
+    la.err = ctx->d_error;
+
+    stage_begin(ctx, "cut_learned");
+    int kernels = 0;
+    int* in_count = counters + 8;
+    init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, in_count, info, tiles, n);
+    ++kernels;
+    const int grid = ctx->sm_count * 8;
+    int4 *cur = fa, *nxt = fb;
+    for (int level = 0; level < kMaxLevels; ++level) {
+        int host_count = 0;
+        ARC_TRY_CUDA(cudaMemcpyAsync(&host_count, in_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ARC_TRY_CUDA(cudaStreamSynchronize(st));
+        if (host_count == 0) break;
+        int* out_count = counters + 8 + 4 * (level + 1);
+        la.in = cur;
+        la.in_count = in_count;
+        la.out = nxt;
+        la.out_count = out_count;
+        la.row_count = counters + 8 + 4 * level + 2;
+        const int blocks = std::max(1, std::min(grid, (host_count + 255) / 256));
+        learned_level<<<blocks, 256, 0, st>>>(la);
+        ++kernels;
+        int rows = 0;
+        ARC_TRY_CUDA(cudaMemcpyAsync(&rows, la.row_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ARC_TRY_CUDA(cudaStreamSynchronize(st));
+        rows = std::min(rows, cap);
+        if (rows > 0) {
+            ARC_TRY(mlp_forward_device(const_cast<arc_mlp*>(cp->model), feats, rows, logits));
+            ++kernels;
+            learned_expand<<<std::max(1, std::min(grid, (rows + 255) / 256)), 256, 0, st>>>(la, logits, thr_logit);
+            ++kernels;
+        }
+        ARC_TRY_CUDA(cudaGetLastError());
+        in_count = out_count;
+        std::swap(cur, nxt);
+    }
+    ScatterArgs sa;
+    sa.accepted = accepted;
+    sa.acc_count = counters + 3;
+    sa.acc_capacity = acc_cap;
+    sa.tile_counts = tile_counts;
+    sa.chunk_base = chunk_base;
+    sa.fill = fill;
+    sa.pool = pool;
+    sa.total_chunks = counters + 4;
+    sa.err = ctx->d_error;
+    tile_chunk_scan<<<1, 1024, 0, st>>>(tile_counts, tiles, chunk_base, counters + 4, pool.max_chunks, ctx->d_error);
+    scatter_tables<<<(tiles + 255) / 256, 256, 0, st>>>(sa, tiles);
+    scatter_nodes<<<grid, 256, 0, st>>>(sa);
+    kernels += 3;
+    ARC_TRY_CUDA(cudaMemcpyAsync(pool.next, counters + 4, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    stage_end(ctx, kernels);
+    ARC_TRY_CUDA(cudaGetLastError());
+    return ARC_OK;
 }
 
 }  // namespace arc
+
+using namespace arc;
+
+// Training samples of the learned cut (see the file comment).  No counterpart in the reference.
+extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gb,
+                                               ArcFloat3 camera_position, const ArcGatherParams* gp,
+                                               const ArcCutParams* cp, float delta, void* features_bf16,
+                                               float* labels, float* errors, int32_t capacity, int32_t* count) {
+    ARC_CHECK_ARG(ctx && bvh && gb && gp && cp && features_bf16 && labels && errors && count, "NULL argument");
+    ARC_CHECK_ARG(bvh->n >= 2, "LBVH not built");
+    ARC_CHECK_ARG(gp->ar_kind >= 0 && gp->ar_kind <= 2, "ar_kind out of range");
+    (void)camera_position;
+    cudaStream_t st = ctx->stream;
+    const int W = gb->width, H = gb->height;
+    const int tiles_x = (W + kTile - 1) / kTile, tiles = tiles_x * ((H + kTile - 1) / kTile);
+    const int n = bvh->n;
+    float4* info = nullptr;
+    ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info));
+    // batch of tiles whose FP64 prefixes fit in ~4 GB
+    const size_t per_tile = (size_t)(n + 1) * 64 * sizeof(double);
+    const int batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)tiles, ((size_t)4 << 30) / per_tile));
+    double* prefix = nullptr;
+    ARC_TRY(ctx->arena.get("label_prefix", per_tile * batch, reinterpret_cast<void**>(&prefix)));
+    int* dcount = nullptr;
+    ARC_TRY(ctx->arena.get("label_count", sizeof(int), reinterpret_cast<void**>(&dcount)));
+    ARC_TRY_CUDA(cudaMemsetAsync(dcount, 0, sizeof(int), st));
+    LabelArgs a{};
+    a.gpos = reinterpret_cast<const float4*>(gb->position);
+    a.gnrm = reinterpret_cast<const float4*>(gb->normal);
+    a.gpitch = gb->pitch;
+    a.width = W;
+    a.height = H;
+    a.mats = ctx->d_materials;
+    a.num_mats = ctx->num_materials;
+    a.n = n;
+    a.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
+    a.records = reinterpret_cast<const float4*>(bvh->view.records);
+    a.info = info;
+    a.bp = bound_params(gp, cp);
+    a.pc.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
+    a.pc.eps = 0.001f;
+    a.pc.inv_clamp2 = gp->dist_clamp > 0.0f ? 1.0f / (gp->dist_clamp * gp->dist_clamp) : INFINITY;
+    a.pc.disk_r2 = gp->disk_radius * gp->disk_radius;
+    a.disk_scale = gp->disk_radius > 0.0f ? 1.0f / (kPi * gp->disk_radius * gp->disk_radius) : 0.0f;
+    a.ar_kind = gp->ar_kind;
+    a.tiles_x = tiles_x;
+    a.prefix = prefix;
+    a.delta = delta;
+    a.feats = static_cast<__nv_bfloat16*>(features_bf16);
+    a.labels = labels;
+    a.errs = errors;
+    a.count = dcount;
+    a.capacity = capacity;
+    a.err = ctx->d_error;
+    for (int t0 = 0; t0 < tiles; t0 += batch) {
+        a.tile0 = t0;
+        a.batch = std::min(batch, tiles - t0);
+        switch (gp->ar_kind) {
+            case 0:
+                label_prefix<0><<<a.batch, 64, 0, st>>>(a);
+                label_traverse<0><<<a.batch, 32, 0, st>>>(a, bvh->view.range);
+                break;
+            case 1:
+                label_prefix<1><<<a.batch, 64, 0, st>>>(a);
+                label_traverse<1><<<a.batch, 32, 0, st>>>(a, bvh->view.range);
+                break;
+            default:
+                label_prefix<2><<<a.batch, 64, 0, st>>>(a);
+                label_traverse<2><<<a.batch, 32, 0, st>>>(a, bvh->view.range);
+                break;
+        }
+        ARC_TRY_CUDA(cudaGetLastError());
+    }
+    int h = 0;
+    ARC_TRY_CUDA(cudaMemcpyAsync(&h, dcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ARC_TRY_CUDA(cudaStreamSynchronize(st));
+    *count = std::min(h, capacity);
+    return ARC_OK;
+}

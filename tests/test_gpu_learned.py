@@ -1,0 +1,112 @@
+"""Learned cut: the level-synchronous selection, its training samples, and the trained model."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+from antiradiancecuts_b200 import _lib as L
+from antiradiancecuts_b200 import api, learned
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+W, HGT, N = 160, 96, 16384
+
+
+@pytest.fixture(scope="module")
+def scene_(ctx):
+    d = H.workload("boxes2_720p_64k", W, HGT, N)
+    ctx.upload_materials(d["mats"])
+    dv = ctx.upload_avpls(d["avpls"])
+    bvh = api.AvplBvh(ctx)
+    bvh.build(dv)
+    assert ctx.synchronize() == 0
+    return d, dv, bvh, bvh.host_arrays(), api.GBuffer(d["pos"], d["nrm"])
+
+
+def _gather(ctx, d, bvh, gb, cut):
+    prm = api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
+    out = api.Outputs(W, HGT)
+    api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, cut, out)
+    assert ctx.synchronize() == 0
+    return out.result64.cpu().numpy().reshape(-1, 3), api.last_cut(ctx)
+
+
+def test_always_refine_equals_error_bound_cut(ctx, scene_):
+    d, dv, bvh, tree, gb = scene_
+    model = learned.Model(ctx, seed=3)
+    img_b, cuts_b = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01))
+    img_l, cuts_l = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=0.01,
+                                                            model=model.handle.value, mlp_threshold=0.0))
+    assert all(np.array_equal(a, b) for a, b in zip(cuts_b, cuts_l))
+    assert H.rel_rmse(img_l, img_b) < 1e-6
+    model.close()
+
+
+def test_learned_cut_evaluation_matches_oracle(ctx, scene_):
+    d, dv, bvh, tree, gb = scene_
+    model = learned.Model(ctx, seed=4)
+    img, cuts = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=0.01,
+                                                        model=model.handle.value, mlp_threshold=0.5))
+    _, _, ref = O.eval_cut(d["pos"], d["nrm"], tree, cuts, d["dif"], 2, 30.0, 0.01)
+    assert H.rel_rmse(img, ref) < 2e-5
+    # every tile's accepted nodes form a cut: no accepted node is an ancestor of another
+    par = tree["parents"]
+    n = len(tree["morton"])
+    for c in cuts[:: max(1, len(cuts) // 40)]:
+        s = set(int(x) for x in c)
+        for x in c:
+            p = par[x]
+            while p != -1:
+                assert (n + p) not in s
+                p = par[n + p]
+    model.close()
+
+
+def test_training_samples(ctx):
+    f, l, e = learned.scene_samples(ctx, 101, capacity=400000, width=96, height=64, num_avpls=8192, delta=5e-4)
+    assert f.shape[0] > 100
+    fl = f.float()
+    assert bool(torch_isfinite(fl)) and set(np.unique(l.cpu().numpy())) <= {0.0, 1.0}
+    f2, l2, _ = learned.scene_samples(ctx, 101, capacity=400000, width=96, height=64, num_avpls=8192, delta=5e-2)
+    assert l2.mean().item() < l.mean().item()  # a looser bound refines less
+
+
+def torch_isfinite(t):
+    import torch
+
+    return torch.isfinite(t).all().item()
+
+
+@pytest.mark.skipif(not os.path.exists(learned.DEFAULT_MODEL), reason="no trained model")
+def test_trained_model_beats_analytic_cut_on_held_out_scene(ctx):
+    """Ablation: on the held-out variant, the trained network's cut against the analytic error-bound
+    cut, both scored against the exact FP64 image: the learned cut must be smaller at an error no
+    larger than the analytic cut's (or at least as accurate at a no larger size)."""
+    d = H.workload("variant500_1080p_1m", 160, 96, 32768)
+    ctx.upload_materials(d["mats"])
+    dv = ctx.upload_avpls(d["avpls"])
+    bvh = api.AvplBvh(ctx)
+    bvh.build(dv)
+    gb = api.GBuffer(d["pos"], d["nrm"])
+    model = learned.load_default_model(ctx)
+    px = np.arange(160 * 96)
+    _, _, exact = O.gather_fp64(d["pos"], d["nrm"], px, d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"],
+                                O.params(2, 30.0, 0.01))
+    global W, HGT
+    W0, H0 = W, HGT
+    W, HGT = 160, 96
+    try:
+        img_b, cuts_b = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01))
+        img_l, cuts_l = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=0.01,
+                                                                model=model.handle.value))
+    finally:
+        W, HGT = W0, H0
+    eb, el = H.rel_rmse(img_b, exact), H.rel_rmse(img_l, exact)
+    nb, nl = sum(map(len, cuts_b)), sum(map(len, cuts_l))
+    print(f"analytic: {nb} nodes, rel RMSE {eb:.4f}; learned: {nl} nodes, rel RMSE {el:.4f}")
+    assert nl <= nb
+    assert el <= max(2.0 * eb, 0.02)
+    model.close()
