@@ -105,7 +105,7 @@ class ArcLbvhView(C.Structure):
 class ArcCutParams(C.Structure):
     _fields_ = [("kind", C.c_int32), ("solid_angle_threshold", C.c_float), ("error_bound", C.c_float),
                 ("ar_uncertain_factor", C.c_float), ("max_cut_nodes", C.c_int32), ("cut_pool_entries", C.c_int64),
-                ("model", C.c_void_p), ("mlp_threshold", C.c_float),
+                ("model", C.c_void_p), ("mlp_threshold", C.c_float), ("mlp_band", C.c_float),
                 ("debug_pixel_x", C.c_int32), ("debug_pixel_y", C.c_int32), ("used_nodes", C.c_void_p)]
 
 
@@ -153,6 +153,7 @@ SIGNATURES = {
     "arc_context_profile": (_st, [_vp, C.c_int32]),
     "arc_context_stage_times": (_st, [_vp, C.c_char_p, C.c_size_t, P(C.c_float), C.c_int32, P(C.c_int32)]),
     "arc_context_launch_count": (C.c_uint64, [_vp]),
+    "arc_context_learned_rows": (C.c_uint64, [_vp]),
     "arc_measure_fp32_peak": (_st, [_vp, P(C.c_double), P(C.c_double)]),
     "arc_device_alloc": (_st, [_vp, C.c_size_t, P(_vp)]),
     "arc_device_free": (_st, [_vp, _vp]),

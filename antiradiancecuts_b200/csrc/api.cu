@@ -52,14 +52,16 @@ void stage_begin(arc_context* ctx, const char* name) {
     }
     t.names[t.used] = name;
     cudaEventRecord(t.begin[t.used], ctx->stream);
+    t.open.push_back(t.used);
+    ++t.used;
 }
 
 void stage_end(arc_context* ctx, int kernels_launched) {
     ctx->launches += (uint64_t)kernels_launched;
     StageTimer& t = ctx->timer;
-    if (!t.enabled || t.used >= t.begin.size()) return;
-    cudaEventRecord(t.end[t.used], ctx->stream);
-    ++t.used;
+    if (!t.enabled || t.open.empty()) return;
+    cudaEventRecord(t.end[t.open.back()], ctx->stream);
+    t.open.pop_back();
 }
 
 size_t Arena::bytes_held() const {
@@ -143,6 +145,7 @@ void arc_cut_params_default(ArcCutParams* p) {
     p->max_cut_nodes = 1 << 20;
     p->cut_pool_entries = 0;
     p->mlp_threshold = 0.5f;
+    p->mlp_band = 4096.0f;
     p->debug_pixel_x = -1;
     p->debug_pixel_y = -1;
 }
@@ -220,6 +223,7 @@ arc_status arc_context_profile(arc_context* ctx, int32_t enable) {
     ARC_CHECK_ARG(ctx != nullptr, "ctx is NULL");
     ctx->timer.enabled = enable != 0;
     ctx->timer.used = 0;
+    ctx->timer.open.clear();
     return ARC_OK;
 }
 
@@ -240,10 +244,13 @@ arc_status arc_context_stage_times(arc_context* ctx, char* names, size_t names_l
     std::snprintf(names, names_len, "%s", joined.c_str());
     *num_stages = n;
     t.used = 0;
+    t.open.clear();
     return ARC_OK;
 }
 
 uint64_t arc_context_launch_count(arc_context* ctx) { return ctx ? ctx->launches : 0; }
+
+uint64_t arc_context_learned_rows(arc_context* ctx) { return ctx ? ctx->learned_rows : 0; }
 
 arc_status arc_device_alloc(arc_context* ctx, size_t bytes, void** out) {
     ARC_CHECK_ARG(ctx && out, "NULL argument");

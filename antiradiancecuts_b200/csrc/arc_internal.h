@@ -68,6 +68,7 @@ struct StageTimer {
     std::vector<std::string> names;
     std::vector<cudaEvent_t> begin, end;
     size_t used = 0;
+    std::vector<size_t> open;  // stages begun and not yet ended (stages may nest)
 };
 
 // Per-tile cut lists: each tile's nodes live in 1024-entry chunks of one device pool, listed in
@@ -107,6 +108,7 @@ struct arc_context {
     arc_lbvh* run_bvh = nullptr;  // tree rebuilt by arc_run every frame
     arc::StageTimer timer;
     uint64_t launches = 0;  // kernels launched by this context
+    uint64_t learned_rows = 0;  // rows scored by the cut network so far
 };
 
 struct arc_lbvh {

@@ -56,28 +56,52 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fm
 
 __device__ __forceinline__ float safe_log2(float v) { return log2f(fmaxf(v, 1e-30f)); }
 
+// Radiance and antiradiance luminance of one packed record at a point p with unit normal n
+// (receiver albedo folded into kdl by the caller).
+__device__ __forceinline__ void record_at(const float4* rec, float px, float py, float pz, float nx, float ny, float nz,
+                                          float clamp2, float cos_thr, float& rad, float& ar) {
+    const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+    const float dx = q0.x - px, dy = q0.y - py, dz = q0.z - pz;
+    const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
+    const float r = rsqrtf(l2);
+    const float c1 = (nx * dx + ny * dy + nz * dz) * r;
+    const float c2 = -(q0.w * dx + q1.x * dy + q1.y * dz) * r;
+    const float inv = 1.0f / fmaxf(l2, clamp2);
+    rad = lum3(q2.y, q2.z, q2.w) * fmaxf(c1, 0.0f) * fmaxf(c2, 0.0f) * inv;
+    const float cw = -(q1.z * dx + q1.w * dy + q2.x * dz) * r;
+    ar = (cw > cos_thr && c1 > 0.001f) ? lum3(q3.x, q3.y, q3.z) * c1 * inv : 0.0f;
+}
+
 // The 16 features of (tile, inner node).  Every input is known at selection time: the tile's
-// geometry and coarse estimate (mean), the node's bounds / cones / record, its depth, and the
-// analytic bound M against tau.
+// geometry and coarse estimate (mean), the node's bounds / cones / record, the records of its two
+// children (a one-level lookahead at the tile centre), its depth, and the analytic bound M against
+// tau.
 __device__ __forceinline__ void node_features(const TileInfo& t, float mean, const NodeGeom& g, float M, float4 nc,
-                                              float4 wc, float4 q0, float4 q1, float4 q2, float4 q3, int depth,
-                                              float* f) {
+                                              float4 wc, const float4* rec, const float4* rec_l, const float4* rec_r,
+                                              int depth, float clamp2, float cos_thr, float* f) {
     const float E = fmaxf(mean, 1e-30f);
+    const float4 q2 = rec[2], q3 = rec[3];
     const float Ls = lum3(q2.y, q2.z, q2.w), As = lum3(q3.x, q3.y, q3.z);
     const float inv_dc = 1.0f / fmaxf(g.dc, 1e-6f);
     const float rt = g.rs - g.rn;
-    // representative's radiance at the tile centre, facing the tile normal-cone axis
     const float cx = 0.5f * (t.tmin[0] + t.tmax[0]), cy = 0.5f * (t.tmin[1] + t.tmax[1]),
                 cz = 0.5f * (t.tmin[2] + t.tmax[2]);
-    const float dx = q0.x - cx, dy = q0.y - cy, dz = q0.z - cz;
-    const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
-    const float r = rsqrtf(l2);
-    const float c1 = fmaxf(0.0f, (t.ncone.x * dx + t.ncone.y * dy + t.ncone.z * dz) * r);
-    const float c2 = fmaxf(0.0f, -(q0.w * dx + q1.x * dy + q1.y * dz) * r);
-    const float grep = c1 * c2 / fmaxf(l2, 1e-4f);
+    float nx = t.ncone.x, ny = t.ncone.y, nz = t.ncone.z;
+    const float nl = nx * nx + ny * ny + nz * nz;
+    if (nl > 0.0f) {
+        const float s = rsqrtf(nl);
+        nx *= s;
+        ny *= s;
+        nz *= s;
+    }
+    float rad, ar, radl, arl, radr, arr;
+    record_at(rec, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, rad, ar);
+    record_at(rec_l, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radl, arl);
+    record_at(rec_r, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radr, arr);
+    const float s = t.kdl / E;
     f[0] = clampf((M > 0.0f ? safe_log2(M / fmaxf(t.tau, 1e-30f)) : -32.0f) * 0.125f, -4.0f, 4.0f);
-    f[1] = clampf(safe_log2(Ls * t.kdl / E) * 0.125f, -4.0f, 4.0f);
-    f[2] = clampf(safe_log2(As * t.kdl / E + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[1] = clampf(safe_log2(Ls * s) * 0.125f, -4.0f, 4.0f);
+    f[2] = clampf(safe_log2(As * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
     f[3] = clampf(g.rn * inv_dc, 0.0f, 4.0f);
     f[4] = clampf(rt * inv_dc, 0.0f, 4.0f);
     f[5] = clampf(sqrtf(g.d2c) * inv_dc, 0.0f, 4.0f);
@@ -87,10 +111,10 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
     f[9] = g.ar_ok > 0.0f ? 1.0f : 0.0f;
     f[10] = nc.w;
     f[11] = wc.w;
-    f[12] = t.ncone.w;
-    f[13] = log2f(fmaxf(q3.w, 1.0f)) * 0.05f;
+    f[12] = clampf(safe_log2(fabsf(rad - radl - radr) * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[13] = clampf(safe_log2(fabsf(ar - arl - arr) * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
     f[14] = depth * (1.0f / 32.0f);
-    f[15] = clampf(safe_log2(Ls * t.kdl * grep / E + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[15] = clampf(safe_log2(rad * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
 }
 
 __device__ __forceinline__ void store_features(__nv_bfloat16* row, const float* f) {
@@ -119,9 +143,9 @@ struct LevelArgs {
     const float4* records;
     const float4* info;
     BoundParams bp;
-    const int4* in;         // {tile, node, depth, 0}
+    const int2* in;         // {tile, node | depth << 26}
     const int* in_count;
-    int4* out;              // next level
+    int2* out;              // next level
     int* out_count;
     int capacity;           // entries per frontier / row buffer
     __nv_bfloat16* feats;   // [capacity][16]
@@ -131,6 +155,9 @@ struct LevelArgs {
     int* acc_count;
     int acc_capacity;
     int* tile_counts;
+    float band;             // M > band * tau: refine without the network
+    float clamp2, cos_thr;
+    int begin, end;         // entries of `in` handled by this launch
     uint32_t* err;
 };
 
@@ -144,21 +171,27 @@ __device__ __forceinline__ void accept_pair(const LevelArgs& a, int tile, int no
     }
 }
 
+constexpr int kDepthShift = 26;  // node ids < 2^26 (trees of up to 32M leaves), depth < 32
+
+__device__ __forceinline__ int2 entry(int tile, int node, int depth) {
+    return make_int2(tile, node | (min(depth, 31) << kDepthShift));
+}
+
 __device__ __forceinline__ void push_children(const LevelArgs& a, int tile, int k, int depth, float4 b0, float4 b1) {
     const int pos = atomicAdd(a.out_count, 2);
     if (pos + 1 < a.capacity) {
-        a.out[pos] = make_int4(tile, child_index(__float_as_int(b0.w), a.n), depth + 1, 0);
-        a.out[pos + 1] = make_int4(tile, child_index(__float_as_int(b1.w), a.n), depth + 1, 0);
+        a.out[pos] = entry(tile, child_index(__float_as_int(b0.w), a.n), depth + 1);
+        a.out[pos + 1] = entry(tile, child_index(__float_as_int(b1.w), a.n), depth + 1);
     } else {
         set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
     }
 }
 
 __global__ void __launch_bounds__(256) learned_level(LevelArgs a) {
-    const int count = min(*a.in_count, a.capacity);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
-        const int4 en = a.in[e];
-        const int tile = en.x, node = en.y, depth = en.z;
+    const int count = min(min(*a.in_count, a.capacity), a.end);
+    for (int e = a.begin + blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const int2 en = a.in[e];
+        const int tile = en.x, node = en.y & ((1 << kDepthShift) - 1), depth = en.y >> kDepthShift;
         if (node < a.n) {
             accept_pair(a, tile, node);
             continue;
@@ -168,12 +201,15 @@ __global__ void __launch_bounds__(256) learned_level(LevelArgs a) {
         const TileInfo t = load_tile_info(a.info, tile, &mean);
         const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
         const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
-        const float4 q0 = a.records[4 * (size_t)node], q1 = a.records[4 * (size_t)node + 1];
         const float4 q2 = a.records[4 * (size_t)node + 2], q3 = a.records[4 * (size_t)node + 3];
         const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
         const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
         if (!(M > t.tau)) {
             accept_pair(a, tile, node);
+            continue;
+        }
+        if (M > a.band * t.tau) {  // far outside the network's band: refine
+            push_children(a, tile, k, depth, b0, b1);
             continue;
         }
         const int r = atomicAdd(a.row_count, 1);
@@ -183,31 +219,34 @@ __global__ void __launch_bounds__(256) learned_level(LevelArgs a) {
             continue;
         }
         float f[kFeat];
-        node_features(t, mean, g, M, nc, wc, q0, q1, q2, q3, depth, f);
+        const int lc = child_index(__float_as_int(b0.w), a.n), rc = child_index(__float_as_int(b1.w), a.n);
+        node_features(t, mean, g, M, nc, wc, a.records + 4 * (size_t)node, a.records + 4 * (size_t)lc,
+                      a.records + 4 * (size_t)rc, depth, a.clamp2, a.cos_thr, f);
         store_features(a.feats + (size_t)r * kFeat, f);
         a.row_entry[r] = e;
     }
 }
 
 __global__ void __launch_bounds__(256) learned_expand(LevelArgs a, const float* logits, float thr_logit) {
-    const int rows = min(*a.row_count, a.capacity);
+    const int rows = min(*a.row_count, 1 << 24);
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
-        const int4 en = a.in[a.row_entry[r]];
-        const int k = en.y - a.n;
+        const int2 en = a.in[a.row_entry[r]];
+        const int node = en.y & ((1 << kDepthShift) - 1), depth = en.y >> kDepthShift;
+        const int k = node - a.n;
         if (logits[r] >= thr_logit) {
-            push_children(a, en.x, k, en.z, a.bounds[4 * (size_t)k], a.bounds[4 * (size_t)k + 1]);
+            push_children(a, en.x, k, depth, a.bounds[4 * (size_t)k], a.bounds[4 * (size_t)k + 1]);
         } else {
-            accept_pair(a, en.x, en.y);
+            accept_pair(a, en.x, node);
         }
     }
 }
 
-__global__ void init_frontier(int4* fr, int* count, const float4* info, int tiles, int root) {
+__global__ void init_frontier(int2* fr, int* count, const float4* info, int tiles, int root) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= tiles) return;
     if (__float_as_int(info[4 * (size_t)t + 3].x) == 0) return;  // no valid pixel
     const int pos = atomicAdd(count, 1);
-    fr[pos] = make_int4(t, root, 0, 0);
+    fr[pos] = entry(t, root, 0);
 }
 
 // exclusive scan of per-tile chunk counts (single block) -> chunk base per tile, total chunks
@@ -318,6 +357,7 @@ struct LabelArgs {
     int tile0, batch;
     double* prefix;  // [batch][n + 1][64]
     float delta;
+    float band;
     __nv_bfloat16* feats;
     float* labels;
     float* errs;
@@ -427,29 +467,45 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
         const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
         const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
         const float4* rec = a.records + 4 * (size_t)node;
-        const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+        const float4 q2 = rec[2], q3 = rec[3];
         const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
         const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
         if (!(M > t.tau)) continue;  // the analytic bound accepts it: no decision to learn
+        const int c0 = child_index(__float_as_int(b0.w), a.n), c1 = child_index(__float_as_int(b1.w), a.n);
+        const int d1 = min(depth + 1, 127) << 24;
+        if (M > a.band * t.tau) {  // outside the network's band: selection always refines it
+            if (!extra) {
+                if (sp + 2 > 128) {
+                    set_error(a.err, ARC_DEVERR_STACK_OVERFLOW);
+                    break;
+                }
+                stack[sp++] = c1 | d1;
+                stack[sp++] = c0 | d1;
+            }
+            continue;
+        }
+        // RMS over the tile's valid pixels of |exact node contribution - node estimate|
         const int f0 = ranges[2 * k], l0 = ranges[2 * k + 1];
-        float emax = 0.0f;
+        float e2 = 0.0f;
         for (int h = 0; h < 2; ++h) {
             if (!valid[h]) continue;
             const int p = lane + 32 * h;
             const float exact = (float)(P[(size_t)(l0 + 1) * 64 + p] - P[(size_t)f0 * 64 + p]);
             const float approx = record_lum<AR>(rec, px[h], kd[h], a.pc, a.disk_scale);
-            emax = fmaxf(emax, fabsf(exact - approx));
+            e2 += (exact - approx) * (exact - approx);
         }
-        for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-        const bool refine = emax > thr;
+        for (int o = 16; o > 0; o >>= 1) e2 += __shfl_xor_sync(0xffffffffu, e2, o);
+        const float erms = sqrtf(e2 / fmaxf(nv, 1.0f));
+        const bool refine = erms > thr;
         if (lane == 0) {
             const int r = atomicAdd(a.count, 1);
             if (r < a.capacity) {
                 float f[kFeat];
-                node_features(t, mean, g, M, nc, wc, q0, q1, q2, q3, depth, f);
+                node_features(t, mean, g, M, nc, wc, rec, a.records + 4 * (size_t)c0, a.records + 4 * (size_t)c1, depth,
+                              a.bp.clamp2, a.bp.cos_thr, f);
                 store_features(a.feats + (size_t)r * kFeat, f);
                 a.labels[r] = refine ? 1.0f : 0.0f;
-                a.errs[r] = Eexact > 0.0f ? emax / Eexact : 0.0f;
+                a.errs[r] = Eexact > 0.0f ? erms / Eexact : 0.0f;
             }
         }
         if (extra) continue;
@@ -457,8 +513,6 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
             set_error(a.err, ARC_DEVERR_STACK_OVERFLOW);
             break;
         }
-        const int c0 = child_index(__float_as_int(b0.w), a.n), c1 = child_index(__float_as_int(b1.w), a.n);
-        const int d1 = min(depth + 1, 127) << 24;
         const int flag = refine ? 0 : (int)0x80000000;  // below an accepted node: one level only
         stack[sp++] = (c1 | d1) | flag;
         stack[sp++] = (c0 | d1) | flag;
@@ -490,27 +544,32 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     const int tiles = tiles_x * tiles_y;
     const int n = bvh->n;
     // capacities: frontier / rows per level and accepted pairs over the whole walk
-    const int cap = (int)std::min<int64_t>((int64_t)tiles * 2048 + 1024, 1 << 30);
+    ARC_CHECK_ARG(2 * n - 1 < (1 << 26), "learned cut supports trees of up to 2^25 leaves");
+    // frontier capacity per level, and rows the network scores per launch (a level with more
+    // rows is processed in slices)
+    const int cap = (int)std::min<int64_t>((int64_t)tiles * 8192 + (1 << 20), 1 << 30);
+    const int row_cap = 1 << 24;
     const int acc_cap = (int)std::min<int64_t>((int64_t)pool.num_chunks * kChunk, (int64_t)INT32_MAX);
-    int4 *fa, *fb;
+    int2 *fa, *fb;
     int2* accepted;
     __nv_bfloat16* feats;
     int *row_entry, *counters, *tile_counts, *chunk_base, *fill;
     float* logits;
     ARC_TRY(arena_get(ctx, "lc_front_a", cap, &fa));
     ARC_TRY(arena_get(ctx, "lc_front_b", cap, &fb));
-    ARC_TRY(arena_get(ctx, "lc_feats", (size_t)cap * kFeat, &feats));
-    ARC_TRY(arena_get(ctx, "lc_row_entry", cap, &row_entry));
-    ARC_TRY(arena_get(ctx, "lc_logits", cap, &logits));
+    ARC_TRY(arena_get(ctx, "lc_feats", (size_t)row_cap * kFeat, &feats));
+    ARC_TRY(arena_get(ctx, "lc_row_entry", row_cap, &row_entry));
+    ARC_TRY(arena_get(ctx, "lc_logits", row_cap, &logits));
     ARC_TRY(arena_get(ctx, "lc_accepted", acc_cap, &accepted));
     // counters: [0] in count, [1] out count, [2] rows, [3] accepted, [4] total chunks, then one
     // (in, out, rows) triple per level
     constexpr int kMaxLevels = 96;
-    ARC_TRY(arena_get(ctx, "lc_counters", 8 + 4 * kMaxLevels, &counters));
+    constexpr int kSlots = 8 + 4 * kMaxLevels + 2 * 4096;  // per level: in, out; per slice: rows
+    ARC_TRY(arena_get(ctx, "lc_counters", kSlots, &counters));
     ARC_TRY(arena_get(ctx, "lc_tile_counts", tiles, &tile_counts));
     ARC_TRY(arena_get(ctx, "lc_chunk_base", tiles, &chunk_base));
     ARC_TRY(arena_get(ctx, "lc_fill", tiles, &fill));
-    ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * (8 + 4 * kMaxLevels), st));
+    ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * kSlots, st));
     ARC_TRY_CUDA(cudaMemsetAsync(tile_counts, 0, sizeof(int) * tiles, st));
     ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * tiles, st));
 
@@ -529,7 +588,13 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.acc_count = counters + 3;
     la.acc_capacity = acc_cap;
     la.tile_counts = tile_counts;
+    la.band = cp->mlp_band > 0.0f ? cp->mlp_band : INFINITY;
+    la.clamp2 = gp->dist_clamp > 0.0f ? gp->dist_clamp * gp->dist_clamp : 0.0f;
+    la.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
     la.err = ctx->d_error;
+    la.capacity = cap;
+    int* slice_rows = counters + 8 + 4 * kMaxLevels;
+    int slice = 0;
 
     stage_begin(ctx, "cut_learned");
     int kernels = 0;
@@ -537,7 +602,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, in_count, info, tiles, n);
     ++kernels;
     const int grid = ctx->sm_count * 8;
-    int4 *cur = fa, *nxt = fb;
+    int2 *cur = fa, *nxt = fb;
     for (int level = 0; level < kMaxLevels; ++level) {
         int host_count = 0;
         ARC_TRY_CUDA(cudaMemcpyAsync(&host_count, in_count, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -548,21 +613,35 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
         la.in_count = in_count;
         la.out = nxt;
         la.out_count = out_count;
-        la.row_count = counters + 8 + 4 * level + 2;
-        const int blocks = std::max(1, std::min(grid, (host_count + 255) / 256));
-        learned_level<<<blocks, 256, 0, st>>>(la);
-        ++kernels;
-        int rows = 0;
-        ARC_TRY_CUDA(cudaMemcpyAsync(&rows, la.row_count, sizeof(int), cudaMemcpyDeviceToHost, st));
-        ARC_TRY_CUDA(cudaStreamSynchronize(st));
-        rows = std::min(rows, cap);
-        if (rows > 0) {
-            ARC_TRY(mlp_forward_device(const_cast<arc_mlp*>(cp->model), feats, rows, logits));
+        // a slice of entries can produce at most one row each
+        const int per_slice = row_cap;
+        for (int b = 0; b < std::min(host_count, cap); b += per_slice) {
+            if (slice >= 2 * 4096) {
+                set_last_error("learned cut: too many level slices");
+                return ARC_ERR_OUT_OF_MEMORY;
+            }
+            la.begin = b;
+            la.end = b + per_slice;
+            la.row_count = slice_rows + slice++;
+            const int n_in = std::min(per_slice, std::min(host_count, cap) - b);
+            const int blocks = std::max(1, std::min(grid, (n_in + 255) / 256));
+            learned_level<<<blocks, 256, 0, st>>>(la);
             ++kernels;
-            learned_expand<<<std::max(1, std::min(grid, (rows + 255) / 256)), 256, 0, st>>>(la, logits, thr_logit);
-            ++kernels;
+            int rows = 0;
+            ARC_TRY_CUDA(cudaMemcpyAsync(&rows, la.row_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+            ARC_TRY_CUDA(cudaStreamSynchronize(st));
+            rows = std::min(rows, row_cap);
+            ctx->learned_rows += rows;
+            if (rows > 0) {
+                ARC_TRY(mlp_forward_device(const_cast<arc_mlp*>(cp->model), feats, rows, logits));
+                ++kernels;
+                LevelArgs ex = la;
+                ex.capacity = cap;
+                learned_expand<<<std::max(1, std::min(grid, (rows + 255) / 256)), 256, 0, st>>>(ex, logits, thr_logit);
+                ++kernels;
+            }
+            ARC_TRY_CUDA(cudaGetLastError());
         }
-        ARC_TRY_CUDA(cudaGetLastError());
         in_count = out_count;
         std::swap(cur, nxt);
     }
@@ -635,6 +714,7 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     a.tiles_x = tiles_x;
     a.prefix = prefix;
     a.delta = delta;
+    a.band = cp->mlp_band > 0.0f ? cp->mlp_band : INFINITY;
     a.feats = static_cast<__nv_bfloat16*>(features_bf16);
     a.labels = labels;
     a.errs = errors;

@@ -30,7 +30,12 @@ NUM_PARAMS = 9473
 # training set-up (the learned-cut configuration)
 TRAIN_SEEDS = range(100, 164)
 TRAIN_W, TRAIN_H, TRAIN_AVPLS = 256, 192, 65536
-LABEL_DELTA = 5e-4  # refine when the node's true error exceeds this fraction of the tile value
+LABEL_DELTA = 1.5e-4  # refine when the node's true error exceeds this fraction of the tile value
+# analytic pre-acceptance shared by labelling and selection: nodes whose error bound is within
+# PREACCEPT_EPS of the tile estimate (antiradiance-uncertain nodes weighted by PREACCEPT_K) are
+# accepted without the network; the network decides every other node
+PREACCEPT_EPS = 1e-3
+PREACCEPT_K = 64.0
 
 
 class Model:
@@ -64,6 +69,12 @@ class Model:
         self.handle = None
 
 
+def cut_params(model: Model, threshold: float = 0.5, **kw):
+    """ArcCutParams of the learned cut with the pre-acceptance the model was trained with."""
+    return api.cut_params(L.ARC_CUT_LEARNED, error_bound=PREACCEPT_EPS, ar_uncertain_factor=PREACCEPT_K,
+                          model=model.handle.value, mlp_threshold=threshold, **kw)
+
+
 def load_default_model(ctx: api.Context, path: str = DEFAULT_MODEL) -> Model:
     if not os.path.exists(path):
         raise FileNotFoundError(f"no trained cut model at {path}")
@@ -71,7 +82,7 @@ def load_default_model(ctx: api.Context, path: str = DEFAULT_MODEL) -> Model:
 
 
 def scene_samples(ctx: api.Context, seed: int, capacity: int, width=TRAIN_W, height=TRAIN_H, num_avpls=TRAIN_AVPLS,
-                  delta=LABEL_DELTA, error_bound=0.01, ar_uncertain=16.0):
+                  delta=LABEL_DELTA, error_bound=PREACCEPT_EPS, ar_uncertain=PREACCEPT_K):
     """(features bf16 [k,16], labels [k], errors [k]) torch CUDA tensors for one training scene."""
     import torch
 

@@ -168,6 +168,8 @@ arc_status arc_context_stage_times(arc_context* ctx, char* names, size_t names_l
                                    int32_t* num_stages);
 /* Number of kernels this context has launched so far. */
 uint64_t arc_context_launch_count(arc_context* ctx);
+/* Number of (tile, node) rows the learned cut's network has scored on this context so far. */
+uint64_t arc_context_learned_rows(arc_context* ctx);
 /* FP32 FMA throughput of the device with scalar FFMA and packed fma.rn.f32x2 chains (TFLOP/s),
  * the roofline denominator of the gather kernels.  No reference counterpart. */
 arc_status arc_measure_fp32_peak(arc_context* ctx, double* scalar_tflops, double* packed_tflops);
@@ -330,6 +332,8 @@ typedef struct ArcCutParams {
     int64_t cut_pool_entries;    /* total cut entries over all tiles; 0 = 65536 per tile */
     const arc_mlp* model;        /* LEARNED only */
     float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this */
+    float mlp_band;              /* LEARNED: nodes whose error bound exceeds mlp_band times the tile's error
+                                    budget are refined without the network (default 4096; 0 = no limit) */
     int32_t debug_pixel_x;       /* SOLID_ANGLE scene probe (cudaGather.cu:338, 392-396); -1 = off */
     int32_t debug_pixel_y;
     int32_t* used_nodes;         /* optional device array[2N-1]: set to 1 for nodes the probe pixel used */

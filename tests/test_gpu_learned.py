@@ -28,7 +28,8 @@ def scene_(ctx):
 
 def _gather(ctx, d, bvh, gb, cut):
     prm = api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
-    out = api.Outputs(W, HGT)
+    h, w = d["pos"].shape[:2]
+    out = api.Outputs(w, h)
     api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, cut, out)
     assert ctx.synchronize() == 0
     return out.result64.cpu().numpy().reshape(-1, 3), api.last_cut(ctx)
@@ -95,15 +96,9 @@ def test_trained_model_beats_analytic_cut_on_held_out_scene(ctx):
     px = np.arange(160 * 96)
     _, _, exact = O.gather_fp64(d["pos"], d["nrm"], px, d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"],
                                 O.params(2, 30.0, 0.01))
-    global W, HGT
-    W0, H0 = W, HGT
-    W, HGT = 160, 96
-    try:
-        img_b, cuts_b = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01))
-        img_l, cuts_l = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=0.01,
-                                                                model=model.handle.value))
-    finally:
-        W, HGT = W0, H0
+    img_b, cuts_b = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01))
+    img_l, cuts_l = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=0.01,
+                                                            model=model.handle.value))
     eb, el = H.rel_rmse(img_b, exact), H.rel_rmse(img_l, exact)
     nb, nl = sum(map(len, cuts_b)), sum(map(len, cuts_l))
     print(f"analytic: {nb} nodes, rel RMSE {eb:.4f}; learned: {nl} nodes, rel RMSE {el:.4f}")
