@@ -208,7 +208,7 @@ class AvplBvh:
 
 def cut_params(kind=L.ARC_CUT_ERROR_BOUND, error_bound=0.01, solid_angle_threshold=math.pi / 10,
                max_cut_nodes=1 << 20, model=None, mlp_threshold=0.5, debug_pixel=(-1, -1), used_nodes=None,
-               ar_uncertain_factor=16.0, cut_pool_entries=0):
+               ar_uncertain_factor=16.0, cut_pool_entries=0, mlp_band=None):
     p = L.ArcCutParams()
     L.load().arc_cut_params_default(C.byref(p))
     p.kind = kind
@@ -219,6 +219,8 @@ def cut_params(kind=L.ARC_CUT_ERROR_BOUND, error_bound=0.01, solid_angle_thresho
     p.cut_pool_entries = cut_pool_entries
     p.model = model
     p.mlp_threshold = mlp_threshold
+    if mlp_band is not None:
+        p.mlp_band = mlp_band
     p.debug_pixel_x, p.debug_pixel_y = debug_pixel
     p.used_nodes = used_nodes
     return p

@@ -1,22 +1,29 @@
 // Learned cut selection and its training data.
 //
 // Selection (ARC_CUT_LEARNED): a level-synchronous walk over all tiles at once.  Level l holds
-// the (tile, node) pairs at depth l.  For each pair, learned_level:
-//   * accepts leaves, and inner nodes whose analytic bound is already within the tile's threshold
-//     (the learned cut is never finer than the analytic one);
-//   * otherwise writes the pair's 16 features (BF16) as one row for the MLP.
-// The tensor-core MLP (mlp.cu) scores every row of the level in one launch, and learned_expand
-// refines the rows whose logit reaches the threshold (children go to level l + 1) and accepts the
-// rest.  Accepted pairs are finally grouped by tile into the chunked cut pool (count, scan,
-// scatter), which the shared cut evaluation reads.
+// the (tile, node) pairs at depth l.  One fused launch per level (learned_level) does, for every
+// pair:
+//   * leaves, and inner nodes whose analytic bound is already within the tile's threshold, are
+//     accepted (the learned cut is never finer than the analytic one);
+//   * inner nodes whose bound exceeds mlp_band times the threshold are refined (their children go
+//     to level l + 1) without the network;
+//   * every other pair's 16 features (BF16) are staged as one row of the CTA's 128-row tile in
+//     shared memory; each full tile is scored on the tensor cores (mlp_tile.cuh) and its pairs are
+//     refined or accepted by the logit, in the same launch.
+// Persistent CTAs take 128 pairs at a time from a per-level work counter; pushes and accepts use
+// warp-aggregated atomics.  The host checks the frontier size only every few levels.  Accepted
+// pairs are finally grouped by tile into the chunked cut pool (count, scan, scatter), which the
+// shared cut evaluation reads.
 //
 // Training data (arc_cut_training_samples): for a batch of tiles, label_prefix computes, per
 // pixel, the FP64 prefix sums over the sorted leaves of the luminance of each leaf's signed
 // contribution; a node's exact contribution is then a difference of two prefixes (its leaves form
 // one contiguous range).  label_traverse walks each tile's tree with the exact decision: refine iff
 // max over the tile's pixels |exact - node estimate| > delta * mean |exact tile value|, and emits
-// (features, label, error) for every visited node the analytic bound cannot accept (plus one level
-// below accepted nodes, so the model also sees the children it would skip).
+// (features, label, error) for every visited node that the selection would score: the analytic
+// bound neither accepts it nor puts it above the refine band (plus one level below accepted
+// nodes, so the model also sees the children it would skip).  The error is the RMS over the tile's
+// pixels of |exact node contribution - node estimate|, against delta * mean |exact tile value|.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -27,12 +34,13 @@
 #include "arc_internal.h"
 #include "cut_bounds.cuh"
 #include "device_common.cuh"
+#include "mlp_tile.cuh"
 #include "pair_math.cuh"
+#include "tcgen05.cuh"
 
 namespace arc {
 
 const float* mlp_params(const arc_mlp* m);
-arc_status mlp_forward_device(arc_mlp* m, const void* x, int64_t rows, float* logits);
 
 namespace {
 
@@ -54,7 +62,8 @@ __device__ __forceinline__ TileInfo load_tile_info(const float4* info, int tile,
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
-__device__ __forceinline__ float safe_log2(float v) { return log2f(fmaxf(v, 1e-30f)); }
+// features are coarse network inputs: fast hardware log2 / division
+__device__ __forceinline__ float safe_log2(float v) { return __log2f(fmaxf(v, 1e-30f)); }
 
 // Radiance and antiradiance luminance of one packed record at a point p with unit normal n
 // (receiver albedo folded into kdl by the caller).
@@ -66,7 +75,7 @@ __device__ __forceinline__ void record_at(const float4* rec, float px, float py,
     const float r = rsqrtf(l2);
     const float c1 = (nx * dx + ny * dy + nz * dz) * r;
     const float c2 = -(q0.w * dx + q1.x * dy + q1.y * dz) * r;
-    const float inv = 1.0f / fmaxf(l2, clamp2);
+    const float inv = __fdividef(1.0f, fmaxf(l2, clamp2));
     rad = lum3(q2.y, q2.z, q2.w) * fmaxf(c1, 0.0f) * fmaxf(c2, 0.0f) * inv;
     const float cw = -(q1.z * dx + q1.w * dy + q2.x * dz) * r;
     ar = (cw > cos_thr && c1 > 0.001f) ? lum3(q3.x, q3.y, q3.z) * c1 * inv : 0.0f;
@@ -82,7 +91,7 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
     const float E = fmaxf(mean, 1e-30f);
     const float4 q2 = rec[2], q3 = rec[3];
     const float Ls = lum3(q2.y, q2.z, q2.w), As = lum3(q3.x, q3.y, q3.z);
-    const float inv_dc = 1.0f / fmaxf(g.dc, 1e-6f);
+    const float inv_dc = __fdividef(1.0f, fmaxf(g.dc, 1e-6f));
     const float rt = g.rs - g.rn;
     const float cx = 0.5f * (t.tmin[0] + t.tmax[0]), cy = 0.5f * (t.tmin[1] + t.tmax[1]),
                 cz = 0.5f * (t.tmin[2] + t.tmax[2]);
@@ -98,7 +107,7 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
     record_at(rec, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, rad, ar);
     record_at(rec_l, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radl, arl);
     record_at(rec_r, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radr, arr);
-    const float s = t.kdl / E;
+    const float s = __fdividef(t.kdl, E);
     f[0] = clampf((M > 0.0f ? safe_log2(M / fmaxf(t.tau, 1e-30f)) : -32.0f) * 0.125f, -4.0f, 4.0f);
     f[1] = clampf(safe_log2(Ls * s) * 0.125f, -4.0f, 4.0f);
     f[2] = clampf(safe_log2(As * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
@@ -147,29 +156,19 @@ struct LevelArgs {
     const int* in_count;
     int2* out;              // next level
     int* out_count;
-    int capacity;           // entries per frontier / row buffer
-    __nv_bfloat16* feats;   // [capacity][16]
-    int* row_entry;         // row -> index into `in`
-    int* row_count;
+    int capacity;           // entries per frontier
+    int* work;              // chunks of 128 entries handed out
+    unsigned long long* rows_scored;
+    const unsigned char* weight_image;  // network, in the shared-memory layout (weight_image)
+    float thr_logit;        // refine iff logit >= thr_logit
     int2* accepted;         // {tile, node}
     int* acc_count;
     int acc_capacity;
     int* tile_counts;
     float band;             // M > band * tau: refine without the network
     float clamp2, cos_thr;
-    int begin, end;         // entries of `in` handled by this launch
     uint32_t* err;
 };
-
-__device__ __forceinline__ void accept_pair(const LevelArgs& a, int tile, int node) {
-    const int pos = atomicAdd(a.acc_count, 1);
-    if (pos < a.acc_capacity) {
-        a.accepted[pos] = make_int2(tile, node);
-        atomicAdd(&a.tile_counts[tile], 1);
-    } else {
-        set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
-    }
-}
 
 constexpr int kDepthShift = 26;  // node ids < 2^26 (trees of up to 32M leaves), depth < 32
 
@@ -177,66 +176,185 @@ __device__ __forceinline__ int2 entry(int tile, int node, int depth) {
     return make_int2(tile, node | (min(depth, 31) << kDepthShift));
 }
 
-__device__ __forceinline__ void push_children(const LevelArgs& a, int tile, int k, int depth, float4 b0, float4 b1) {
-    const int pos = atomicAdd(a.out_count, 2);
-    if (pos + 1 < a.capacity) {
-        a.out[pos] = entry(tile, child_index(__float_as_int(b0.w), a.n), depth + 1);
-        a.out[pos + 1] = entry(tile, child_index(__float_as_int(b1.w), a.n), depth + 1);
-    } else {
-        set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
-    }
-}
+enum Action : int { kNone = 0, kAccept = 1, kRefine = 2, kScore = 3 };
 
-__global__ void __launch_bounds__(256) learned_level(LevelArgs a) {
-    const int count = min(min(*a.in_count, a.capacity), a.end);
-    for (int e = a.begin + blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
-        const int2 en = a.in[e];
-        const int tile = en.x, node = en.y & ((1 << kDepthShift) - 1), depth = en.y >> kDepthShift;
-        if (node < a.n) {
-            accept_pair(a, tile, node);
-            continue;
-        }
-        const int k = node - a.n;
-        float mean;
-        const TileInfo t = load_tile_info(a.info, tile, &mean);
-        const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
-        const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
-        const float4 q2 = a.records[4 * (size_t)node + 2], q3 = a.records[4 * (size_t)node + 3];
-        const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
-        const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
-        if (!(M > t.tau)) {
-            accept_pair(a, tile, node);
-            continue;
-        }
-        if (M > a.band * t.tau) {  // far outside the network's band: refine
-            push_children(a, tile, k, depth, b0, b1);
-            continue;
-        }
-        const int r = atomicAdd(a.row_count, 1);
-        if (r >= a.capacity) {  // no room to score it: refine, the safe choice
+// Accepts (tile, node) or pushes (tile, lc), (tile, rc) at depth + 1, per the lane's action; one
+// atomic per warp and kind.  Every lane of the warp calls it.
+__device__ __forceinline__ void emit(const LevelArgs& a, int action, int tile, int node, int lc, int rc, int depth) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned am = __ballot_sync(0xffffffffu, action == kAccept);
+    const unsigned pm = __ballot_sync(0xffffffffu, action == kRefine);
+    int abase = 0, pbase = 0;
+    if (am) {
+        const int leader = __ffs(am) - 1;
+        if (lane == leader) abase = atomicAdd(a.acc_count, __popc(am));
+        abase = __shfl_sync(0xffffffffu, abase, leader);
+    }
+    if (pm) {
+        const int leader = __ffs(pm) - 1;
+        if (lane == leader) pbase = atomicAdd(a.out_count, 2 * __popc(pm));
+        pbase = __shfl_sync(0xffffffffu, pbase, leader);
+    }
+    if (action == kAccept) {
+        const int pos = abase + __popc(am & lt);
+        const bool ok = pos < a.acc_capacity;
+        if (ok)
+            a.accepted[pos] = make_int2(tile, node);
+        else
             set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
-            push_children(a, tile, k, depth, b0, b1);
-            continue;
+        // one per-tile count update per group of lanes with the same tile
+        const unsigned grp = __match_any_sync(am, ok ? tile : -1 - lane);
+        if (ok && lane == __ffs(grp) - 1) atomicAdd(&a.tile_counts[tile], __popc(grp));
+    } else if (action == kRefine) {
+        const int pos = pbase + 2 * __popc(pm & lt);
+        if (pos + 1 < a.capacity) {
+            a.out[pos] = entry(tile, lc, depth + 1);
+            a.out[pos + 1] = entry(tile, rc, depth + 1);
+        } else {
+            set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
         }
-        float f[kFeat];
-        const int lc = child_index(__float_as_int(b0.w), a.n), rc = child_index(__float_as_int(b1.w), a.n);
-        node_features(t, mean, g, M, nc, wc, a.records + 4 * (size_t)node, a.records + 4 * (size_t)lc,
-                      a.records + 4 * (size_t)rc, depth, a.clamp2, a.cos_thr, f);
-        store_features(a.feats + (size_t)r * kFeat, f);
-        a.row_entry[r] = e;
     }
 }
 
-__global__ void __launch_bounds__(256) learned_expand(LevelArgs a, const float* logits, float thr_logit) {
-    const int rows = min(*a.row_count, 1 << 24);
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
-        const int2 en = a.in[a.row_entry[r]];
-        const int node = en.y & ((1 << kDepthShift) - 1), depth = en.y >> kDepthShift;
-        const int k = node - a.n;
-        if (logits[r] >= thr_logit) {
-            push_children(a, en.x, k, depth, a.bounds[4 * (size_t)k], a.bounds[4 * (size_t)k + 1]);
+// shared memory of learned_level: weights and vectors (the image built by weight_image) | staged
+// feature rows (256, K-major, K = 16) | hidden | staged pairs {tile, node | depth, left child,
+// right child}
+constexpr uint32_t fW = 0, fVec = mlp::kWeightBytes, fX = ((mlp::kImageBytes + 127) / 128) * 128, fH = fX + 8192,
+                   fMeta = fH + 16384, kLevelSmem = fMeta + 256 * 16;
+constexpr int kLevelThreads = 128;
+
+// BF16 core-matrix weights + FP32 vectors, once per selection
+__global__ void weight_image(const float* params, unsigned char* img) {
+    mlp::load_weights(img, reinterpret_cast<float*>(img + mlp::kWeightBytes), params, threadIdx.x, blockDim.x);
+}
+
+__global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t bar, wbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_chunk, s_staged;
+    const int t = threadIdx.x, w = t >> 5;
+    const int count = min(*a.in_count, a.capacity);
+    if ((int64_t)blockIdx.x * kLevelThreads >= count) return;  // no chunk can be left for this CTA
+    float* vec = reinterpret_cast<float*>(sm + fVec);
+    int4* meta = reinterpret_cast<int4*>(sm + fMeta);
+    if (t == 0) {
+        mbar_init(&bar, 1);
+        mbar_init(&wbar, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(&wbar, mlp::kImageBytes);
+        bulk_g2s(sm + fW, a.weight_image, mlp::kImageBytes, &wbar);
+        s_staged = 0;
+    }
+    for (int i = t; i < 8192 / 16; i += kLevelThreads)  // rows past the staged ones stay finite
+        reinterpret_cast<uint4*>(sm + fX)[i] = make_uint4(0, 0, 0, 0);
+    if (w == 0) tc::alloc(&tmem_base, 64);
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    bool ok = __syncthreads_and(mbar_wait_bounded(&wbar, 0, a.err)) != 0;
+    mlp::InferCta c{smem_u32(sm), fW, fH, sm, vec, tmem_base, &bar, 0u, a.err};
+    unsigned long long scored = 0;
+    while (ok) {
+        if (t == 0) s_chunk = atomicAdd(a.work, 1);
+        __syncthreads();
+        const int64_t first = (int64_t)s_chunk * kLevelThreads;
+        const bool done = first >= count;
+        const int64_t e = first + t;
+        int action = kNone, tile = 0, node = 0, lc = 0, rc = 0, depth = 0;
+        if (!done && e < count) {
+            const int2 en = a.in[e];
+            tile = en.x;
+            node = en.y & ((1 << kDepthShift) - 1);
+            depth = en.y >> kDepthShift;
+            action = kAccept;
+            if (node >= a.n) {
+                const int k = node - a.n;
+                float mean;
+                const TileInfo ti = load_tile_info(a.info, tile, &mean);
+                const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
+                const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
+                const float4 q2 = a.records[4 * (size_t)node + 2], q3 = a.records[4 * (size_t)node + 3];
+                const NodeGeom g = node_geom(ti, b0, b1, nc, wc, a.bp);
+                const float M = node_bound(ti, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
+                lc = child_index(__float_as_int(b0.w), a.n);
+                rc = child_index(__float_as_int(b1.w), a.n);
+                if (M > ti.tau) action = M > a.band * ti.tau ? kRefine : kScore;
+                if (action == kScore) {
+                    float f[kFeat];
+                    node_features(ti, mean, g, M, nc, wc, a.records + 4 * (size_t)node, a.records + 4 * (size_t)lc,
+                                  a.records + 4 * (size_t)rc, depth, a.clamp2, a.cos_thr, f);
+                    const int slot = atomicAdd(&s_staged, 1);  // < 256: at most 127 rows are left over
+                    uint4 x0, x1;
+                    x0.x = mlp::pack2(f[0], f[1]);
+                    x0.y = mlp::pack2(f[2], f[3]);
+                    x0.z = mlp::pack2(f[4], f[5]);
+                    x0.w = mlp::pack2(f[6], f[7]);
+                    x1.x = mlp::pack2(f[8], f[9]);
+                    x1.y = mlp::pack2(f[10], f[11]);
+                    x1.z = mlp::pack2(f[12], f[13]);
+                    x1.w = mlp::pack2(f[14], f[15]);
+                    *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(slot, 0, kFeat)) = x0;
+                    *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(slot, 8, kFeat)) = x1;
+                    meta[slot] = make_int4(tile, node | (depth << kDepthShift), lc, rc);
+                }
+            }
+        }
+        emit(a, action, tile, node, lc, rc, depth);
+        __syncthreads();
+        int staged = s_staged;
+        // score full tiles now, and whatever is left once the level is exhausted
+        while (staged >= kLevelThreads || (done && staged > 0)) {
+            float y = 0.0f;
+            if (!mlp::infer_tile(c, fX, t, &y)) {
+                ok = false;
+                break;
+            }
+            const int n_rows = min(staged, kLevelThreads);
+            scored += n_rows;
+            int act = kNone;
+            int4 m = make_int4(0, 0, 0, 0);
+            if (t < n_rows) {
+                m = meta[t];
+                act = y >= a.thr_logit ? kRefine : kAccept;
+            }
+            const int mnode = m.y & ((1 << kDepthShift) - 1), mdepth = m.y >> kDepthShift;
+            emit(a, act, m.x, mnode, m.z, m.w, mdepth);
+            __syncthreads();  // rows 0..127 and their pairs are consumed
+            const int rest = staged - n_rows;
+            if (t < rest) {
+                const int r = kLevelThreads + t;
+                *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(t, 0, kFeat)) =
+                    *reinterpret_cast<const uint4*>(sm + fX + tc::kmajor_offset(r, 0, kFeat));
+                *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(t, 8, kFeat)) =
+                    *reinterpret_cast<const uint4*>(sm + fX + tc::kmajor_offset(r, 8, kFeat));
+                meta[t] = meta[r];
+            }
+            if (t == 0) s_staged = rest;
+            __syncthreads();
+            staged = rest;
+        }
+        if (!ok || done) break;
+    }
+    if (t == 0 && scored) atomicAdd(a.rows_scored, scored);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (w == 0) tc::dealloc(tmem_base, 64);
+}
+
+// Past the last level the host runs: every pair still in the frontier is accepted.
+__global__ void accept_frontier(LevelArgs a) {
+    const int count = min(*a.in_count, a.capacity);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+        const int2 en = a.in[e];
+        const int pos = atomicAdd(a.acc_count, 1);
+        if (pos < a.acc_capacity) {
+            a.accepted[pos] = make_int2(en.x, en.y & ((1 << kDepthShift) - 1));
+            atomicAdd(&a.tile_counts[en.x], 1);
         } else {
-            accept_pair(a, en.x, node);
+            set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
         }
     }
 }
@@ -324,11 +442,22 @@ __global__ void scatter_tables(ScatterArgs s, int tiles) {
     s.pool.counts[t] = cnt;
 }
 
+// (blockDim a multiple of 32: every lane of a warp takes the same loop trips)
 __global__ void scatter_nodes(ScatterArgs s) {
     const int count = min(*s.acc_count, s.acc_capacity);
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
-        const int2 p = s.accepted[e];
-        const int pos = atomicAdd(&s.fill[p.x], 1);
+    const int lane = threadIdx.x & 31;
+    for (int b = blockIdx.x * blockDim.x; b < count; b += gridDim.x * blockDim.x) {
+        const int e = b + threadIdx.x;
+        const bool valid = e < count;
+        const int2 p = valid ? s.accepted[e] : make_int2(-1 - lane, 0);
+        // lanes with the same tile take consecutive slots with one atomic
+        const unsigned grp = __match_any_sync(0xffffffffu, p.x);
+        const int leader = __ffs(grp) - 1;
+        int base = 0;
+        if (valid && lane == leader) base = atomicAdd(&s.fill[p.x], __popc(grp));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (!valid) continue;
+        const int pos = base + __popc(grp & ((1u << lane) - 1u));
         const int id = s.chunk_base[p.x] + pos / kChunk;
         if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p.x])
             s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p.y;
@@ -545,36 +674,30 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     const int n = bvh->n;
     // capacities: frontier / rows per level and accepted pairs over the whole walk
     ARC_CHECK_ARG(2 * n - 1 < (1 << 26), "learned cut supports trees of up to 2^25 leaves");
-    // frontier capacity per level, and rows the network scores per launch (a level with more
-    // rows is processed in slices)
+    // frontier capacity per level
     const int cap = (int)std::min<int64_t>((int64_t)tiles * 8192 + (1 << 20), 1 << 30);
-    const int row_cap = 1 << 24;
     const int acc_cap = (int)std::min<int64_t>((int64_t)pool.num_chunks * kChunk, (int64_t)INT32_MAX);
     int2 *fa, *fb;
     int2* accepted;
-    __nv_bfloat16* feats;
-    int *row_entry, *counters, *tile_counts, *chunk_base, *fill;
-    float* logits;
+    int *counters, *tile_counts, *chunk_base, *fill;
+    unsigned long long* rows_scored;
     ARC_TRY(arena_get(ctx, "lc_front_a", cap, &fa));
     ARC_TRY(arena_get(ctx, "lc_front_b", cap, &fb));
-    ARC_TRY(arena_get(ctx, "lc_feats", (size_t)row_cap * kFeat, &feats));
-    ARC_TRY(arena_get(ctx, "lc_row_entry", row_cap, &row_entry));
-    ARC_TRY(arena_get(ctx, "lc_logits", row_cap, &logits));
     ARC_TRY(arena_get(ctx, "lc_accepted", acc_cap, &accepted));
-    // counters: [0] in count, [1] out count, [2] rows, [3] accepted, [4] total chunks, then one
-    // (in, out, rows) triple per level
+    // counters: [3] accepted, [4] total chunks, then per level l at 8 + 4 l: [0] entries, [2] work
     constexpr int kMaxLevels = 96;
-    constexpr int kSlots = 8 + 4 * kMaxLevels + 2 * 4096;  // per level: in, out; per slice: rows
+    constexpr int kSlots = 8 + 4 * (kMaxLevels + 1);
     ARC_TRY(arena_get(ctx, "lc_counters", kSlots, &counters));
+    ARC_TRY(arena_get(ctx, "lc_rows", 1, &rows_scored));
     ARC_TRY(arena_get(ctx, "lc_tile_counts", tiles, &tile_counts));
     ARC_TRY(arena_get(ctx, "lc_chunk_base", tiles, &chunk_base));
     ARC_TRY(arena_get(ctx, "lc_fill", tiles, &fill));
     ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * kSlots, st));
+    ARC_TRY_CUDA(cudaMemsetAsync(rows_scored, 0, sizeof(unsigned long long), st));
     ARC_TRY_CUDA(cudaMemsetAsync(tile_counts, 0, sizeof(int) * tiles, st));
     ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * tiles, st));
 
     const float p = cp->mlp_threshold;
-    const float thr_logit = p <= 0.0f ? -INFINITY : (p >= 1.0f ? INFINITY : logf(p / (1.0f - p)));
     LevelArgs la{};
     la.n = n;
     la.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
@@ -582,8 +705,11 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.info = info;
     la.bp = bound_params(gp, cp);
     la.capacity = cap;
-    la.feats = feats;
-    la.row_entry = row_entry;
+    la.rows_scored = rows_scored;
+    unsigned char* img;
+    ARC_TRY(arena_get(ctx, "lc_weight_image", mlp::kImageBytes, &img));
+    la.weight_image = img;
+    la.thr_logit = p <= 0.0f ? -INFINITY : (p >= 1.0f ? INFINITY : logf(p / (1.0f - p)));
     la.accepted = accepted;
     la.acc_count = counters + 3;
     la.acc_capacity = acc_cap;
@@ -592,59 +718,54 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.clamp2 = gp->dist_clamp > 0.0f ? gp->dist_clamp * gp->dist_clamp : 0.0f;
     la.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
     la.err = ctx->d_error;
-    la.capacity = cap;
-    int* slice_rows = counters + 8 + 4 * kMaxLevels;
-    int slice = 0;
 
+    // resident CTAs per SM, from shared memory (the runtime's occupancy query assumes a smaller
+    // shared-memory carve-out than the launch gets); 64 TMEM columns each, 4 at most
+    int smem_sm = 0;
+    ARC_TRY_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+    const int per_sm = std::max(1, std::min(4, smem_sm / (int)(kLevelSmem + 2048)));
+    ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmem));
+    ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
     stage_begin(ctx, "cut_learned");
     int kernels = 0;
-    int* in_count = counters + 8;
-    init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, in_count, info, tiles, n);
-    ++kernels;
     const int grid = ctx->sm_count * 8;
+    weight_image<<<1, 256, 0, st>>>(mlp_params(cp->model), img);
+    init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, counters + 8, info, tiles, n);
+    kernels += 2;
     int2 *cur = fa, *nxt = fb;
-    for (int level = 0; level < kMaxLevels; ++level) {
-        int host_count = 0;
-        ARC_TRY_CUDA(cudaMemcpyAsync(&host_count, in_count, sizeof(int), cudaMemcpyDeviceToHost, st));
-        ARC_TRY_CUDA(cudaStreamSynchronize(st));
-        if (host_count == 0) break;
-        int* out_count = counters + 8 + 4 * (level + 1);
-        la.in = cur;
-        la.in_count = in_count;
-        la.out = nxt;
-        la.out_count = out_count;
-        // a slice of entries can produce at most one row each
-        const int per_slice = row_cap;
-        for (int b = 0; b < std::min(host_count, cap); b += per_slice) {
-            if (slice >= 2 * 4096) {
-                set_last_error("learned cut: too many level slices");
-                return ARC_ERR_OUT_OF_MEMORY;
-            }
-            la.begin = b;
-            la.end = b + per_slice;
-            la.row_count = slice_rows + slice++;
-            const int n_in = std::min(per_slice, std::min(host_count, cap) - b);
-            const int blocks = std::max(1, std::min(grid, (n_in + 255) / 256));
-            learned_level<<<blocks, 256, 0, st>>>(la);
+    // the frontier size is read back every kCheck levels; launches past the last level return
+    // at once
+    constexpr int kCheck = 6;
+    int level = 0;
+    bool empty = false;
+    while (level < kMaxLevels && !empty) {
+        const int upto = std::min(kMaxLevels, level + kCheck);
+        for (; level < upto; ++level) {
+            la.in = cur;
+            la.in_count = counters + 8 + 4 * level;
+            la.work = counters + 8 + 4 * level + 2;
+            la.out = nxt;
+            la.out_count = counters + 8 + 4 * (level + 1);
+            learned_level<<<ctx->sm_count * per_sm, kLevelThreads, kLevelSmem, st>>>(la);
             ++kernels;
-            int rows = 0;
-            ARC_TRY_CUDA(cudaMemcpyAsync(&rows, la.row_count, sizeof(int), cudaMemcpyDeviceToHost, st));
-            ARC_TRY_CUDA(cudaStreamSynchronize(st));
-            rows = std::min(rows, row_cap);
-            ctx->learned_rows += rows;
-            if (rows > 0) {
-                ARC_TRY(mlp_forward_device(const_cast<arc_mlp*>(cp->model), feats, rows, logits));
-                ++kernels;
-                LevelArgs ex = la;
-                ex.capacity = cap;
-                learned_expand<<<std::max(1, std::min(grid, (rows + 255) / 256)), 256, 0, st>>>(ex, logits, thr_logit);
-                ++kernels;
-            }
-            ARC_TRY_CUDA(cudaGetLastError());
+            std::swap(cur, nxt);
         }
-        in_count = out_count;
-        std::swap(cur, nxt);
+        int host_count = 0;
+        ARC_TRY_CUDA(cudaMemcpyAsync(&host_count, counters + 8 + 4 * level, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ARC_TRY_CUDA(cudaStreamSynchronize(st));
+        empty = host_count == 0;
     }
+    if (!empty) {  // deeper than the walk goes: accept what is left
+        la.in = cur;
+        la.in_count = counters + 8 + 4 * level;
+        accept_frontier<<<grid, 256, 0, st>>>(la);
+        ++kernels;
+    }
+    unsigned long long rows = 0;
+    ARC_TRY_CUDA(cudaMemcpyAsync(&rows, rows_scored, sizeof(rows), cudaMemcpyDeviceToHost, st));
+    ARC_TRY_CUDA(cudaStreamSynchronize(st));
+    ctx->learned_rows += (int64_t)rows;
     ScatterArgs sa;
     sa.accepted = accepted;
     sa.acc_count = counters + 3;

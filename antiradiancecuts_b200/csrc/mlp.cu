@@ -2,10 +2,10 @@
 // the 5th-generation tensor cores.  No counterpart in the reference: it predicts, for an 8x8 pixel
 // tile and a tree node, whether the cut must refine the node.
 //
-// One kernel, two modes.  Each 128-thread CTA walks 128-row tiles of the input (thread t owns
-// row t):
+// Two kernels.  Each 128-thread CTA walks 128-row tiles of the input (thread t owns row t):
 //   forward   X[128x16] -> tcgen05.mma -> TMEM -> +b, GELU -> BF16 core-matrix smem -> next layer;
-//             the 64 -> 1 output layer runs on the CUDA cores from registers.
+//             the 64 -> 1 output layer runs on the CUDA cores from registers (mlp_tile.cuh, shared
+//             with the fused level kernel of the learned cut).
 //   training  the forward pass, then BCE gradient, and the backward pass:
 //             dH_l = dZ_{l+1} W_{l+1}                       (M = 128 rows, B read MN-major)
 //             dW_l += dZ_l^T H_{l-1}   (accumulated in TMEM over every tile the CTA owns;
@@ -24,16 +24,12 @@
 
 #include "arc_internal.h"
 #include "device_common.cuh"
+#include "mlp_tile.cuh"
 #include "pcg32.h"
 #include "tcgen05.cuh"
 
 namespace arc {
 namespace mlp {
-
-constexpr int kIn = 16, kHid = 64, kRows = 128;
-// parameter layout of the FP32 master copy
-constexpr int oW1 = 0, oB1 = oW1 + kHid * kIn, oW2 = oB1 + kHid, oB2 = oW2 + kHid * kHid, oW3 = oB2 + kHid,
-              oB3 = oW3 + kHid * kHid, oW4 = oB3 + kHid, oB4 = oW4 + kHid, kParams = oB4 + 1;  // 9473
 
 // shared-memory carve-up (bytes); dZ is followed by 2 KB because the M-padded weight-gradient
 // MMA reads up to that far past it (the extra rows land in D rows 64..127, which are ignored)
@@ -41,8 +37,10 @@ constexpr uint32_t sW1 = 0, sW2 = sW1 + 2048, sW3 = sW2 + 8192, sX = sW3 + 8192,
                    sH2 = sH1 + 16384, sZ1 = sH2 + 16384, sZ2 = sZ1 + 16384, sDZ = sZ2 + 16384,
                    sVecTrain = sDZ + 16384 + 2048;
 constexpr uint32_t kVecBytes = (4 * 64 + 4 * 64 + 4) * 4;
-constexpr uint32_t kSmemInfer = sZ1 + kVecBytes;  // vectors follow H2 in inference mode
 constexpr uint32_t kSmemTrain = sVecTrain + kVecBytes;
+// inference: weights | X tile (4 KB) | hidden (16 KB) | vectors
+constexpr uint32_t sInX = kWeightBytes, sInH = sInX + 4096, sInVec = sInH + 16384,
+                   kSmemInfer = sInVec + kVecBytesInfer;
 
 struct Args {
     const float* params;
@@ -56,16 +54,6 @@ struct Args {
     float* loss;              // [1]
     uint32_t* err;
 };
-
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118f)); }
-__device__ __forceinline__ float gelu_grad(float x) {
-    return 0.5f * (1.0f + erff(x * 0.70710678118f)) + x * 0.39894228040f * expf(-0.5f * x * x);
-}
-
-__device__ __forceinline__ uint32_t pack2(float a, float b) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<const uint32_t*>(&v);
-}
 
 // store 64 values of row t as BF16 into a K-major (K = 64) core-matrix buffer
 __device__ __forceinline__ void store_row64(unsigned char* buf, int t, const float* v) {
@@ -115,13 +103,52 @@ __device__ __forceinline__ void accumulate_columns(const float* v, float* g, int
     }
 }
 
-template <bool TRAIN>
-__global__ void __launch_bounds__(128) mlp_kernel(Args a) {
+// Forward over every row of the input: persistent CTAs, one 128-row tile at a time.
+__global__ void __launch_bounds__(128) mlp_infer_kernel(Args a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    const int t = threadIdx.x, w = t >> 5;
+    float* vec = reinterpret_cast<float*>(sm + sInVec);
+    load_weights(sm, vec, a.params, t, 128);
+    if (w == 0) tc::alloc(&tmem_base, 64);
+    if (t == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    InferCta c{smem_u32(sm), 0, sInH, sm, vec, tmem_base, &bar, 0u, a.err};
+    const int64_t ntiles = (a.rows + kRows - 1) / kRows;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t row = tile * kRows + t;
+        const bool valid = row < a.rows;
+        uint4 x0 = make_uint4(0, 0, 0, 0), x1 = make_uint4(0, 0, 0, 0);
+        if (valid) {
+            const uint4* xp = reinterpret_cast<const uint4*>(a.x + row * kIn);
+            x0 = xp[0];
+            x1 = xp[1];
+        }
+        *reinterpret_cast<uint4*>(sm + sInX + tc::kmajor_offset(t, 0, kIn)) = x0;
+        *reinterpret_cast<uint4*>(sm + sInX + tc::kmajor_offset(t, 8, kIn)) = x1;
+        float y;
+        if (!infer_tile(c, sInX, t, &y)) break;
+        if (valid) a.logits[row] = y;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (w == 0) tc::dealloc(tmem_base, 64);
+}
+
+// Forward + backward with weight-gradient accumulation in TMEM (training).
+__global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_base;
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-    float* vec = reinterpret_cast<float*>(sm + (TRAIN ? sVecTrain : sZ1));
+    float* vec = reinterpret_cast<float*>(sm + sVecTrain);
     float* b1 = vec;
     float* b2 = vec + 64;
     float* b3 = vec + 128;
@@ -131,7 +158,7 @@ __global__ void __launch_bounds__(128) mlp_kernel(Args a) {
     float* gb3 = vec + 384;
     float* gw4 = vec + 448;
     float* gb4 = vec + 512;
-    constexpr uint32_t kCols = TRAIN ? 256 : 64;  // D | dW3 | dW2 | dW1
+    constexpr uint32_t kCols = 256;  // D | dW3 | dW2 | dW1
 
     // weights -> BF16 core-matrix layouts, vectors -> FP32
     for (int i = t; i < kHid * kIn; i += 128)
@@ -150,8 +177,7 @@ __global__ void __launch_bounds__(128) mlp_kernel(Args a) {
         w4[t] = a.params[oW4 + t];
     }
     const float b4 = a.params[oB4];
-    if (TRAIN)
-        for (int i = t; i < 4 * 64 + 4; i += 128) gb1[i] = 0.0f;
+    for (int i = t; i < 4 * 64 + 4; i += 128) gb1[i] = 0.0f;
     if (w == 0) tc::alloc(&tmem_base, kCols);
     if (t == 0) {
         mbar_init(&bar, 1);
@@ -226,7 +252,7 @@ __global__ void __launch_bounds__(128) mlp_kernel(Args a) {
             h[j] = gelu(z[j]);
         }
         store_row64(sm + sH1, t, h);
-        if (TRAIN) store_row64(sm + sZ1, t, z);
+        store_row64(sm + sZ1, t, z);
         // ---- layer 2 ----
         publish_smem();
         layer64(sH1, sW2);
@@ -238,7 +264,7 @@ __global__ void __launch_bounds__(128) mlp_kernel(Args a) {
             h[j] = gelu(z[j]);
         }
         store_row64(sm + sH2, t, h);
-        if (TRAIN) store_row64(sm + sZ2, t, z);
+        store_row64(sm + sZ2, t, z);
         // ---- layer 3 (kept in registers) ----
         publish_smem();
         layer64(sH2, sW3);
@@ -253,10 +279,6 @@ __global__ void __launch_bounds__(128) mlp_kernel(Args a) {
         float y = b4;
 #pragma unroll
         for (int j = 0; j < 64; ++j) y = fmaf(h[j], w4[j], y);
-        if (!TRAIN) {
-            if (valid) a.logits[row] = y;
-            continue;
-        }
 
         // ---- loss, output-layer gradients, dZ3 ----
         float dy = 0.0f, l = 0.0f;
@@ -338,7 +360,7 @@ __global__ void __launch_bounds__(128) mlp_kernel(Args a) {
         any_tile = true;
     }
 
-    if (TRAIN && any_tile) {
+    if (any_tile) {
         // weight gradients: D rows 0..63 (= output features) live in TMEM lanes 0..63
         if (w < 2) {
             float v[64];
@@ -418,24 +440,24 @@ arc_status mlp_launch(arc_mlp* m, bool train, const void* x, int64_t rows, float
     if (train) {
         static bool attr = false;
         if (!attr) {
-            ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)mlp::kSmemTrain));
             attr = true;
         }
         const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
         stage_begin(ctx, "mlp_train");
-        mlp::mlp_kernel<true><<<grid, 128, mlp::kSmemTrain, ctx->stream>>>(a);
+        mlp::mlp_train_kernel<<<grid, 128, mlp::kSmemTrain, ctx->stream>>>(a);
         stage_end(ctx, 1);
     } else {
         static bool attr = false;
         if (!attr) {
-            ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)mlp::kSmemInfer));
             attr = true;
         }
         const int grid = (int)std::min<int64_t>(tiles, (int64_t)ctx->sm_count * 4);
         stage_begin(ctx, "mlp_forward");
-        mlp::mlp_kernel<false><<<grid, 128, mlp::kSmemInfer, ctx->stream>>>(a);
+        mlp::mlp_infer_kernel<<<grid, 128, mlp::kSmemInfer, ctx->stream>>>(a);
         stage_end(ctx, 1);
     }
     ARC_TRY_CUDA(cudaGetLastError());

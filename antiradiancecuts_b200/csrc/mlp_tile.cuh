@@ -1,0 +1,228 @@
+// Shared pieces of the cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1): parameter layout, the
+// activation, and the inference of one 128-row tile on the tensor cores, used by the stand-alone
+// forward kernel (mlp.cu) and by the fused level kernel of the learned cut (learned.cu).
+//
+// Activation: GELU in its tanh form (Hendrycks & Gimpel 2016),
+//     gelu(x) = x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))),
+// with the hardware tanh (tanh.approx.f32).  Training, inference and the FP64 oracle use this same
+// function, so the network is trained for the activation it is evaluated with.
+#ifndef ARC_MLP_TILE_CUH_
+#define ARC_MLP_TILE_CUH_
+
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "tcgen05.cuh"
+
+namespace arc {
+namespace mlp {
+
+constexpr int kIn = 16, kHid = 64, kRows = 128;
+// parameter layout of the FP32 master copy
+constexpr int oW1 = 0, oB1 = oW1 + kHid * kIn, oW2 = oB1 + kHid, oB2 = oW2 + kHid * kHid, oW3 = oB2 + kHid,
+              oB3 = oW3 + kHid * kHid, oW4 = oB3 + kHid, oB4 = oW4 + kHid, kParams = oB4 + 1;  // 9473
+
+constexpr float kGeluA = 0.7978845608f;           // sqrt(2 / pi)
+constexpr float kGeluB = 0.7978845608f * 0.044715f;
+
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float gelu(float x) {
+    const float th = tanh_hw(x * fmaf(kGeluB, x * x, kGeluA));
+    const float hx = 0.5f * x;
+    return fmaf(hx, th, hx);
+}
+
+// d gelu / dx = (1 + th) / 2 + x/2 (1 - th^2) sqrt(2/pi) (1 + 3 * 0.044715 x^2)
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float x2 = x * x;
+    const float th = tanh_hw(x * fmaf(kGeluB, x2, kGeluA));
+    return fmaf(0.5f, th, 0.5f) + 0.5f * x * (1.0f - th * th) * fmaf(3.0f * kGeluB, x2, kGeluA);
+}
+
+// Packed FP32 pairs (sm_100 f32x2 instructions: two IEEE round-to-nearest operations each, the
+// same results as the scalar forms).
+__device__ __forceinline__ uint64_t f2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_split(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// gelu of z + b for a pair, the same operations as gelu()
+__device__ __forceinline__ uint64_t gelu2(uint64_t z, uint64_t b) {
+    const uint64_t x = f2_add(z, b);
+    const uint64_t u = f2_mul(x, f2_fma(f2(kGeluB, kGeluB), f2_mul(x, x), f2(kGeluA, kGeluA)));
+    float u0, u1;
+    f2_split(u, u0, u1);
+    const uint64_t th = f2(tanh_hw(u0), tanh_hw(u1));
+    const uint64_t hx = f2_mul(x, f2(0.5f, 0.5f));
+    return f2_fma(hx, th, hx);
+}
+
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// Weights of one CTA for inference: W1 | W2 | W3 as BF16 K-major core matrices, then b1, b2,
+// b3, w4, b4 as FP32.
+constexpr uint32_t kW1 = 0, kW2 = kW1 + 2048, kW3 = kW2 + 8192, kWeightBytes = kW3 + 8192;
+constexpr uint32_t kVecBytesInfer = (4 * 64 + 4) * 4;
+// weights followed by the vectors: the image a CTA copies into shared memory in one bulk copy
+constexpr uint32_t kImageBytes = kWeightBytes + kVecBytesInfer;
+static_assert(kImageBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
+
+// Every thread of the CTA (nthreads of them) helps load the weights (into shared memory, or into
+// a global image in the same layout).
+__device__ __forceinline__ void load_weights(unsigned char* w, float* vec, const float* params, int t, int nthreads) {
+    for (int i = t; i < kHid * kIn; i += nthreads)
+        *reinterpret_cast<__nv_bfloat16*>(w + kW1 + tc::kmajor_offset(i / kIn, i % kIn, kIn)) =
+            __float2bfloat16_rn(params[oW1 + i]);
+    for (int i = t; i < kHid * kHid; i += nthreads) {
+        *reinterpret_cast<__nv_bfloat16*>(w + kW2 + tc::kmajor_offset(i / kHid, i % kHid, kHid)) =
+            __float2bfloat16_rn(params[oW2 + i]);
+        *reinterpret_cast<__nv_bfloat16*>(w + kW3 + tc::kmajor_offset(i / kHid, i % kHid, kHid)) =
+            __float2bfloat16_rn(params[oW3 + i]);
+    }
+    for (int i = t; i < 64; i += nthreads) {
+        vec[i] = params[oB1 + i];
+        vec[64 + i] = params[oB2 + i];
+        vec[128 + i] = params[oB3 + i];
+        vec[192 + i] = params[oW4 + i];
+    }
+    if (t == 0) vec[256] = params[oB4];
+}
+
+// Inference state of one 128-thread CTA: the smem base address (shared window), the weight block,
+// the 128-row hidden buffer, the FP32 vectors, 64 TMEM columns and one mbarrier.
+struct InferCta {
+    uint32_t base;     // smem_u32 of the dynamic shared memory
+    uint32_t w;        // byte offsets within it
+    uint32_t h;        // 16 KB, K-major [128][64]
+    unsigned char* sm;
+    const float* vec;  // b1 | b2 | b3 | w4 | b4
+    uint32_t tmem;
+    uint64_t* bar;
+    uint32_t phase;  // parity of the next barrier completion
+    uint32_t* err;
+};
+
+// Waits for the MMAs committed on the barrier; every thread learns whether all threads got there.
+__device__ __forceinline__ bool wait_mma(InferCta& c) {
+    const bool ok = mbar_wait_bounded(c.bar, c.phase, c.err);
+    c.phase ^= 1u;
+    tc::fence_after_sync();
+    return __syncthreads_and(ok) != 0;
+}
+
+// Makes this thread's generic-proxy smem writes visible to the tensor cores, then barrier.
+__device__ __forceinline__ void publish_smem() {
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+}
+
+// Hidden layer epilogue for this thread's row: 16 columns at a time from TMEM, + bias, GELU,
+// BF16 into the K-major hidden buffer.
+__device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const float* bias) {
+    const uint32_t lane_off = (uint32_t)((t >> 5) * 32) << 16;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float z[16];
+        tc::ld16(c.tmem + lane_off + 16 * q, z);
+        uint32_t u[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float2 bb = *reinterpret_cast<const float2*>(bias + 16 * q + 2 * j);
+            float g0, g1;
+            f2_split(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), g0, g1);
+            u[j] = pack2(g0, g1);
+        }
+        *reinterpret_cast<uint4*>(c.sm + c.h + tc::kmajor_offset(t, 16 * q, 64)) = make_uint4(u[0], u[1], u[2], u[3]);
+        *reinterpret_cast<uint4*>(c.sm + c.h + tc::kmajor_offset(t, 16 * q + 8, 64)) =
+            make_uint4(u[4], u[5], u[6], u[7]);
+    }
+}
+
+// Logit of row t of the 128-row K-major input tile at smem offset x (stride between 8-row groups:
+// 256 bytes).  Called by all 128 threads; returns false (every thread) if a tensor-core wait gave
+// up, after which the caller frees its TMEM and stops.
+__device__ __forceinline__ bool infer_tile(InferCta& c, uint32_t x, int t, float* logit) {
+    constexpr uint32_t id = tc::idesc_bf16(128, 64, false, false);
+    // layer 1 (K = 16)
+    publish_smem();
+    if (t == 0) {
+        tc::fence_after_sync();
+        tc::mma(c.tmem, tc::smem_desc(c.base + x, 128, 256), tc::smem_desc(c.base + c.w + kW1, 128, 256), id, false);
+        tc::commit(c.bar);
+    }
+    if (!wait_mma(c)) return false;
+    hidden_epilogue(c, t, c.vec);
+    // layers 2 and 3 (K = 64); layer 2 overwrites the hidden buffer it read once its MMAs are done
+#pragma unroll 1
+    for (int l = 0; l < 2; ++l) {
+        publish_smem();
+        if (t == 0) {
+            tc::fence_after_sync();
+            const uint32_t wb = c.w + (l == 0 ? kW2 : kW3);
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                tc::mma(c.tmem, tc::smem_desc(c.base + c.h + 256 * s, 128, 1024),
+                        tc::smem_desc(c.base + wb + 256 * s, 128, 1024), id, s > 0);
+            tc::commit(c.bar);
+        }
+        if (!wait_mma(c)) return false;
+        if (l == 0) hidden_epilogue(c, t, c.vec + 64);
+    }
+    // layer 3 epilogue and the 64 -> 1 output layer on the CUDA cores
+    const uint32_t lane_off = (uint32_t)((t >> 5) * 32) << 16;
+    const float* b3 = c.vec + 128;
+    const float* w4 = c.vec + 192;
+    uint64_t y2 = f2(c.vec[256], 0.0f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float z[16];
+        tc::ld16(c.tmem + lane_off + 16 * q, z);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float2 bb = *reinterpret_cast<const float2*>(b3 + 16 * q + 2 * j);
+            const float2 ww = *reinterpret_cast<const float2*>(w4 + 16 * q + 2 * j);
+            y2 = f2_fma(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), f2(ww.x, ww.y), y2);
+        }
+    }
+    float y0, y1;
+    f2_split(y2, y0, y1);
+    const float y = y0 + y1;
+    // every thread's TMEM reads are done before the next tile's MMAs overwrite the accumulator
+    tc::fence_before_sync();
+    *logit = y;
+    return true;
+}
+
+}  // namespace mlp
+}  // namespace arc
+
+#endif  // ARC_MLP_TILE_CUH_

@@ -1,5 +1,5 @@
-"""FP64 NumPy restatement of the cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, exact GELU) with
-its weighted binary-cross-entropy gradient.  TEST INFRASTRUCTURE ONLY: the checker for the
+"""FP64 NumPy restatement of the cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, GELU in its tanh
+form, Hendrycks & Gimpel 2016) with its weighted binary-cross-entropy gradient.  TEST INFRASTRUCTURE ONLY: the checker for the
 tensor-core kernels in antiradiancecuts_b200/csrc/mlp.cu; the product never imports it.
 
 Parameter layout (FP32 master copy of the library): W1[64][16], b1[64], W2[64][64], b2[64],
@@ -29,15 +29,18 @@ def pack(d):
     return np.concatenate([np.asarray(d[name], np.float64).ravel() for name, _ in SIZES])
 
 
-_erf = np.vectorize(math.erf)
+_A = math.sqrt(2.0 / math.pi)
+_B = 0.044715
 
 
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    """x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))"""
+    return 0.5 * x * (1.0 + np.tanh(_A * (x + _B * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    th = np.tanh(_A * (x + _B * x ** 3))
+    return 0.5 * (1.0 + th) + 0.5 * x * (1.0 - th * th) * _A * (1.0 + 3.0 * _B * x * x)
 
 
 def forward(p, x):

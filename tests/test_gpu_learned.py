@@ -46,6 +46,21 @@ def test_always_refine_equals_error_bound_cut(ctx, scene_):
     model.close()
 
 
+@pytest.mark.parametrize("band", [4.0, 64.0])
+def test_band_only_cut_equals_scaled_error_bound_cut(ctx, scene_, band):
+    """With threshold 1 the network never refines, so the learned cut refines exactly the nodes whose
+    bound exceeds band * tau: the error-bound cut at band * eps (powers of two scale exactly)."""
+    d, dv, bvh, tree, gb = scene_
+    model = learned.Model(ctx, seed=5)
+    eps = float(np.float32(0.01))
+    img_b, cuts_b = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=eps * band))
+    img_l, cuts_l = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=eps, mlp_band=band,
+                                                            model=model.handle.value, mlp_threshold=1.0))
+    assert all(np.array_equal(a, b) for a, b in zip(cuts_b, cuts_l))
+    assert H.rel_rmse(img_l, img_b) < 1e-6
+    model.close()
+
+
 def test_learned_cut_evaluation_matches_oracle(ctx, scene_):
     d, dv, bvh, tree, gb = scene_
     model = learned.Model(ctx, seed=4)

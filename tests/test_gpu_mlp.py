@@ -23,7 +23,7 @@ def _torch_forward(p, x):
     import torch
 
     P = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in M.unpack(p).items()}
-    gelu = lambda z: 0.5 * z * (1 + torch.erf(z / np.sqrt(2.0)))  # noqa: E731
+    gelu = lambda z: 0.5 * z * (1 + torch.tanh(np.sqrt(2.0 / np.pi) * (z + 0.044715 * z ** 3)))  # noqa: E731
     h = _bf16(x)
     z1 = h @ _bf16(P["W1"]).T + P["b1"]
     h1 = _bf16(gelu(z1))
@@ -84,7 +84,7 @@ def test_gradients_match_torch_and_oracle(ctx, mlp):
     assert abs(loss.value - l64) <= 1e-2 * abs(l64)
     # torch autograd with the kernel's rounding points (straight-through in the backward)
     P = {k: torch.tensor(v, dtype=torch.float32, device="cuda", requires_grad=True) for k, v in M.unpack(p).items()}
-    gelu = lambda z: 0.5 * z * (1 + torch.erf(z / np.sqrt(2.0)))  # noqa: E731
+    gelu = lambda z: 0.5 * z * (1 + torch.tanh(np.sqrt(2.0 / np.pi) * (z + 0.044715 * z ** 3)))  # noqa: E731
     st = lambda t: t + (_bf16(t) - t).detach()  # noqa: E731
     z1 = st(x.float()) @ st(P["W1"]).T + P["b1"]
     h1 = st(gelu(z1))
