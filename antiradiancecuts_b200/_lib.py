@@ -35,6 +35,7 @@ ARC_AR_NONE, ARC_AR_DISK, ARC_AR_CONE = 0, 1, 2
 ARC_PREC_KAHAN, ARC_PREC_KAHAN_STRICT, ARC_PREC_NAIVE, ARC_PREC_FP64 = 0, 1, 2, 3
 ARC_BBOX_SCENE, ARC_BBOX_AVPL_REFERENCE = 0, 1
 ARC_CUT_SOLID_ANGLE, ARC_CUT_ERROR_BOUND, ARC_CUT_LEARNED = 0, 1, 2
+ARC_MLP_LOSS_BCE, ARC_MLP_LOSS_SQUARED = 0, 1
 ARC_SCENE_ROOM, ARC_SCENE_ROOM_2BOXES, ARC_SCENE_ROOM_RANDOM, ARC_SCENE_TRAIN_VARIANT = 0, 1, 2, 3
 
 
@@ -99,7 +100,7 @@ class ArcLbvhView(C.Structure):
     _fields_ = [("num_leaves", C.c_int32), ("num_nodes", C.c_int32), ("morton", C.c_void_p),
                 ("sorted_index", C.c_void_p), ("left", C.c_void_p), ("right", C.c_void_p),
                 ("parents", C.c_void_p), ("range", C.c_void_p), ("bounds", C.c_void_p), ("records", C.c_void_p),
-                ("node_data", ArcAvplBvhNodeDataParam)]
+                ("node_data", ArcAvplBvhNodeDataParam), ("dirstat", C.c_void_p)]
 
 
 class ArcCutParams(C.Structure):
@@ -118,7 +119,9 @@ class ArcRunConfig(C.Structure):
     _fields_ = [("useLightCuts", C.c_int32), ("cut_kind", C.c_int32), ("clusterRefinementThreshold", C.c_float),
                 ("error_bound", C.c_float), ("photonRadiusScale", C.c_float), ("ar_kind", C.c_int32),
                 ("cone_half_angle", C.c_float), ("dist_clamp", C.c_float), ("precision", C.c_int32),
-                ("considerNormals", C.c_int32), ("model", C.c_void_p), ("profile", C.c_int32)]
+                ("considerNormals", C.c_int32), ("model", C.c_void_p), ("profile", C.c_int32),
+                ("ar_uncertain_factor", C.c_float), ("mlp_threshold", C.c_float), ("mlp_band", C.c_float),
+                ("cut_pool_entries", C.c_int64)]
 
 
 class ArcBox(C.Structure):
@@ -181,6 +184,8 @@ SIGNATURES = {
     "arc_mlp_forward": (_st, [_vp, _vp, C.c_int64, _vp]),
     "arc_mlp_gradients": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, P(C.c_float), P(C.c_float)]),
     "arc_mlp_train_step": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float, _vp]),
+    "arc_mlp_set_loss": (_st, [_vp, C.c_int32]),
+    "arc_mlp_get_loss": (C.c_int32, [_vp]),
     "arc_cut_training_samples": (_st, [_vp, _vp, P(ArcGBufferView), ArcFloat3, P(ArcGatherParams), P(ArcCutParams),
                                        C.c_float, _vp, _vp, _vp, C.c_int32, P(C.c_int32)]),
     "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),

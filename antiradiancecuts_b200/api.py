@@ -179,6 +179,7 @@ class AvplBvh:
             "range": d(v.range, np.int32, 2 * (n - 1)).reshape(-1, 2),
             "bounds": d(v.bounds, np.float32, 16 * (n - 1)).reshape(-1, 16),
             "records": d(v.records, np.float32, 16 * t).reshape(-1, 16),
+            "dirstat": d(v.dirstat, np.float32, 4 * t).reshape(-1, 4),
             "size": d(nd.size, np.int32, t),
             "materialIndex": d(nd.materialIndex, np.int32, t),
             "randomNumbers": d(nd.randomNumbers, np.float32, t),

@@ -161,6 +161,12 @@ void arc_run_config_default(ArcRunConfig* c) {
     c->ar_kind = ARC_AR_DISK;
     c->cone_half_angle = 30.0f * 3.14159265358979f / 180.0f;
     c->precision = ARC_PREC_KAHAN;
+    ArcCutParams cp;
+    arc_cut_params_default(&cp);
+    c->ar_uncertain_factor = cp.ar_uncertain_factor;
+    c->mlp_threshold = cp.mlp_threshold;
+    c->mlp_band = cp.mlp_band;
+    c->cut_pool_entries = cp.cut_pool_entries;
 }
 
 arc_status arc_context_create(int32_t device, void* cuda_stream, arc_context** out) {
@@ -463,6 +469,10 @@ arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcF
         cp.solid_angle_threshold = config->clusterRefinementThreshold;
         cp.error_bound = config->error_bound;
         cp.model = config->model;
+        cp.ar_uncertain_factor = config->ar_uncertain_factor;
+        cp.mlp_threshold = config->mlp_threshold;
+        cp.mlp_band = config->mlp_band;
+        cp.cut_pool_entries = config->cut_pool_entries;
         s = arc_gather_cut(ctx, tl_bvh, &d, gbuffer, camera_position, &gp, &cp, out);
     } else {
         if (prof) ARC_TRY_CUDA(cudaEventRecord(ev[2], ctx->stream));

@@ -536,13 +536,14 @@ __global__ void __launch_bounds__(64) cut_eval_kernel(EvalArgs a) {
         __syncthreads();
         for (int j = 0; j < cnt; ++j) {
             float g, ga;
-            pair_terms<AR, float>(srec[4 * j], srec[4 * j + 1], srec[4 * j + 2], srec[4 * j + 3], px, a.pc, g, ga);
-            px.r0 += srec[4 * j + 2].y * g;
-            px.r1 += srec[4 * j + 2].z * g;
-            px.r2 += srec[4 * j + 2].w * g;
-            px.a0 += srec[4 * j + 3].x * ga;
-            px.a1 += srec[4 * j + 3].y * ga;
-            px.a2 += srec[4 * j + 3].z * ga;
+            const float4* q = srec + 4 * j;
+            pair_terms<AR, float>(q[0], q[1], q[2], q[3], px, a.pc, g, ga);
+            px.r0 += q[2].y * g;
+            px.r1 += q[2].z * g;
+            px.r2 += q[2].w * g;
+            px.a0 += q[3].x * ga;
+            px.a1 += q[3].y * ga;
+            px.a2 += q[3].z * ga;
         }
         kahan_add(ss[0], sc[0], px.r0);
         kahan_add(ss[1], sc[1], px.r1);

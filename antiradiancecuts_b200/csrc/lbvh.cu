@@ -309,6 +309,7 @@ struct KarrasArgs {
     int32_t* range;
     float4* records;   // [2N-1][4]
     float4* cones;     // [2N-1][2] {normal axis, cos}, {direction axis, cos}
+    float4* dirstat;   // [2N-1] {S.xyz, a}: a = sum of antiradiance luminances, S = sum of a_i w_i / |w_i|
     float* bbox;       // [2N-1][6] scratch: leaf boxes then inner boxes
     ArcAvplBvhNodeDataParam nd;
     ArcFloat3* sorted_pos;
@@ -373,11 +374,14 @@ __global__ void __launch_bounds__(256) lbvh_karras(KarrasArgs k) {
     float4* c = k.cones + 2 * (size_t)i;
     c[0] = make_float4(nr.x, nr.y, nr.z, 1.0f);
     const float ww = rn_dot(w.x, w.y, w.z, w.x, w.y, w.z);
+    const float a_lum = rn_add(rn_add(rn_mul(0.2126f, A.x), rn_mul(0.7152f, A.y)), rn_mul(0.0722f, A.z));
     if (ww > 0.0f) {
         const float inv = rn_div(1.0f, rn_sqrt(ww));
         c[1] = make_float4(rn_mul(w.x, inv), rn_mul(w.y, inv), rn_mul(w.z, inv), 1.0f);
+        k.dirstat[i] = make_float4(rn_mul(a_lum, c[1].x), rn_mul(a_lum, c[1].y), rn_mul(a_lum, c[1].z), a_lum);
     } else {
         c[1] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        k.dirstat[i] = make_float4(0.0f, 0.0f, 0.0f, a_lum);
     }
     float* b = k.bbox + 6 * (size_t)i;
     b[0] = b[3] = p.x;
@@ -435,6 +439,7 @@ struct BottomUpArgs {
     int32_t* visit;
     float4* records;
     float4* cones;
+    float4* dirstat;
     float* bbox;
     float4* bounds;  // [N-1][4]
     ArcAvplBvhNodeDataParam nd;
@@ -497,11 +502,19 @@ __global__ void __launch_bounds__(256) lbvh_bottom_up(BottomUpArgs b) {
             N[3 * t + q] = ldcg(N + 3 * repr + q);
             W[3 * t + q] = ldcg(W + 3 * repr + q);
         }
-        // packed record: representative p/n/w, summed L' and A, count
+        // direction statistics, and the antiradiance representative: drawn in proportion to
+        // antiradiance luminance with the same random number; its direction is the record's w
+        const float4 dl = __ldcg(b.dirstat + l), dr = __ldcg(b.dirstat + r);
+        const float4 dt = make_float4(rn_add(dl.x, dr.x), rn_add(dl.y, dr.y), rn_add(dl.z, dr.z), rn_add(dl.w, dr.w));
+        b.dirstat[t] = dt;
+        const int arep = dt.w > 0.0f ? (rnd > rn_div(dl.w, dt.w) ? r : l) : repr;
+        // packed record: representative p/n, antiradiance representative's w, summed L' and A, count
         const float* R = reinterpret_cast<const float*>(b.records);
         float rt[16];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) rt[q] = ldcg(R + 16 * (size_t)repr + q);
+        for (int q = 0; q < 6; ++q) rt[q] = ldcg(R + 16 * (size_t)repr + q);
+#pragma unroll
+        for (int q = 6; q < 9; ++q) rt[q] = ldcg(R + 16 * (size_t)arep + q);
 #pragma unroll
         for (int q = 9; q < 15; ++q) rt[q] = rn_add(ldcg(R + 16 * (size_t)l + q), ldcg(R + 16 * (size_t)r + q));
         rt[15] = (float)(__ldcg(b.nd.size + l) + __ldcg(b.nd.size + r));
@@ -561,7 +574,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
 
     uint32_t *keys0, *keys1, *hist, *status, *bb;
     int32_t *vals0, *vals1, *left, *right, *parents, *range, *visit;
-    float4 *records, *cones, *bounds;
+    float4 *records, *cones, *bounds, *dirstat;
     float* bbox;
     ARC_TRY(get(bvh, "keys0", n, &keys0));
     ARC_TRY(get(bvh, "keys1", n, &keys1));
@@ -577,6 +590,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     ARC_TRY(get(bvh, "visit", n - 1, &visit));
     ARC_TRY(get(bvh, "records", (size_t)4 * total, &records));
     ARC_TRY(get(bvh, "cones", (size_t)2 * total, &cones));
+    ARC_TRY(get(bvh, "dirstat", total, &dirstat));
     ARC_TRY(get(bvh, "bounds", (size_t)4 * (n - 1), &bounds));
     ARC_TRY(get(bvh, "bbox", (size_t)6 * total, &bbox));
     ArcAvplBvhNodeDataParam nd;
@@ -659,6 +673,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     k.range = range;
     k.records = records;
     k.cones = cones;
+    k.dirstat = dirstat;
     k.bbox = bbox;
     k.nd = nd;
     k.sorted_pos = bvh->sorted_positions;
@@ -677,6 +692,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     bu.visit = visit;
     bu.records = records;
     bu.cones = cones;
+    bu.dirstat = dirstat;
     bu.bbox = bbox;
     bu.bounds = bounds;
     bu.nd = nd;
@@ -699,6 +715,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     v.bounds = reinterpret_cast<const float*>(bounds);
     v.records = reinterpret_cast<const float*>(records);
     v.node_data = nd;
+    v.dirstat = reinterpret_cast<const float*>(dirstat);
     bvh->has_reference_nodes = false;
     return ARC_OK;
 }

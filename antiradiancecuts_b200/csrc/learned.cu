@@ -41,6 +41,7 @@
 namespace arc {
 
 const float* mlp_params(const arc_mlp* m);
+int32_t mlp_loss_kind(const arc_mlp* m);
 
 namespace {
 
@@ -82,12 +83,12 @@ __device__ __forceinline__ void record_at(const float4* rec, float px, float py,
 }
 
 // The 16 features of (tile, inner node).  Every input is known at selection time: the tile's
-// geometry and coarse estimate (mean), the node's bounds / cones / record, the records of its two
-// children (a one-level lookahead at the tile centre), its depth, and the analytic bound M against
-// tau.
+// geometry and coarse estimate (mean), the node's bounds / cones / record / direction statistics,
+// the records of its two children (a one-level lookahead at the tile centre), its depth, and the
+// analytic bound M against tau.
 __device__ __forceinline__ void node_features(const TileInfo& t, float mean, const NodeGeom& g, float M, float4 nc,
                                               float4 wc, const float4* rec, const float4* rec_l, const float4* rec_r,
-                                              int depth, float clamp2, float cos_thr, float* f) {
+                                              float4 ds, int depth, float clamp2, float cos_thr, float* f) {
     const float E = fmaxf(mean, 1e-30f);
     const float4 q2 = rec[2], q3 = rec[3];
     const float Ls = lum3(q2.y, q2.z, q2.w), As = lum3(q3.x, q3.y, q3.z);
@@ -123,7 +124,9 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
     f[12] = clampf(safe_log2(fabsf(rad - radl - radr) * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
     f[13] = clampf(safe_log2(fabsf(ar - arl - arr) * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
     f[14] = depth * (1.0f / 32.0f);
-    f[15] = clampf(safe_log2(rad * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    // mean resultant length of the antiradiance directions, in [-1, 1]
+    const float sl = sqrtf(ds.x * ds.x + ds.y * ds.y + ds.z * ds.z);
+    f[15] = ds.w > 0.0f ? clampf(2.0f * __fdividef(sl, ds.w) - 1.0f, -1.0f, 1.0f) : -1.0f;
 }
 
 __device__ __forceinline__ void store_features(__nv_bfloat16* row, const float* f) {
@@ -150,6 +153,7 @@ struct LevelArgs {
     int n;
     const float4* bounds;
     const float4* records;
+    const float4* dirstat;
     const float4* info;
     BoundParams bp;
     const int2* in;         // {tile, node | depth << 26}
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 if (action == kScore) {
                     float f[kFeat];
                     node_features(ti, mean, g, M, nc, wc, a.records + 4 * (size_t)node, a.records + 4 * (size_t)lc,
-                                  a.records + 4 * (size_t)rc, depth, a.clamp2, a.cos_thr, f);
+                                  a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
                     const int slot = atomicAdd(&s_staged, 1);  // < 256: at most 127 rows are left over
                     uint4 x0, x1;
                     x0.x = mlp::pack2(f[0], f[1]);
@@ -477,6 +481,7 @@ struct LabelArgs {
     int n;
     const float4* bounds;
     const float4* records;
+    const float4* dirstat;
     const float4* info;
     BoundParams bp;
     PairConsts pc;
@@ -540,17 +545,46 @@ __device__ __forceinline__ bool load_pixel(const LabelArgs& a, int tile, int p, 
     return true;
 }
 
+// The prefix sums are built in segments of seg_len leaves so that every (tile, segment) pair is
+// its own CTA: label_segment_sums totals each segment, label_segment_scan turns the totals into
+// each segment's starting value (per tile and pixel, in segment order), and label_prefix writes
+// the running sums from there.
 template <int AR>
-__global__ void __launch_bounds__(64) label_prefix(LabelArgs a) {
-    const int b = blockIdx.x, p = threadIdx.x;
-    const int tile = a.tile0 + b;
+__global__ void __launch_bounds__(64) label_segment_sums(LabelArgs a, int seg_len, double* seg) {
+    const int b = blockIdx.x, s = blockIdx.y, p = threadIdx.x;
     Pixel<float> px;
     float kd[3];
-    const bool valid = load_pixel(a, tile, p, px, kd);
-    double* P = a.prefix + (size_t)b * (a.n + 1) * 64;
+    const bool valid = load_pixel(a, a.tile0 + b, p, px, kd);
     double run = 0.0;
-    P[p] = 0.0;
-    for (int i = 0; i < a.n; ++i) {
+    const int i1 = min(a.n, (s + 1) * seg_len);
+    if (valid)
+        for (int i = s * seg_len; i < i1; ++i)
+            run += (double)record_lum<AR>(a.records + 4 * (size_t)i, px, kd, a.pc, a.disk_scale);
+    seg[((size_t)b * gridDim.y + s) * 64 + p] = run;
+}
+
+__global__ void label_segment_scan(double* seg, int nseg) {
+    const int b = blockIdx.x, p = threadIdx.x;
+    double run = 0.0;
+    for (int s = 0; s < nseg; ++s) {
+        double* v = seg + ((size_t)b * nseg + s) * 64 + p;
+        const double t = *v;
+        *v = run;
+        run += t;
+    }
+}
+
+template <int AR>
+__global__ void __launch_bounds__(64) label_prefix(LabelArgs a, int seg_len, const double* seg) {
+    const int b = blockIdx.x, s = blockIdx.y, p = threadIdx.x;
+    Pixel<float> px;
+    float kd[3];
+    const bool valid = load_pixel(a, a.tile0 + b, p, px, kd);
+    double* P = a.prefix + (size_t)b * (a.n + 1) * 64;
+    double run = seg[((size_t)b * gridDim.y + s) * 64 + p];
+    if (s == 0) P[p] = 0.0;
+    const int i1 = min(a.n, (s + 1) * seg_len);
+    for (int i = s * seg_len; i < i1; ++i) {
         if (valid) run += (double)record_lum<AR>(a.records + 4 * (size_t)i, px, kd, a.pc, a.disk_scale);
         P[(size_t)(i + 1) * 64 + p] = run;
     }
@@ -630,7 +664,8 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
             const int r = atomicAdd(a.count, 1);
             if (r < a.capacity) {
                 float f[kFeat];
-                node_features(t, mean, g, M, nc, wc, rec, a.records + 4 * (size_t)c0, a.records + 4 * (size_t)c1, depth,
+                node_features(t, mean, g, M, nc, wc, rec, a.records + 4 * (size_t)c0, a.records + 4 * (size_t)c1,
+                              a.dirstat[node], depth,
                               a.bp.clamp2, a.bp.cos_thr, f);
                 store_features(a.feats + (size_t)r * kFeat, f);
                 a.labels[r] = refine ? 1.0f : 0.0f;
@@ -675,7 +710,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     // capacities: frontier / rows per level and accepted pairs over the whole walk
     ARC_CHECK_ARG(2 * n - 1 < (1 << 26), "learned cut supports trees of up to 2^25 leaves");
     // frontier capacity per level
-    const int cap = (int)std::min<int64_t>((int64_t)tiles * 8192 + (1 << 20), 1 << 30);
+    const int cap = (int)std::min<int64_t>((int64_t)tiles * 16384 + (1 << 20), 1 << 30);
     const int acc_cap = (int)std::min<int64_t>((int64_t)pool.num_chunks * kChunk, (int64_t)INT32_MAX);
     int2 *fa, *fb;
     int2* accepted;
@@ -702,6 +737,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.n = n;
     la.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
     la.records = reinterpret_cast<const float4*>(bvh->view.records);
+    la.dirstat = reinterpret_cast<const float4*>(bvh->view.dirstat);
     la.info = info;
     la.bp = bound_params(gp, cp);
     la.capacity = cap;
@@ -709,7 +745,10 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     unsigned char* img;
     ARC_TRY(arena_get(ctx, "lc_weight_image", mlp::kImageBytes, &img));
     la.weight_image = img;
-    la.thr_logit = p <= 0.0f ? -INFINITY : (p >= 1.0f ? INFINITY : logf(p / (1.0f - p)));
+    if (mlp_loss_kind(cp->model) == ARC_MLP_LOSS_SQUARED)  // output: log2 of the relative node error
+        la.thr_logit = p <= 0.0f ? -INFINITY : log2f(p);
+    else  // output: logit of the refine probability
+        la.thr_logit = p <= 0.0f ? -INFINITY : (p >= 1.0f ? INFINITY : logf(p / (1.0f - p)));
     la.accepted = accepted;
     la.acc_count = counters + 3;
     la.acc_capacity = acc_cap;
@@ -805,9 +844,13 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     const int n = bvh->n;
     float4* info = nullptr;
     ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info));
-    // batch of tiles whose FP64 prefixes fit in ~4 GB
+    // batch of tiles whose FP64 prefixes fit in ~8 GB
     const size_t per_tile = (size_t)(n + 1) * 64 * sizeof(double);
-    const int batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)tiles, ((size_t)4 << 30) / per_tile));
+    const int batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)tiles, ((size_t)8 << 30) / per_tile));
+    const int seg_len = 4096, nseg = (n + seg_len - 1) / seg_len;
+    double* seg = nullptr;
+    ARC_TRY(ctx->arena.get("label_segments", (size_t)batch * nseg * 64 * sizeof(double),
+                           reinterpret_cast<void**>(&seg)));
     double* prefix = nullptr;
     ARC_TRY(ctx->arena.get("label_prefix", per_tile * batch, reinterpret_cast<void**>(&prefix)));
     int* dcount = nullptr;
@@ -824,6 +867,7 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     a.n = n;
     a.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
     a.records = reinterpret_cast<const float4*>(bvh->view.records);
+    a.dirstat = reinterpret_cast<const float4*>(bvh->view.dirstat);
     a.info = info;
     a.bp = bound_params(gp, cp);
     a.pc.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
@@ -845,17 +889,24 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     for (int t0 = 0; t0 < tiles; t0 += batch) {
         a.tile0 = t0;
         a.batch = std::min(batch, tiles - t0);
+        const dim3 g2(a.batch, nseg);
         switch (gp->ar_kind) {
             case 0:
-                label_prefix<0><<<a.batch, 64, 0, st>>>(a);
+                label_segment_sums<0><<<g2, 64, 0, st>>>(a, seg_len, seg);
+                label_segment_scan<<<a.batch, 64, 0, st>>>(seg, nseg);
+                label_prefix<0><<<g2, 64, 0, st>>>(a, seg_len, seg);
                 label_traverse<0><<<a.batch, 32, 0, st>>>(a, bvh->view.range);
                 break;
             case 1:
-                label_prefix<1><<<a.batch, 64, 0, st>>>(a);
+                label_segment_sums<1><<<g2, 64, 0, st>>>(a, seg_len, seg);
+                label_segment_scan<<<a.batch, 64, 0, st>>>(seg, nseg);
+                label_prefix<1><<<g2, 64, 0, st>>>(a, seg_len, seg);
                 label_traverse<1><<<a.batch, 32, 0, st>>>(a, bvh->view.range);
                 break;
             default:
-                label_prefix<2><<<a.batch, 64, 0, st>>>(a);
+                label_segment_sums<2><<<g2, 64, 0, st>>>(a, seg_len, seg);
+                label_segment_scan<<<a.batch, 64, 0, st>>>(seg, nseg);
+                label_prefix<2><<<g2, 64, 0, st>>>(a, seg_len, seg);
                 label_traverse<2><<<a.batch, 32, 0, st>>>(a, bvh->view.range);
                 break;
         }

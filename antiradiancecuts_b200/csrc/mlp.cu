@@ -52,6 +52,7 @@ struct Args {
     float loss_scale;         // 1 / sum of weights
     float* grads;             // [kParams] (atomicAdd)
     float* loss;              // [1]
+    int loss_kind;            // arc_mlp_loss
     uint32_t* err;
 };
 
@@ -285,9 +286,15 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         if (valid) {
             const float lab = a.labels[row];
             const float wgt = a.weights ? a.weights[row] : 1.0f;
-            const float p = 1.0f / (1.0f + expf(-y));
-            dy = wgt * (p - lab) * a.loss_scale;
-            l = wgt * (fmaxf(y, 0.0f) - y * lab + log1pf(expf(-fabsf(y)))) * a.loss_scale;
+            if (a.loss_kind == ARC_MLP_LOSS_SQUARED) {
+                const float d = y - lab;
+                dy = wgt * 2.0f * d * a.loss_scale;
+                l = wgt * d * d * a.loss_scale;
+            } else {
+                const float p = 1.0f / (1.0f + expf(-y));
+                dy = wgt * (p - lab) * a.loss_scale;
+                l = wgt * (fmaxf(y, 0.0f) - y * lab + log1pf(expf(-fabsf(y)))) * a.loss_scale;
+            }
         }
         {
             const float ls = warp_sum(l), ds = warp_sum(dy);
@@ -417,6 +424,7 @@ struct arc_mlp {
     float* adam_v = nullptr;
     float* loss = nullptr;
     int64_t step = 0;
+    int32_t loss_kind = ARC_MLP_LOSS_BCE;
 };
 
 namespace {
@@ -434,6 +442,7 @@ arc_status mlp_launch(arc_mlp* m, bool train, const void* x, int64_t rows, float
     a.loss_scale = loss_scale;
     a.grads = m->grads;
     a.loss = m->loss;
+    a.loss_kind = m->loss_kind;
     a.err = ctx->d_error;
     const int64_t tiles = (rows + mlp::kRows - 1) / mlp::kRows;
     if (tiles == 0) return ARC_OK;
@@ -468,6 +477,7 @@ arc_status mlp_launch(arc_mlp* m, bool train, const void* x, int64_t rows, float
 
 namespace arc {
 const float* mlp_params(const arc_mlp* m) { return m->params; }
+int32_t mlp_loss_kind(const arc_mlp* m) { return m->loss_kind; }
 arc_status mlp_forward_device(arc_mlp* m, const void* x, int64_t rows, float* logits) {
     return mlp_launch(m, false, x, rows, logits, nullptr, nullptr, 0.0f);
 }
@@ -563,6 +573,15 @@ arc_status arc_mlp_gradients(arc_mlp* m, const void* features_bf16, const float*
     ARC_TRY_CUDA(cudaMemsetAsync(m->grads, 0, sizeof(float) * mlp::kParams, m->ctx->stream));
     return ARC_OK;
 }
+
+arc_status arc_mlp_set_loss(arc_mlp* m, int32_t kind) {
+    ARC_CHECK_ARG(m, "NULL model");
+    ARC_CHECK_ARG(kind == ARC_MLP_LOSS_BCE || kind == ARC_MLP_LOSS_SQUARED, "unknown loss");
+    m->loss_kind = kind;
+    return ARC_OK;
+}
+
+int32_t arc_mlp_get_loss(const arc_mlp* m) { return m ? m->loss_kind : -1; }
 
 arc_status arc_mlp_train_step(arc_mlp* m, const void* features_bf16, const float* labels, const float* weights,
                               int64_t rows, float weight_sum, float lr, float* device_loss_accum) {

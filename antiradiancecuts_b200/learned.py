@@ -3,11 +3,15 @@
     python -m antiradiancecuts_b200.learned train [--scenes 64] [--samples 20000000] [--out PATH]
 
 Training data come from the exact gather itself: for each training scene (room variants with
-seeds 100..163: 0-16 random boxes, random light position and wall albedo) the GPU walks every
-8x8 tile's tree with the exact refine/accept decision and records the features, label and error
-of every node the analytic bound cannot decide (arc_cut_training_samples).  The network is then
-trained on the GPU by the library's own tensor-core forward/backward kernels (arc_mlp_train_step,
-Adam, weighted binary cross-entropy).
+seeds 100..163: 0-16 random boxes, random light position and wall albedo) rendered at the
+evaluation scale (1920x1080 G-buffer, 1,048,576 AVPLs), the GPU walks the trees of the 8x8 tiles in
+a few seeded 64x64-pixel windows with the exact refine/accept decision and records the features,
+label and error of every node the selection would score (arc_cut_training_samples).  The network
+is then trained on the GPU by the library's own tensor-core forward/backward kernels
+(arc_mlp_train_step, Adam) as a classifier of the 0/1 labels (weighted binary cross-entropy); the
+selection refines a node when the predicted probability reaches the threshold.  A regression of
+log2 of each node's exact relative error (squared loss; refine when the predicted error reaches
+the threshold) is the alternative objective.
 """
 from __future__ import annotations
 
@@ -24,31 +28,48 @@ from . import _lib as L
 from . import api, scene
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_MODEL = os.path.join(PKG, "models", "cutnet.npy")
+DEFAULT_MODEL = os.path.join(PKG, "models", "cutnet.npz")
 NUM_PARAMS = 9473
 
 # training set-up (the learned-cut configuration)
 TRAIN_SEEDS = range(100, 164)
-TRAIN_W, TRAIN_H, TRAIN_AVPLS = 256, 192, 65536
-LABEL_DELTA = 1.5e-4  # refine when the node's true error exceeds this fraction of the tile value
+TRAIN_W, TRAIN_H, TRAIN_AVPLS = 1920, 1080, 1 << 20
+TRAIN_CROPS, TRAIN_CROP = 16, 32  # windows per scene and their size in pixels
+LABEL_DELTA = 1e-4  # label: refine when the node's true error exceeds this fraction of the tile value
+LOG2_FLOOR = -30.0  # regression targets: log2 of the relative error, at least this
 # analytic pre-acceptance shared by labelling and selection: nodes whose error bound is within
 # PREACCEPT_EPS of the tile estimate (antiradiance-uncertain nodes weighted by PREACCEPT_K) are
-# accepted without the network; the network decides every other node
-PREACCEPT_EPS = 1e-3
-PREACCEPT_K = 64.0
+# accepted, nodes whose bound exceeds PREACCEPT_BAND times that are refined, both without the
+# network; the network decides the nodes in between (it prunes refinements of the analytic cut)
+PREACCEPT_EPS = 2e-3
+PREACCEPT_K = 16.0
+PREACCEPT_BAND = 16.0
 
 
 class Model:
-    """An arc_mlp handle with its parameters."""
+    """An arc_mlp handle with its parameters, its loss (L.ARC_MLP_LOSS_*) and the selection
+    threshold recommended for it (probability for a classifier, relative error for a regressor)."""
 
-    def __init__(self, ctx: api.Context, params: np.ndarray | None = None, seed: int = 1):
+    def __init__(self, ctx: api.Context, params: np.ndarray | None = None, seed: int = 1,
+                 loss: int = L.ARC_MLP_LOSS_BCE, threshold: float | None = None):
         self.ctx = ctx
         h = C.c_void_p()
         L.check(ctx.lib.arc_mlp_create(ctx.handle, seed, C.byref(h)), "arc_mlp_create")
         self.handle = h
         ctx._children.add(self)
+        L.check(ctx.lib.arc_mlp_set_loss(h, int(loss)), "arc_mlp_set_loss")
+        self.loss = int(loss)
+        self.threshold = threshold if threshold is not None else (0.5 if loss == L.ARC_MLP_LOSS_BCE else 1e-4)
         if params is not None:
             self.set_params(params)
+
+    def save(self, path: str) -> None:
+        np.savez(path, params=self.params(), loss=np.int32(self.loss), threshold=np.float32(self.threshold))
+
+    @classmethod
+    def load(cls, ctx: api.Context, path: str) -> "Model":
+        z = np.load(path)
+        return cls(ctx, z["params"], loss=int(z["loss"]), threshold=float(z["threshold"]))
 
     def set_params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, np.float32)
@@ -69,21 +90,25 @@ class Model:
         self.handle = None
 
 
-def cut_params(model: Model, threshold: float = 0.5, **kw):
+def cut_params(model: Model, threshold: float | None = None, **kw):
     """ArcCutParams of the learned cut with the pre-acceptance the model was trained with."""
+    kw.setdefault("mlp_band", PREACCEPT_BAND)
     return api.cut_params(L.ARC_CUT_LEARNED, error_bound=PREACCEPT_EPS, ar_uncertain_factor=PREACCEPT_K,
-                          model=model.handle.value, mlp_threshold=threshold, **kw)
+                          model=model.handle.value,
+                          mlp_threshold=model.threshold if threshold is None else threshold, **kw)
 
 
 def load_default_model(ctx: api.Context, path: str = DEFAULT_MODEL) -> Model:
     if not os.path.exists(path):
         raise FileNotFoundError(f"no trained cut model at {path}")
-    return Model(ctx, np.load(path))
+    return Model.load(ctx, path)
 
 
 def scene_samples(ctx: api.Context, seed: int, capacity: int, width=TRAIN_W, height=TRAIN_H, num_avpls=TRAIN_AVPLS,
-                  delta=LABEL_DELTA, error_bound=PREACCEPT_EPS, ar_uncertain=PREACCEPT_K):
-    """(features bf16 [k,16], labels [k], errors [k]) torch CUDA tensors for one training scene."""
+                  delta=LABEL_DELTA, error_bound=PREACCEPT_EPS, ar_uncertain=PREACCEPT_K, band=PREACCEPT_BAND,
+                  crops=TRAIN_CROPS, crop=TRAIN_CROP):
+    """(features bf16 [k,16], labels [k], errors [k]) torch CUDA tensors for one training scene: the
+    tiles of `crops` seeded crop x crop windows of the width x height G-buffer (crops=0: all of it)."""
     import torch
 
     desc = scene.scene_desc(L.ARC_SCENE_TRAIN_VARIANT, seed)
@@ -96,35 +121,54 @@ def scene_samples(ctx: api.Context, seed: int, capacity: int, width=TRAIN_W, hei
     bvh.build(dv)
     gb = api.GBuffer(pos, nrm)
     prm = api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
-    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=error_bound, ar_uncertain_factor=ar_uncertain)
+    cut = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=error_bound, ar_uncertain_factor=ar_uncertain,
+                         mlp_band=band)
     feats = torch.empty((capacity, 16), dtype=torch.bfloat16, device="cuda")
     labels = torch.empty(capacity, dtype=torch.float32, device="cuda")
     errs = torch.empty(capacity, dtype=torch.float32, device="cuda")
-    count = C.c_int32()
     cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
-    gv = gb.view()
-    L.check(ctx.lib.arc_cut_training_samples(ctx.handle, bvh.handle, C.byref(gv), L.f3(cam), C.byref(prm), C.byref(cut),
-                                             delta, C.c_void_p(feats.data_ptr()), C.c_void_p(labels.data_ptr()),
-                                             C.c_void_p(errs.data_ptr()), capacity, C.byref(count)),
-            "arc_cut_training_samples")
-    word = ctx.synchronize()
-    if word:
-        raise RuntimeError(f"device error word 0x{word:x} while labelling scene {seed}")
-    k = count.value
+    full = gb.view()
+    if crops:
+        rng = np.random.default_rng(seed)
+        # windows on the 8-pixel tile grid, inside the image
+        xs = rng.integers(0, (width - crop) // 8 + 1, crops) * 8
+        ys = rng.integers(0, (height - crop) // 8 + 1, crops) * 8
+        views = [L.ArcGBufferView(full.position + 16 * (int(y) * width + int(x)), full.normal + 16 * (int(y) * width + int(x)),
+                                  crop, crop, width) for x, y in zip(xs, ys)]
+    else:
+        views = [full]
+    k = 0
+    for gv in views:
+        count = C.c_int32()
+        o = k
+        L.check(ctx.lib.arc_cut_training_samples(ctx.handle, bvh.handle, C.byref(gv), L.f3(cam), C.byref(prm),
+                                                 C.byref(cut), delta, C.c_void_p(feats[o:].data_ptr()),
+                                                 C.c_void_p(labels[o:].data_ptr()), C.c_void_p(errs[o:].data_ptr()),
+                                                 capacity - o, C.byref(count)), "arc_cut_training_samples")
+        word = ctx.synchronize()
+        if word:
+            raise RuntimeError(f"device error word 0x{word:x} while labelling scene {seed}")
+        k = min(capacity, o + count.value)
+        if k >= capacity:
+            break
     bvh.close()
     return feats[:k].clone(), labels[:k].clone(), errs[:k].clone()
 
 
 def train(ctx: api.Context, feats, labels, epochs: float = 3.0, batch: int = 8192, lr: float = 2e-3,
-          pos_weight: float = 2.0, seed: int = 1, log=print) -> Model:
-    """Adam on the weighted BCE (refine samples weighted pos_weight) with a cosine learning rate."""
+          pos_weight: float = 2.0, seed: int = 1, log=print, loss: int = L.ARC_MLP_LOSS_BCE) -> Model:
+    """Adam with a cosine learning rate on the weighted BCE of 0/1 labels (refine samples weighted
+    pos_weight), or on the squared error of real-valued labels."""
     import torch
 
-    model = Model(ctx, seed=seed)
+    model = Model(ctx, seed=seed, loss=loss)
     n = feats.shape[0]
     steps = max(1, int(epochs * n / batch))
     g = torch.Generator(device="cuda").manual_seed(seed)
-    weights = torch.where(labels > 0.5, torch.full_like(labels, pos_weight), torch.ones_like(labels))
+    if loss == L.ARC_MLP_LOSS_BCE:
+        weights = torch.where(labels > 0.5, torch.full_like(labels, pos_weight), torch.ones_like(labels))
+    else:
+        weights = torch.ones_like(labels)
     loss_acc = torch.zeros(1, device="cuda")
     t0 = time.time()
     perm = torch.randperm(n, device="cuda", generator=g)
@@ -149,19 +193,26 @@ def train(ctx: api.Context, feats, labels, epochs: float = 3.0, batch: int = 819
     return model
 
 
-def evaluate(ctx: api.Context, model: Model, feats, labels):
+def evaluate(ctx: api.Context, model: Model, feats, labels, delta: float = LABEL_DELTA):
+    """Decision quality on held-out rows: for a regressor, `labels` are log2 relative errors and
+    the decision is "error >= delta"; also the regression's RMS error in log2 units."""
     import torch
 
     logits = torch.empty(feats.shape[0], device="cuda")
     model.forward(feats, logits)
     ctx.synchronize()
-    pred = logits > 0
-    lab = labels > 0.5
+    extra = {}
+    if model.loss == L.ARC_MLP_LOSS_SQUARED:
+        t = math.log2(delta)
+        pred, lab = logits >= t, labels >= t
+        extra["rms_log2"] = float(torch.sqrt(torch.mean((logits - labels) ** 2)).item())
+    else:
+        pred, lab = logits > 0, labels > 0.5
     acc = (pred == lab).float().mean().item()
     fn = (~pred & lab).float().sum().item() / max(1.0, lab.float().sum().item())
     fp = (pred & ~lab).float().sum().item() / max(1.0, (~lab).float().sum().item())
     return {"accuracy": acc, "missed_refine_rate": fn, "extra_refine_rate": fp, "rows": int(feats.shape[0]),
-            "refine_fraction": lab.float().mean().item()}
+            "refine_fraction": lab.float().mean().item(), **extra}
 
 
 def main(argv=None):
@@ -172,24 +223,29 @@ def main(argv=None):
     tr.add_argument("--samples", type=int, default=20_000_000)
     tr.add_argument("--epochs", type=float, default=3.0)
     tr.add_argument("--delta", type=float, default=LABEL_DELTA)
+    tr.add_argument("--objective", choices=["regression", "classification"], default="classification")
+    tr.add_argument("--threshold", type=float, default=None, help="selection threshold stored with the model")
     tr.add_argument("--out", default=DEFAULT_MODEL)
     a = ap.parse_args(argv)
     import torch
 
     ctx = api.Context(0)
+    regress = a.objective == "regression"
     per_scene = max(1, a.samples // a.scenes)
     fs, ls = [], []
     t0 = time.time()
     seeds = list(TRAIN_SEEDS)[: a.scenes]
     for s in seeds:
-        f, l, e = scene_samples(ctx, s, capacity=4 * per_scene, delta=a.delta)
+        f, l, e = scene_samples(ctx, s, capacity=24 * per_scene, delta=a.delta)
+        if regress:
+            l = torch.log2(torch.clamp(e, min=2.0 ** LOG2_FLOOR))
         if f.shape[0] > per_scene:  # uniform subsample to the per-scene budget
             keep = torch.randperm(f.shape[0], device="cuda")[:per_scene]
             f, l = f[keep], l[keep]
         fs.append(f)
         ls.append(l)
-        print(f"scene {s}: {f.shape[0]} samples, refine fraction {l.mean().item():.3f} ({time.time() - t0:.1f} s)",
-              flush=True)
+        stat = f"mean log2 error {l.mean().item():.2f}" if regress else f"refine fraction {l.mean().item():.3f}"
+        print(f"scene {s}: {f.shape[0]} samples, {stat} ({time.time() - t0:.1f} s)", flush=True)
     feats = torch.cat(fs)
     labels = torch.cat(ls)
     # hold out 2% for a validation report
@@ -197,10 +253,13 @@ def main(argv=None):
     perm = torch.randperm(n, device="cuda")
     nv = max(1, n // 50)
     val, trn = perm[:nv], perm[nv:]
-    model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs)
-    print("validation:", evaluate(ctx, model, feats[val].contiguous(), labels[val].contiguous()), flush=True)
-    os.makedirs(os.path.dirname(a.out), exist_ok=True)
-    np.save(a.out, model.params())
+    loss = L.ARC_MLP_LOSS_SQUARED if regress else L.ARC_MLP_LOSS_BCE
+    model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs, loss=loss)
+    if a.threshold is not None:
+        model.threshold = a.threshold
+    print("validation:", evaluate(ctx, model, feats[val].contiguous(), labels[val].contiguous(), a.delta), flush=True)
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    model.save(a.out)
     print("saved", a.out, f"({time.time() - t0:.1f} s total)")
     return 0
 

@@ -293,6 +293,11 @@ typedef struct ArcLbvhView {
     const float* bounds;
     const float* records;
     ArcAvplBvhNodeDataParam node_data;
+    /* [2N-1][4] per node {S.xyz, a}: a = sum over its AVPLs of the antiradiance luminance a_i,
+       S = sum of a_i * w_i / |w_i|.  An inner node's packed-record direction w is that of an
+       antiradiance representative drawn in proportion to a (w only enters the antiradiance
+       cone test); |S| / a measures how concentrated its directions are. */
+    const float* dirstat;
 } ArcLbvhView;
 
 typedef struct arc_lbvh arc_lbvh;
@@ -331,7 +336,9 @@ typedef struct ArcCutParams {
     int32_t max_cut_nodes;       /* per-tile cut capacity, default 2^20 (ARC_DEVERR_CUT_OVERFLOW beyond it) */
     int64_t cut_pool_entries;    /* total cut entries over all tiles; 0 = 65536 per tile */
     const arc_mlp* model;        /* LEARNED only */
-    float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this */
+    float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this (BCE model), or
+                                    when the predicted relative node error >= this (squared-loss model
+                                    regressing log2 of the error) */
     float mlp_band;              /* LEARNED: nodes whose error bound exceeds mlp_band times the tile's error
                                     budget are refined without the network (default 4096; 0 = no limit) */
     int32_t debug_pixel_x;       /* SOLID_ANGLE scene probe (cudaGather.cu:338, 392-396); -1 = off */
@@ -369,7 +376,14 @@ arc_status arc_last_cut(arc_context* ctx, ArcCutLists* out);
 /* 16 -> 64 -> 64 -> 64 -> 1 multilayer perceptron with GELU activations: BF16 weights and
  * activations on the tensor cores (tcgen05), FP32 accumulation, FP32 master parameters
  * (layout: W1[64][16], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4).  Features
- * are BF16 rows of 16 values (16-byte aligned); the output is the logit of "refine this node". */
+ * are BF16 rows of 16 values (16-byte aligned).  What the output means follows the model's loss:
+ * ARC_MLP_LOSS_BCE (default): the logit of "refine this node" (labels 0 / 1);
+ * ARC_MLP_LOSS_SQUARED: a regression of the label value, for the learned cut log2 of the node's
+ * error relative to the tile value. */
+typedef enum arc_mlp_loss {
+    ARC_MLP_LOSS_BCE = 0,    /* weighted binary cross-entropy on the logit */
+    ARC_MLP_LOSS_SQUARED = 1 /* weighted squared error */
+} arc_mlp_loss;
 int32_t arc_mlp_num_params(void);
 arc_status arc_mlp_create(arc_context* ctx, uint64_t seed, arc_mlp** out);
 arc_status arc_mlp_destroy(arc_mlp* mlp);
@@ -377,11 +391,14 @@ arc_status arc_mlp_set_params(arc_mlp* mlp, const float* host_params, int32_t nu
 arc_status arc_mlp_get_params(arc_mlp* mlp, float* host_params, int32_t num);
 /* logits[rows] = MLP(features[rows][16]) (device pointers, enqueued on the context's stream). */
 arc_status arc_mlp_forward(arc_mlp* mlp, const void* features_bf16, int64_t rows, float* logits);
-/* Weighted binary cross-entropy gradient of the whole batch (sum(w * bce) / weight_sum) into
+/* Gradient of the whole batch's weighted loss (sum(w * loss) / weight_sum) into
  * host_grads[num params] and host_loss; waits for the stream.  labels / weights: device arrays
  * (weights may be NULL = 1). */
 arc_status arc_mlp_gradients(arc_mlp* mlp, const void* features_bf16, const float* labels, const float* weights,
                              int64_t rows, float weight_sum, float* host_grads, float* host_loss);
+/* Loss used by arc_mlp_gradients / arc_mlp_train_step, and the meaning of the output (above). */
+arc_status arc_mlp_set_loss(arc_mlp* mlp, int32_t kind);
+int32_t arc_mlp_get_loss(const arc_mlp* mlp);
 /* One Adam step (beta 0.9 / 0.999) on the batch's gradient; device_loss_accum (optional, device
  * float) accumulates the batch loss.  Enqueued only. */
 arc_status arc_mlp_train_step(arc_mlp* mlp, const void* features_bf16, const float* labels, const float* weights,
@@ -416,6 +433,11 @@ typedef struct ArcRunConfig {
     int32_t considerNormals;
     const arc_mlp* model;
     int32_t profile; /* print per-stage CUDA-event timings, as run(..., profile) */
+    /* cut details (ArcCutParams fields of the same names) */
+    float ar_uncertain_factor;
+    float mlp_threshold;
+    float mlp_band;
+    int64_t cut_pool_entries;
 } ArcRunConfig;
 
 void arc_run_config_default(ArcRunConfig* c);

@@ -56,15 +56,21 @@ def forward(p, x):
     return y, (x, z1, h1, z2, h2, z3, h3)
 
 
-def loss_and_grad(p, x, labels, weights=None):
-    """sum(w * bce(y, label)) / sum(w) and its gradient w.r.t. the parameters."""
+def loss_and_grad(p, x, labels, weights=None, loss="bce"):
+    """sum(w * loss(y, label)) / sum(w) and its gradient w.r.t. the parameters; loss "bce"
+    (binary cross-entropy on the logit y) or "squared" ((y - label)^2)."""
     y, (x, z1, h1, z2, h2, z3, h3) = forward(p, x)
     lab = np.asarray(labels, np.float64)
     w = np.ones_like(lab) if weights is None else np.asarray(weights, np.float64)
     ws = w.sum()
-    loss = float(np.sum(w * (np.maximum(y, 0) - y * lab + np.log1p(np.exp(-np.abs(y))))) / ws)
     P = unpack(p)
-    dy = w * (1.0 / (1.0 + np.exp(-y)) - lab) / ws
+    if loss == "squared":
+        loss_v = float(np.sum(w * (y - lab) ** 2) / ws)
+        dy = w * 2.0 * (y - lab) / ws
+    else:
+        loss_v = float(np.sum(w * (np.maximum(y, 0) - y * lab + np.log1p(np.exp(-np.abs(y))))) / ws)
+        dy = w * (1.0 / (1.0 + np.exp(-y)) - lab) / ws
+    loss = loss_v
     g = {"w4": h3.T @ dy, "b4": np.array([dy.sum()])}
     dz3 = np.outer(dy, P["w4"]) * gelu_grad(z3)
     g["W3"], g["b3"] = dz3.T @ h2, dz3.sum(0)

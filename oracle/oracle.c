@@ -565,14 +565,19 @@ static void cone_union(const float* a1, float c1, const float* a2, float c2, flo
  * Per node j in 0..2N-2 (leaf i -> i, inner k -> N+k):
  *   size, materialIndex, randomNumbers, position, normal, incRadiance (raw sum of L), incDirection
  *   records[16j..] {p.xyz, n.x}, {n.y, n.z, w.x, w.y}, {w.z, L'.rgb}, {A.rgb, count}
+ *   dirstat[4j..]  {S.xyz, a}: a = sum of the antiradiance luminances a_i, S = sum of a_i w_i/|w_i|
  * The representative is left or right by rand(N+k) > |L_l| / (|L_l| + |L_r|), rand from the
  * counter-based PCG32 stream (seed, N+k).  L' = L * (0.318309886 * diffuse) of the AVPL's
- * material, or L when w = 0 (the light-source case of getRadiance).
+ * material, or L when w = 0 (the light-source case of getRadiance).  The record's direction w is
+ * that of a second representative drawn in proportion to antiradiance luminance,
+ * rand(N+k) > a_l / (a_l + a_r), since w only enters the antiradiance cone test (the node-data
+ * incDirection keeps the radiance representative's, as the reference's cluster() does).
  */
 OR_EXPORT void oracle_bottom_up(int32_t n, const float* pos, const float* nrm, const float* w, const float* L,
                                 const float* A, const int32_t* mat, const float* diffuse, const int32_t* left,
                                 const int32_t* right, uint32_t seed, float* bounds, int32_t* size, int32_t* matidx,
-                                float* rnd, float* npos, float* nnrm, float* nL, float* nw, float* records) {
+                                float* rnd, float* npos, float* nnrm, float* nL, float* nw, float* records,
+                                float* dirstat) {
     const int32_t total = 2 * n - 1;
     /* leaves */
     for (int32_t i = 0; i < n; ++i) {
@@ -595,19 +600,27 @@ OR_EXPORT void oracle_bottom_up(int32_t n, const float* pos, const float* nrm, c
         r[12] = A[3 * i]; r[13] = A[3 * i + 1]; r[14] = A[3 * i + 2]; r[15] = 1.0f;
     }
     if (n < 2) return;
-    /* leaf cones: normal cone = (n, 1); direction cone = (w/|w|, 1), or the sphere when w = 0 */
+    /* leaf cones: normal cone = (n, 1); direction cone = (w/|w|, 1), or the sphere when w = 0;
+       direction statistics (a w/|w|, a) */
     float* cone = (float*)malloc(sizeof(float) * 8 * (size_t)total);
+    float* ds = (float*)malloc(sizeof(float) * 4 * (size_t)total);
     for (int32_t i = 0; i < n; ++i) {
         float* c = cone + 8 * (size_t)i;
+        float* d = ds + 4 * (size_t)i;
         c[0] = nrm[3 * i]; c[1] = nrm[3 * i + 1]; c[2] = nrm[3 * i + 2]; c[3] = 1.0f;
         const float* wi = w + 3 * i;
+        const float* ai = A + 3 * i;
+        const float a = (0.2126f * ai[0] + 0.7152f * ai[1]) + 0.0722f * ai[2];
         float l2 = dot3(wi, wi);
         if (l2 > 0.0f) {
             float inv = 1.0f / sqrtf(l2);
             c[4] = wi[0] * inv; c[5] = wi[1] * inv; c[6] = wi[2] * inv; c[7] = 1.0f;
+            d[0] = a * c[4]; d[1] = a * c[5]; d[2] = a * c[6];
         } else {
             c[4] = c[5] = c[6] = 0.0f; c[7] = -1.0f;
+            d[0] = d[1] = d[2] = 0.0f;
         }
+        d[3] = a;
     }
     float* bb = (float*)malloc(sizeof(float) * 6 * (size_t)total);
     for (int32_t i = 0; i < n; ++i)
@@ -648,7 +661,12 @@ OR_EXPORT void oracle_bottom_up(int32_t n, const float* pos, const float* nrm, c
         const float* rl = records + 16 * (size_t)l;
         const float* rr = records + 16 * (size_t)r;
         const float* rp = records + 16 * (size_t)repr;
-        for (int c = 0; c < 9; ++c) rt[c] = rp[c];
+        for (int c = 0; c < 4; ++c) ds[4 * (size_t)t + c] = ds[4 * (size_t)l + c] + ds[4 * (size_t)r + c];
+        const float at = ds[4 * (size_t)t + 3];
+        const int32_t arep = at > 0.0f ? (rnd[t] > ds[4 * (size_t)l + 3] / at ? r : l) : repr;
+        const float* ra = records + 16 * (size_t)arep;
+        for (int c = 0; c < 6; ++c) rt[c] = rp[c];
+        for (int c = 6; c < 9; ++c) rt[c] = ra[c];
         for (int c = 9; c < 15; ++c) rt[c] = rl[c] + rr[c];
         rt[15] = (float)size[t];
         cone_union(cone + 8 * l, cone[8 * l + 3], cone + 8 * r, cone[8 * r + 3], cone + 8 * t, cone + 8 * t + 3);
@@ -661,9 +679,11 @@ OR_EXPORT void oracle_bottom_up(int32_t n, const float* pos, const float* nrm, c
         memcpy(&b[7], &right[k], 4);
         for (int c = 0; c < 8; ++c) b[8 + c] = cone[8 * t + c];
     }
+    if (dirstat) memcpy(dirstat, ds, sizeof(float) * 4 * (size_t)total);
     free(st);
     free(bb);
     free(cone);
+    free(ds);
 }
 
 /* ---------------------------------------------------------------------------------------- */

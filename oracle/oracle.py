@@ -180,11 +180,12 @@ def bottom_up(sorted_avpls, diffuse, left, right, seed):
         "incRadiance": np.zeros((t, 3), np.float32),
         "incDirection": np.zeros((t, 3), np.float32),
         "records": np.zeros((t, 16), np.float32),
+        "dirstat": np.zeros((t, 4), np.float32),
     }
     lib().oracle_bottom_up(C.c_int32(n), _p(pos), _p(nrm), _p(w), _p(L), _p(A), _p(mat), _p(diffuse),
                            _p(left), _p(right), C.c_uint32(seed), _p(out["bounds"]), _p(out["size"]),
                            _p(out["materialIndex"]), _p(out["randomNumbers"]), _p(out["position"]), _p(out["normal"]),
-                           _p(out["incRadiance"]), _p(out["incDirection"]), _p(out["records"]))
+                           _p(out["incRadiance"]), _p(out["incDirection"]), _p(out["records"]), _p(out["dirstat"]))
     out["bounds"] = out["bounds"][: n - 1]
     return out
 

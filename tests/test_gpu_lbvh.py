@@ -11,7 +11,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 INT_KEYS = ["morton", "sorted_index", "left", "right", "parents", "size", "materialIndex"]
-FLOAT_KEYS = ["randomNumbers", "position", "normal", "incRadiance", "incDirection", "records"]
+FLOAT_KEYS = ["randomNumbers", "position", "normal", "incRadiance", "incDirection", "records", "dirstat"]
 
 
 def _compare(gpu, ref, n):

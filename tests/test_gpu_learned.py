@@ -51,7 +51,7 @@ def test_band_only_cut_equals_scaled_error_bound_cut(ctx, scene_, band):
     """With threshold 1 the network never refines, so the learned cut refines exactly the nodes whose
     bound exceeds band * tau: the error-bound cut at band * eps (powers of two scale exactly)."""
     d, dv, bvh, tree, gb = scene_
-    model = learned.Model(ctx, seed=5)
+    model = learned.Model(ctx, seed=5, loss=L.ARC_MLP_LOSS_BCE)  # probability threshold 1: never refines
     eps = float(np.float32(0.01))
     img_b, cuts_b = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=eps * band))
     img_l, cuts_l = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_LEARNED, error_bound=eps, mlp_band=band,

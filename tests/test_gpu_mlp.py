@@ -66,22 +66,31 @@ def test_forward_matches_torch_and_oracle(ctx, mlp, rows):
         assert np.max(np.abs(out.cpu().numpy() - y64)) <= 3e-2 * max(1.0, np.abs(y64).max())
 
 
-def test_gradients_match_torch_and_oracle(ctx, mlp):
+@pytest.mark.parametrize("loss", ["bce", "squared"])
+def test_gradients_match_torch_and_oracle(ctx, mlp, loss):
     import torch
 
     rows = 1000
     g = torch.Generator(device="cuda").manual_seed(11)
     x = torch.randn(rows, 16, device="cuda", generator=g).to(torch.bfloat16).contiguous()
-    lab = (torch.rand(rows, device="cuda", generator=g) > 0.5).float()
+    if loss == "bce":
+        lab = (torch.rand(rows, device="cuda", generator=g) > 0.5).float()
+    else:
+        lab = torch.randn(rows, device="cuda", generator=g) * 0.5
     wts = torch.rand(rows, device="cuda", generator=g) + 0.5
+    kind = L.ARC_MLP_LOSS_BCE if loss == "bce" else L.ARC_MLP_LOSS_SQUARED
+    L.check(ctx.lib.arc_mlp_set_loss(mlp, kind), "set_loss")
+    assert ctx.lib.arc_mlp_get_loss(mlp) == kind
     grads = np.zeros(M.NUM_PARAMS, np.float32)
-    loss = C.c_float()
+    loss_v = C.c_float()
     L.check(ctx.lib.arc_mlp_gradients(mlp, C.c_void_p(x.data_ptr()), C.c_void_p(lab.data_ptr()),
                                       C.c_void_p(wts.data_ptr()), rows, float(wts.sum().item()),
-                                      grads.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)), "gradients")
+                                      grads.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss_v)), "gradients")
     p = _params(ctx, mlp)
-    l64, g64 = M.loss_and_grad(p.astype(np.float64), x.float().cpu().numpy(), lab.cpu().numpy(), wts.cpu().numpy())
-    assert abs(loss.value - l64) <= 1e-2 * abs(l64)
+    L.check(ctx.lib.arc_mlp_set_loss(mlp, L.ARC_MLP_LOSS_BCE), "set_loss")
+    l64, g64 = M.loss_and_grad(p.astype(np.float64), x.float().cpu().numpy(), lab.cpu().numpy(), wts.cpu().numpy(),
+                               loss=loss)
+    assert abs(loss_v.value - l64) <= 1e-2 * abs(l64)
     # torch autograd with the kernel's rounding points (straight-through in the backward)
     P = {k: torch.tensor(v, dtype=torch.float32, device="cuda", requires_grad=True) for k, v in M.unpack(p).items()}
     gelu = lambda z: 0.5 * z * (1 + torch.tanh(np.sqrt(2.0 / np.pi) * (z + 0.044715 * z ** 3)))  # noqa: E731
@@ -92,7 +101,11 @@ def test_gradients_match_torch_and_oracle(ctx, mlp):
     h2 = st(gelu(z2))
     z3 = h2 @ st(P["W3"]).T + P["b3"]
     y = gelu(z3) @ P["w4"] + P["b4"][0]
-    ref_loss = (wts * torch.nn.functional.binary_cross_entropy_with_logits(y, lab, reduction="none")).sum() / wts.sum()
+    if loss == "bce":
+        per = torch.nn.functional.binary_cross_entropy_with_logits(y, lab, reduction="none")
+    else:
+        per = (y - lab) ** 2
+    ref_loss = (wts * per).sum() / wts.sum()
     ref_loss.backward()
     gt = np.concatenate([P[k].grad.detach().cpu().numpy().ravel() for k, _ in M.SIZES])
     for ref, tol in ((gt, 0.03), (g64, 0.05)):
