@@ -576,6 +576,120 @@ __global__ void __launch_bounds__(64) cut_eval_kernel(EvalArgs a) {
     }
 }
 
+// Cut evaluation with packed FP32 pairs (no or cone antiradiance): each thread (one pixel) takes
+// two cut nodes per step with f32x2 arithmetic.  The chunk's records are staged interleaved by
+// node pair: float pair * 32 + 2 f + h holds field f (0..15 of the packed record) of node
+// 2 pair + h, so one 16-byte shared load brings two fields of both nodes.  An odd chunk is padded
+// with a zero record, which contributes exactly 0.  Same terms as pair_terms; the even and odd
+// nodes' partial sums are added before the chunk's Kahan step.
+template <int AR>
+__global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
+    constexpr int kChunk = 256;
+    __shared__ __align__(16) float srec[kChunk * 16];
+    const int tile = blockIdx.x;
+    const int i = threadIdx.x;
+    const int x = (tile % a.tiles_x) * kTile + i % kTile, y = (tile / a.tiles_x) * kTile + i / kTile;
+    bool valid = x < a.width && y < a.height;
+    float4 gp = make_float4(0, 0, 0, 0), gn = make_float4(0, 0, 0, 0);
+    int mat = 0;
+    if (valid) {
+        gp = a.gpos[(int64_t)y * a.gpitch + x];
+        gn = a.gnrm[(int64_t)y * a.gpitch + x];
+        mat = (int)gn.w;
+        valid = mat > 0 && mat < a.num_mats;
+    }
+    float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+    if (valid) {
+        const float l = rsqrtf(gn.x * gn.x + gn.y * gn.y + gn.z * gn.z);
+        nx = gn.x * l;
+        ny = gn.y * l;
+        nz = gn.z * l;
+    }
+    const uint64_t PX = f2(-gp.x, -gp.x), PY = f2(-gp.y, -gp.y), PZ = f2(-gp.z, -gp.z);
+    const uint64_t NX = f2(nx, nx), NY = f2(ny, ny), NZ = f2(nz, nz);
+    const float cos_thr = a.pc.cos_thr, eps = a.pc.eps, inv_clamp2 = a.pc.inv_clamp2;
+    float ss[6] = {0, 0, 0, 0, 0, 0}, sc[6] = {0, 0, 0, 0, 0, 0};
+    const int count = a.pool.counts[tile];
+    for (int base = 0; base < count; base += kChunk) {
+        const int cnt = min(kChunk, count - base);
+        const int pairs = (cnt + 1) >> 1;
+        // kChunk divides kChunkSize: a sub-chunk never straddles two pool chunks
+        const int32_t* nodes = a.pool.entries + (size_t)a.pool.tables[(size_t)tile * a.pool.max_chunks + base / kChunkSize] *
+                                                    kChunkSize + base % kChunkSize;
+        __syncthreads();
+        for (int j = i; j < pairs * 8; j += 64) {
+            const int nl = j >> 2, quad = j & 3;
+            const float4 q = nl < cnt ? a.records[4 * (size_t)nodes[nl] + quad] : make_float4(0, 0, 0, 0);
+            float* d = srec + (nl >> 1) * 32 + 8 * quad + (nl & 1);
+            d[0] = q.x;
+            d[2] = q.y;
+            d[4] = q.z;
+            d[6] = q.w;
+        }
+        __syncthreads();
+        uint64_t R0 = 0, R1 = 0, R2 = 0, A0 = 0, A1 = 0, A2 = 0;  // packed zeros
+#pragma unroll 2
+        for (int pr = 0; pr < pairs; ++pr) {
+            const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(srec + pr * 32);
+            const ulonglong2 f01 = s2[0], f23 = s2[1], f45 = s2[2], f67 = s2[3], f89 = s2[4], f1011 = s2[5];
+            const uint64_t dx = f2_add(f01.x, PX), dy = f2_add(f01.y, PY), dz = f2_add(f23.x, PZ);
+            const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+            float l2a, l2b;
+            f2_split(l2, l2a, l2b);
+            const uint64_t r = f2(rsqrtf(fmaxf(l2a, 1e-30f)), rsqrtf(fmaxf(l2b, 1e-30f)));
+            const uint64_t c1 = f2_mul(f2_fma(NZ, dz, f2_fma(NY, dy, f2_mul(NX, dx))), r);
+            const uint64_t c2n = f2_mul(f2_fma(f45.y, dz, f2_fma(f45.x, dy, f2_mul(f23.y, dx))), r);  // -c2
+            float c1a, c1b, c2a, c2b, rra, rrb;
+            f2_split(c1, c1a, c1b);
+            f2_split(c2n, c2a, c2b);
+            f2_split(f2_mul(r, r), rra, rrb);
+            const uint64_t inv = f2(fminf(rra, inv_clamp2), fminf(rrb, inv_clamp2));
+            const uint64_t g = f2_mul(f2(fmaxf(c1a, 0.0f) * fmaxf(-c2a, 0.0f), fmaxf(c1b, 0.0f) * fmaxf(-c2b, 0.0f)), inv);
+            R0 = f2_fma(f89.y, g, R0);
+            R1 = f2_fma(f1011.x, g, R1);
+            R2 = f2_fma(f1011.y, g, R2);
+            if (AR == ARC_AR_CONE) {
+                const ulonglong2 f1213 = s2[6], f1415 = s2[7];
+                const uint64_t wdr = f2_mul(f2_fma(f89.x, dz, f2_fma(f67.y, dy, f2_mul(f67.x, dx))), r);  // -cw
+                float wa, wb, ia, ib;
+                f2_split(wdr, wa, wb);
+                f2_split(f2_mul(c1, inv), ia, ib);
+                const uint64_t ga = f2((-wa > cos_thr && c1a > eps) ? ia : 0.0f, (-wb > cos_thr && c1b > eps) ? ib : 0.0f);
+                A0 = f2_fma(f1213.x, ga, A0);
+                A1 = f2_fma(f1213.y, ga, A1);
+                A2 = f2_fma(f1415.x, ga, A2);
+            }
+        }
+        const uint64_t acc[6] = {R0, R1, R2, A0, A1, A2};
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            float lo, hi;
+            f2_split(acc[c], lo, hi);
+            kahan_add(ss[c], sc[c], lo + hi);
+        }
+    }
+    if (x >= a.width || y >= a.height) return;
+    double rad[3] = {0, 0, 0}, ar[3] = {0, 0, 0};
+    if (valid) {
+        const float4 d = a.mats[mat].diffuse_exp;
+        const double kd[3] = {(double)(kOneOverPi * d.x), (double)(kOneOverPi * d.y), (double)(kOneOverPi * d.z)};
+        for (int c = 0; c < 3; ++c) {
+            rad[c] = kd[c] * ((double)ss[c] - (double)sc[c]);
+            ar[c] = kd[c] * ((double)ss[3 + c] - (double)sc[3 + c]);
+        }
+    }
+    const int64_t o = (int64_t)y * a.opitch + x;
+    const double res[3] = {rad[0] - ar[0], rad[1] - ar[1], rad[2] - ar[2]};
+    if (a.out_res) a.out_res[o] = make_float4((float)res[0], (float)res[1], (float)res[2], 1.0f);
+    if (a.out_rad) a.out_rad[o] = make_float4((float)rad[0], (float)rad[1], (float)rad[2], 1.0f);
+    if (a.out_ar) a.out_ar[o] = make_float4((float)ar[0], (float)ar[1], (float)ar[2], 1.0f);
+    if (a.out_res64) {
+        a.out_res64[3 * o + 0] = res[0];
+        a.out_res64[3 * o + 1] = res[1];
+        a.out_res64[3 * o + 2] = res[2];
+    }
+}
+
 // result = radiance - antiradiance in FP64 (kernel_combine, cudaGather.cu:782-803)
 __global__ void combine_kernel(const double* rad64, const double* ar64, int width, int height, float4* out_res,
                                float4* out_ar, double* out_res64, int64_t opitch) {
@@ -757,9 +871,9 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ea.out_res64 = out->result_fp64;
     ea.opitch = out->pitch;
     stage_begin(ctx, "cut_eval");
-    if (gp->ar_kind == 0) cut_eval_kernel<0><<<tiles, 64, 0, st>>>(ea);
+    if (gp->ar_kind == 0) cut_eval_packed_kernel<0><<<tiles, 64, 0, st>>>(ea);
     if (gp->ar_kind == 1) cut_eval_kernel<1><<<tiles, 64, 0, st>>>(ea);
-    if (gp->ar_kind == 2) cut_eval_kernel<2><<<tiles, 64, 0, st>>>(ea);
+    if (gp->ar_kind == 2) cut_eval_packed_kernel<2><<<tiles, 64, 0, st>>>(ea);
     stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
     ctx->last_cut.num_tiles = tiles;

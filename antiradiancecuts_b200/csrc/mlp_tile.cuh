@@ -45,32 +45,6 @@ __device__ __forceinline__ float gelu_grad(float x) {
     return fmaf(0.5f, th, 0.5f) + 0.5f * x * (1.0f - th * th) * fmaf(3.0f * kGeluB, x2, kGeluA);
 }
 
-// Packed FP32 pairs (sm_100 f32x2 instructions: two IEEE round-to-nearest operations each, the
-// same results as the scalar forms).
-__device__ __forceinline__ uint64_t f2(float lo, float hi) {
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void f2_split(uint64_t v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
-    uint64_t d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
-    uint64_t d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-
 // gelu of z + b for a pair, the same operations as gelu()
 __device__ __forceinline__ uint64_t gelu2(uint64_t z, uint64_t b) {
     const uint64_t x = f2_add(z, b);

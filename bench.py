@@ -2,7 +2,7 @@
 """ms/frame at 1920x1080 with 1,048,576 AVPLs: the cut gather (LBVH build + cut selection + cut
 evaluation) against the exact brute-force gather, with the cut image's RMSE against an FP64 image.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--method learned|error_bound]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--method learned|error_bound] [--small]
     python bench.py --impl reference      # the CPU gather (scalar FP32 restatement), same metric
 
 One step = one frame rendered from device-resident inputs (AVPL arrays, G-buffer): LBVH build +
@@ -38,6 +38,8 @@ UNIT = "ms/frame"
 #   cone antiradiance: w.d (5) + cos (1) + G_A (1) + 3 FFMA accumulate (6)           = 13
 #   disk antiradiance: w.n (5) + t (2) + hit (6) + |h - p|^2 (5) + 3 FFMA (6)         = 24
 FLOP_PER_PAIR = {0: 30, 1: 54, 2: 43}
+# MLP forward per scored row: 2 * (16*64 + 64*64 + 64*64 + 64) multiply-adds
+FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64)
 
 
 def lbvh_bytes_per_avpl() -> dict:
@@ -196,7 +198,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="variant500_1080p_1m")
     ap.add_argument("--method", default="auto", choices=["auto", "learned", "error_bound"])
-    ap.add_argument("--error-bound", type=float, default=0.01)
+    ap.add_argument("--error-bound", type=float, default=0.002, help="analytic cut (error_bound method)")
     ap.add_argument("--small", action="store_true", help="640x360 / 262,144 AVPLs, no extras (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip exact / FP64 / CPU legs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -231,10 +233,10 @@ def main():
 
     method = args.method
     model = None
+    from antiradiancecuts_b200 import learned
+
     if method in ("auto", "learned"):
         try:
-            from antiradiancecuts_b200 import learned
-
             model = learned.load_default_model(ctx)
             method = "learned"
         except Exception as e:  # no trained model available
@@ -244,8 +246,11 @@ def main():
             model_error = str(e)
     kind = L.ARC_CUT_LEARNED if method == "learned" else L.ARC_CUT_ERROR_BOUND
     tiles = ((W + 7) // 8) * ((H + 7) // 8)
-    cut = api.cut_params(kind, error_bound=args.error_bound, model=model.handle.value if model else None,
-                         cut_pool_entries=tiles * 65536)
+    pool = tiles * 65536
+    if model is not None:
+        cut = learned.cut_params(model, cut_pool_entries=pool)
+    else:
+        cut = api.cut_params(kind, error_bound=args.error_bound, cut_pool_entries=pool)
 
     stream = ctx.stream  # the context's stream (also torch's current stream)
 
@@ -261,6 +266,7 @@ def main():
     torch.cuda.synchronize()
     lib.arc_context_profile(ctx.handle, 1)
     launches0 = lib.arc_context_launch_count(ctx.handle)
+    rows0 = lib.arc_context_learned_rows(ctx.handle)
     clocks = Clocks(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -272,6 +278,7 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
     launches = lib.arc_context_launch_count(ctx.handle) - launches0
+    rows_per_frame = (lib.arc_context_learned_rows(ctx.handle) - rows0) / args.steps
     names = C.create_string_buffer(4096)
     st_ms = (C.c_float * 256)()
     nst = C.c_int32()
@@ -299,14 +306,25 @@ def main():
     L.check(lib.arc_measure_fp32_peak(ctx.handle, C.byref(sc), C.byref(pk)), "arc_measure_fp32_peak")
     fp32_peak = max(sc.value, pk.value)
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0, "fallback": True}
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
     dom = max(per_stage, key=per_stage.get) if per_stage else "cut_eval"
+    eval_roof = None
+    if "cut_eval" in per_stage:
+        ach = pairs * FLOP_PER_PAIR[wl.ar_kind] / (per_stage["cut_eval"] * 1e-3) / 1e12
+        eval_roof = {"kernel": "cut_eval", "bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": ach / fp32_peak, "traffic": None, "ms": per_stage["cut_eval"],
+                     "peak_source": "measured FFMA microbenchmark (arc_measure_fp32_peak), max of scalar/packed"}
     if dom == "cut_eval":
-        flops = pairs * FLOP_PER_PAIR[wl.ar_kind]
-        ach = flops / (per_stage[dom] * 1e-3) / 1e12
-        roof = {"kernel": "cut_eval", "bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": ach / fp32_peak, "traffic": None,
-                "peak_source": "measured FFMA microbenchmark (arc_measure_fp32_peak), max of scalar/packed"}
+        roof = dict(eval_roof)
+    elif dom == "cut_learned":
+        # the fused level kernel's algorithmic work is the network's forward pass over the scored
+        # rows (feature computation and frontier expansion are counted as overhead)
+        bf16 = peaks.get("bf16_tflops", 1590.0)
+        ach = rows_per_frame * FLOP_PER_ROW / (per_stage[dom] * 1e-3) / 1e12
+        roof = {"kernel": "learned_level", "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
+                "frac": ach / bf16, "traffic": None, "rows_per_frame": rows_per_frame,
+                "flop_per_row": FLOP_PER_ROW, "ms": per_stage[dom],
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if "bf16_tflops" in peaks else "fallback"}
     elif dom.startswith("lbvh"):
         b = lbvh_bytes_per_avpl()[dom] * N
         ach = b / (per_stage[dom] * 1e-3) / 1e9
@@ -360,7 +378,29 @@ def main():
         sample = rng.choice(np.nonzero(valid_px.ravel())[0], size=64, replace=False)
         _, _, o64 = O.gather_fp64(pos, nrm, sample, avpls, dif, spe, ex, cam,
                                   O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp))
+        # ---- the analytic error-bound cut at the bound that keeps it within 1% (the method the
+        # learned cut is measured against) ----
+        out_an = api.Outputs(W, H)
+        cut_an = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=args.error_bound, cut_pool_entries=pool)
+
+        def frame_an():
+            bvh.build(dv)
+            api.gather_cut(ctx, bvh, None, gb, cam, prm, cut_an, out_an)
+
+        frame_an()
+        assert ctx.synchronize() == 0
+        e0.record(stream)
+        for _ in range(2):
+            frame_an()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        an_ms = e0.elapsed_time(e1) / 2
+        an_nodes = float(api.cut_counts(ctx).mean())
+        assert ctx.synchronize() == 0
         result = {
+            "analytic_cut": {"error_bound": args.error_bound, "ms_per_frame": an_ms,
+                             "rel_rmse_vs_fp64": rel_rmse(out_an.result64.cpu().numpy().reshape(-1, 3), ref64),
+                             "nodes_per_tile": an_nodes},
             "exact_ms_per_frame": exact_ms,
             "speedup_vs_exact": exact_ms / ms,
             "rel_rmse_vs_fp64": rel_rmse(cut_img, ref64),
@@ -372,11 +412,10 @@ def main():
 
     # ---- e2e through the public API: CudaGather::run with host AVPLs, result read back ----
     g = api.CudaGather(ctx, gb, mats, outputs=api.Outputs(W, H, fp64=False, parts=False))
-    # arc_run uses the default cut pool (16384 entries per tile) unless the config sets a model;
-    # the e2e run below therefore goes through the same entry point a user calls
-    rcfg = api.run_config(useLightCuts=1, cut_kind=kind, error_bound=args.error_bound, ar_kind=wl.ar_kind,
+    rcfg = api.run_config(useLightCuts=1, cut_kind=kind, error_bound=cut.error_bound, ar_kind=wl.ar_kind,
                           cone_half_angle=math.radians(wl.cone_half_angle_deg), dist_clamp=wl.dist_clamp,
-                          model=model.handle.value if model else None)
+                          model=model.handle.value if model else None, ar_uncertain_factor=cut.ar_uncertain_factor,
+                          mlp_threshold=cut.mlp_threshold, mlp_band=cut.mlp_band, cut_pool_entries=pool)
     host_out = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
     for _ in range(args.warmup):
         g.run(avpls, cam, scene.scene_extent(desc), rcfg)
@@ -401,12 +440,14 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload if not args.small else args.workload + "_small",
                        "resolution": [W, H], "avpls": N, "light_paths": paths, "method": method,
-                       "error_bound": args.error_bound, "antiradiance": "cone", "cone_half_angle_deg":
+                       "error_bound": cut.error_bound, "ar_uncertain_factor": cut.ar_uncertain_factor,
+                       "mlp_threshold": cut.mlp_threshold if model else None,
+                       "mlp_band": cut.mlp_band if model else None, "antiradiance": "cone", "cone_half_angle_deg":
                            wl.cone_half_angle_deg, "dist_clamp": wl.dist_clamp,
                        "l2": "inputs larger than L2 (AVPLs 71 MB, G-buffer 66 MB, tree ~0.9 GB); no flush",
                        "parallelism": f"replicas x{world}", "frames_per_s_all_gpus": world * 1000.0 / ms},
             "stage_ms": per_stage, "cut_nodes_per_tile": cut_stats, "gpu_launches": int(launches), "launches_per_frame": launches / args.steps,
-            "roofline": roof, "lbvh_roofline": lbvh_roof, **result,
+            "roofline": roof, "cut_eval_roofline": eval_roof, "lbvh_roofline": lbvh_roof, **result,
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
             "cpu_baseline": cpu, "clocks": clk,
