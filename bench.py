@@ -48,8 +48,9 @@ def lbvh_bytes_per_avpl() -> dict:
     return {
         "lbvh_morton": 12 + 8,                     # positions in; key + index out
         "lbvh_sort": 4 * (8 + 8),                  # 4 passes: (key, index) in and out
-        "lbvh_karras": (4 + 4 + 64) + (16 + 4 + 64 + 32 + 24 + 60 + 24),  # codes, index, AVPL in; tree out
-        "lbvh_bottom_up": 2 * (24 + 12 + 4 + 64 + 32) + (24 + 60 + 64 + 32 + 64),
+        # codes, index, AVPL in; leaf records, cones, direction statistics, node data out
+        "lbvh_karras": (4 + 4 + 64) + (16 + 4 + 64 + 32 + 16 + 24 + 60 + 24),
+        "lbvh_bottom_up": 2 * (24 + 12 + 4 + 64 + 32 + 16) + (24 + 60 + 64 + 32 + 16 + 64),
     }
 
 

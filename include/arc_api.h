@@ -405,11 +405,13 @@ arc_status arc_mlp_train_step(arc_mlp* mlp, const void* features_bf16, const flo
                               int64_t rows, float weight_sum, float lr, float* device_loss_accum);
 
 /* Training samples of the learned cut (no counterpart in the reference): walks every 8x8 tile's
- * tree with the exact decision "refine iff max over the tile's pixels |exact node contribution -
- * node estimate| > delta * mean |exact tile value|" (exact contributions from FP64 prefix sums
- * over the sorted leaves) and writes, for each visited node the analytic bound of `cut` cannot
- * accept, its 16 BF16 features, its 0/1 label and its error relative to the tile value.  Device
- * output arrays of `capacity` rows; *count receives the rows written.  Waits for the stream. */
+ * tree with the exact decision "refine iff the RMS over the tile's pixels of |exact node
+ * contribution - node estimate| > delta * mean |exact tile value|" (exact contributions from FP64
+ * prefix sums over the sorted leaves) and writes, for each visited node that the learned selection
+ * with `cut` would score (its bound above cut->error_bound times the estimate and not above
+ * cut->mlp_band times that), its 16 BF16 features, its 0/1 label and its error relative to the
+ * tile value.  Device output arrays of `capacity` rows; *count receives the rows written.  Waits
+ * for the stream. */
 arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gbuffer,
                                     ArcFloat3 camera_position, const ArcGatherParams* params, const ArcCutParams* cut,
                                     float delta, void* features_bf16, float* labels, float* errors, int32_t capacity,
