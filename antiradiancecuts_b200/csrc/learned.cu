@@ -7,10 +7,11 @@
 //     accepted (the learned cut is never finer than the analytic one);
 //   * inner nodes whose bound exceeds mlp_band times the threshold are refined (their children go
 //     to level l + 1) without the network;
-//   * every other pair's 16 features (BF16) are staged as one row of the CTA's 128-row tile in
-//     shared memory; each full tile is scored on the tensor cores (mlp_tile.cuh) and its pairs are
-//     refined or accepted by the logit, in the same launch.
-// Persistent CTAs take 128 pairs at a time from a per-level work counter; pushes and accepts use
+//   * every other pair's 16 features (BF16) are staged as one row in shared memory; each time
+//     the CTA has 256 rows (two 128-row tiles, one set of weights) they are scored on the tensor
+//     cores (mlp_tile.cuh) and their pairs are refined or accepted by the logit, in the same
+//     launch.
+// Persistent CTAs take 256 pairs at a time from a per-level work counter; pushes and accepts use
 // warp-aggregated atomics.  The host checks the frontier size only every few levels.  Accepted
 // pairs are finally grouped by tile into the chunked cut pool (count, scan, scatter), which the
 // shared cut evaluation reads.
@@ -161,7 +162,7 @@ struct LevelArgs {
     int2* out;              // next level
     int* out_count;
     int capacity;           // entries per frontier
-    int* work;              // chunks of 128 entries handed out
+    int* work;              // chunks of kLevelThreads entries handed out
     unsigned long long* rows_scored;
     const unsigned char* weight_image;  // network, in the shared-memory layout (weight_image)
     float thr_logit;        // refine iff logit >= thr_logit
@@ -182,26 +183,41 @@ __device__ __forceinline__ int2 entry(int tile, int node, int depth) {
 
 enum Action : int { kNone = 0, kAccept = 1, kRefine = 2, kScore = 3 };
 
-// Accepts (tile, node) or pushes (tile, lc), (tile, rc) at depth + 1, per the lane's action; one
-// atomic per warp and kind.  Every lane of the warp calls it.
-__device__ __forceinline__ void emit(const LevelArgs& a, int action, int tile, int node, int lc, int rc, int depth) {
-    const int lane = threadIdx.x & 31;
+constexpr int kLevelThreads = 256;
+
+// Accepts (tile, node) or pushes (tile, lc), (tile, rc) at depth + 1, per the thread's action;
+// one atomic per CTA and kind (the two global counters are shared by every CTA of the level, so
+// reservations are aggregated over the CTA's 8 warps).  Every thread of the CTA calls it (it
+// holds barriers); se: 2 * warps + 2 shared ints, not touched by anything else.
+__device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, int tile, int node, int lc, int rc,
+                                     int depth) {
+    constexpr int kW = kLevelThreads / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const unsigned am = __ballot_sync(0xffffffffu, action == kAccept);
     const unsigned pm = __ballot_sync(0xffffffffu, action == kRefine);
-    int abase = 0, pbase = 0;
-    if (am) {
-        const int leader = __ffs(am) - 1;
-        if (lane == leader) abase = atomicAdd(a.acc_count, __popc(am));
-        abase = __shfl_sync(0xffffffffu, abase, leader);
+    if (lane == 0) {
+        se[w] = __popc(am);
+        se[kW + w] = 2 * __popc(pm);
     }
-    if (pm) {
-        const int leader = __ffs(pm) - 1;
-        if (lane == leader) pbase = atomicAdd(a.out_count, 2 * __popc(pm));
-        pbase = __shfl_sync(0xffffffffu, pbase, leader);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int sa = 0, sp = 0;
+        for (int i = 0; i < kW; ++i) {
+            const int x = se[i], y = se[kW + i];
+            se[i] = sa;
+            se[kW + i] = sp;
+            sa += x;
+            sp += y;
+        }
+        const int ba = sa ? atomicAdd(a.acc_count, sa) : 0;
+        const int bp = sp ? atomicAdd(a.out_count, sp) : 0;
+        se[2 * kW] = ba;
+        se[2 * kW + 1] = bp;
     }
+    __syncthreads();
     if (action == kAccept) {
-        const int pos = abase + __popc(am & lt);
+        const int pos = se[2 * kW] + se[w] + __popc(am & lt);
         const bool ok = pos < a.acc_capacity;
         if (ok)
             a.accepted[pos] = make_int2(tile, node);
@@ -211,7 +227,7 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int action, int tile, i
         const unsigned grp = __match_any_sync(am, ok ? tile : -1 - lane);
         if (ok && lane == __ffs(grp) - 1) atomicAdd(&a.tile_counts[tile], __popc(grp));
     } else if (action == kRefine) {
-        const int pos = pbase + 2 * __popc(pm & lt);
+        const int pos = se[2 * kW + 1] + se[kW + w] + 2 * __popc(pm & lt);
         if (pos + 1 < a.capacity) {
             a.out[pos] = entry(tile, lc, depth + 1);
             a.out[pos + 1] = entry(tile, rc, depth + 1);
@@ -221,12 +237,14 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int action, int tile, i
     }
 }
 
-// shared memory of learned_level: weights and vectors (the image built by weight_image) | staged
-// feature rows (256, K-major, K = 16) | hidden | staged pairs {tile, node | depth, left child,
-// right child}
-constexpr uint32_t fW = 0, fVec = mlp::kWeightBytes, fX = ((mlp::kImageBytes + 127) / 128) * 128, fH = fX + 8192,
-                   fMeta = fH + 16384, kLevelSmem = fMeta + 256 * 16;
-constexpr int kLevelThreads = 128;
+// learned_level: 256 threads, one pair per thread per chunk, rows scored two 128-row tiles at a
+// time.  Shared memory: weights and vectors (the image built by weight_image) | staged feature
+// rows (512, K-major, K = 16: fewer than 256 left over plus one chunk) | hidden rows (256 x 64)
+// | staged pairs {tile, node | depth}
+constexpr int kLevelTiles = kLevelThreads / 128, kStageRows = 2 * kLevelThreads;
+constexpr uint32_t fW = 0, fVec = mlp::kWeightBytes, fX = ((mlp::kImageBytes + 127) / 128) * 128,
+                   fH = fX + kStageRows * 32, fMeta = fH + kLevelThreads * 128, kLevelSmem = fMeta + kStageRows * 8;
+constexpr uint32_t kLevelTmemCols = 64 * kLevelTiles;
 
 // BF16 core-matrix weights + FP32 vectors, once per selection
 __global__ void weight_image(const float* params, unsigned char* img) {
@@ -238,11 +256,12 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     __shared__ __align__(8) uint64_t bar, wbar;
     __shared__ uint32_t tmem_base;
     __shared__ int s_chunk, s_staged;
+    __shared__ int s_emit[2 * (kLevelThreads / 32) + 2];
     const int t = threadIdx.x, w = t >> 5;
     const int count = min(*a.in_count, a.capacity);
     if ((int64_t)blockIdx.x * kLevelThreads >= count) return;  // no chunk can be left for this CTA
     float* vec = reinterpret_cast<float*>(sm + fVec);
-    int4* meta = reinterpret_cast<int4*>(sm + fMeta);
+    int2* meta = reinterpret_cast<int2*>(sm + fMeta);
     if (t == 0) {
         mbar_init(&bar, 1);
         mbar_init(&wbar, 1);
@@ -251,9 +270,9 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
         bulk_g2s(sm + fW, a.weight_image, mlp::kImageBytes, &wbar);
         s_staged = 0;
     }
-    for (int i = t; i < 8192 / 16; i += kLevelThreads)  // rows past the staged ones stay finite
+    for (int i = t; i < kStageRows * 2; i += kLevelThreads)  // rows past the staged ones stay finite
         reinterpret_cast<uint4*>(sm + fX)[i] = make_uint4(0, 0, 0, 0);
-    if (w == 0) tc::alloc(&tmem_base, 64);
+    if (w == 0) tc::alloc(&tmem_base, kLevelTmemCols);
     fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -263,7 +282,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     unsigned long long scored = 0;
     while (ok) {
         if (t == 0) s_chunk = atomicAdd(a.work, 1);
-        __syncthreads();
+        __syncthreads();  // also: every thread has read s_staged before this chunk adds to it
         const int64_t first = (int64_t)s_chunk * kLevelThreads;
         const bool done = first >= count;
         const int64_t e = first + t;
@@ -290,7 +309,8 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                     float f[kFeat];
                     node_features(ti, mean, g, M, nc, wc, a.records + 4 * (size_t)node, a.records + 4 * (size_t)lc,
                                   a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
-                    const int slot = atomicAdd(&s_staged, 1);  // < 256: at most 127 rows are left over
+                    // < kStageRows: fewer than kLevelThreads rows are left over from the last round
+                    const int slot = atomicAdd(&s_staged, 1);
                     uint4 x0, x1;
                     x0.x = mlp::pack2(f[0], f[1]);
                     x0.y = mlp::pack2(f[2], f[3]);
@@ -302,31 +322,36 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                     x1.w = mlp::pack2(f[14], f[15]);
                     *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(slot, 0, kFeat)) = x0;
                     *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(slot, 8, kFeat)) = x1;
-                    meta[slot] = make_int4(tile, node | (depth << kDepthShift), lc, rc);
+                    meta[slot] = make_int2(tile, node | (depth << kDepthShift));
                 }
             }
         }
-        emit(a, action, tile, node, lc, rc, depth);
+        emit(a, s_emit, action, tile, node, lc, rc, depth);
         __syncthreads();
         int staged = s_staged;
         // score full tiles now, and whatever is left once the level is exhausted
         while (staged >= kLevelThreads || (done && staged > 0)) {
             float y = 0.0f;
-            if (!mlp::infer_tile(c, fX, t, &y)) {
+            if (!mlp::infer_tiles<kLevelTiles>(c, fX, t, &y)) {
                 ok = false;
                 break;
             }
             const int n_rows = min(staged, kLevelThreads);
             scored += n_rows;
-            int act = kNone;
-            int4 m = make_int4(0, 0, 0, 0);
+            int act = kNone, mlc = 0, mrc = 0;
+            int2 m = make_int2(0, 0);
             if (t < n_rows) {
                 m = meta[t];
                 act = y >= a.thr_logit ? kRefine : kAccept;
             }
             const int mnode = m.y & ((1 << kDepthShift) - 1), mdepth = m.y >> kDepthShift;
-            emit(a, act, m.x, mnode, m.z, m.w, mdepth);
-            __syncthreads();  // rows 0..127 and their pairs are consumed
+            if (act == kRefine) {  // an inner node: its children from the bounds
+                const size_t k = (size_t)(mnode - a.n);
+                mlc = child_index(__float_as_int(a.bounds[4 * k].w), a.n);
+                mrc = child_index(__float_as_int(a.bounds[4 * k + 1].w), a.n);
+            }
+            emit(a, s_emit, act, m.x, mnode, mlc, mrc, mdepth);
+            __syncthreads();  // the scored rows and their pairs are consumed
             const int rest = staged - n_rows;
             if (t < rest) {
                 const int r = kLevelThreads + t;
@@ -345,7 +370,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     if (t == 0 && scored) atomicAdd(a.rows_scored, scored);
     tc::fence_before_sync();
     __syncthreads();
-    if (w == 0) tc::dealloc(tmem_base, 64);
+    if (w == 0) tc::dealloc(tmem_base, kLevelTmemCols);
 }
 
 // Past the last level the host runs: every pair still in the frontier is accepted.
@@ -759,10 +784,11 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.err = ctx->d_error;
 
     // resident CTAs per SM, from shared memory (the runtime's occupancy query assumes a smaller
-    // shared-memory carve-out than the launch gets); 64 TMEM columns each, 4 at most
+    // shared-memory carve-out than the launch gets) and TMEM (kLevelTmemCols of 512 columns each)
     int smem_sm = 0;
     ARC_TRY_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
-    const int per_sm = std::max(1, std::min(4, smem_sm / (int)(kLevelSmem + 2048)));
+    // (1 KB per CTA reserved by the system, plus the kernel's static shared variables)
+    const int per_sm = std::max(1, std::min(512 / (int)kLevelTmemCols, smem_sm / (int)(kLevelSmem + 1280)));
     ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmem));
     ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));

@@ -119,14 +119,20 @@ __device__ __forceinline__ void publish_smem() {
     __syncthreads();
 }
 
+// TMEM address of thread t's row: tile t / 128 owns accumulator columns 64 (t / 128) ..+63, and a
+// warp may only read its lane quarter, 32 ((t / 32) % 4) .. +31.
+__device__ __forceinline__ uint32_t row_tmem(const InferCta& c, int t) {
+    return c.tmem + ((uint32_t)(((t >> 5) & 3) * 32) << 16) + 64u * (uint32_t)(t >> 7);
+}
+
 // Hidden layer epilogue for this thread's row: 16 columns at a time from TMEM, + bias, GELU,
-// BF16 into the K-major hidden buffer.
+// BF16 into the K-major hidden buffer (rows of all tiles, 64 columns).
 __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const float* bias) {
-    const uint32_t lane_off = (uint32_t)((t >> 5) * 32) << 16;
+    const uint32_t taddr = row_tmem(c, t);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         float z[16];
-        tc::ld16(c.tmem + lane_off + 16 * q, z);
+        tc::ld16(taddr + 16 * q, z);
         uint32_t u[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -141,16 +147,22 @@ __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const 
     }
 }
 
-// Logit of row t of the 128-row K-major input tile at smem offset x (stride between 8-row groups:
-// 256 bytes).  Called by all 128 threads; returns false (every thread) if a tensor-core wait gave
-// up, after which the caller frees its TMEM and stops.
-__device__ __forceinline__ bool infer_tile(InferCta& c, uint32_t x, int t, float* logit) {
+// Logits of NT 128-row tiles: row t (of 128 NT, one per thread of the CTA) of the K-major input
+// rows at smem offset x (stride between 8-row groups: 256 bytes), hidden rows at c.h (1024 bytes
+// between 8-row groups), tile u's accumulator in TMEM columns 64 u .. 64 u + 63.  Called by all
+// 128 NT threads; returns false (every thread) if a tensor-core wait gave up, after which the
+// caller frees its TMEM and stops.
+template <int NT>
+__device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, float* logit) {
     constexpr uint32_t id = tc::idesc_bf16(128, 64, false, false);
     // layer 1 (K = 16)
     publish_smem();
     if (t == 0) {
         tc::fence_after_sync();
-        tc::mma(c.tmem, tc::smem_desc(c.base + x, 128, 256), tc::smem_desc(c.base + c.w + kW1, 128, 256), id, false);
+#pragma unroll
+        for (int u = 0; u < NT; ++u)
+            tc::mma(c.tmem + 64 * u, tc::smem_desc(c.base + x + 4096 * u, 128, 256),
+                    tc::smem_desc(c.base + c.w + kW1, 128, 256), id, false);
         tc::commit(c.bar);
     }
     if (!wait_mma(c)) return false;
@@ -163,23 +175,25 @@ __device__ __forceinline__ bool infer_tile(InferCta& c, uint32_t x, int t, float
             tc::fence_after_sync();
             const uint32_t wb = c.w + (l == 0 ? kW2 : kW3);
 #pragma unroll
-            for (int s = 0; s < 4; ++s)
-                tc::mma(c.tmem, tc::smem_desc(c.base + c.h + 256 * s, 128, 1024),
-                        tc::smem_desc(c.base + wb + 256 * s, 128, 1024), id, s > 0);
+            for (int u = 0; u < NT; ++u)
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    tc::mma(c.tmem + 64 * u, tc::smem_desc(c.base + c.h + 16384 * u + 256 * s, 128, 1024),
+                            tc::smem_desc(c.base + wb + 256 * s, 128, 1024), id, s > 0);
             tc::commit(c.bar);
         }
         if (!wait_mma(c)) return false;
         if (l == 0) hidden_epilogue(c, t, c.vec + 64);
     }
     // layer 3 epilogue and the 64 -> 1 output layer on the CUDA cores
-    const uint32_t lane_off = (uint32_t)((t >> 5) * 32) << 16;
+    const uint32_t taddr = row_tmem(c, t);
     const float* b3 = c.vec + 128;
     const float* w4 = c.vec + 192;
     uint64_t y2 = f2(c.vec[256], 0.0f);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         float z[16];
-        tc::ld16(c.tmem + lane_off + 16 * q, z);
+        tc::ld16(taddr + 16 * q, z);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const float2 bb = *reinterpret_cast<const float2*>(b3 + 16 * q + 2 * j);
@@ -190,10 +204,14 @@ __device__ __forceinline__ bool infer_tile(InferCta& c, uint32_t x, int t, float
     float y0, y1;
     f2_split(y2, y0, y1);
     const float y = y0 + y1;
-    // every thread's TMEM reads are done before the next tile's MMAs overwrite the accumulator
+    // every thread's TMEM reads are done before the next round's MMAs overwrite the accumulators
     tc::fence_before_sync();
     *logit = y;
     return true;
+}
+
+__device__ __forceinline__ bool infer_tile(InferCta& c, uint32_t x, int t, float* logit) {
+    return infer_tiles<1>(c, x, t, logit);
 }
 
 }  // namespace mlp
