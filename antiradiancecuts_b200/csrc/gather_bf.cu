@@ -57,15 +57,17 @@ struct BfArgs {
     uint32_t* err;
     // general path (raw SoA)
     ArcAvplsGpuParam soa;
+    // packed path over a compacted pixel list (nullptr: rectangular tiles)
+    const int* pixel_list;
+    const int* pixel_count;
 };
 
 // ---------------------------------------------------------------------------------------
 // pack: SoA -> 64-byte records
 // ---------------------------------------------------------------------------------------
-__global__ void pack_bf_records(ArcAvplsGpuParam a, const MaterialRecord* mats, int32_t num_mats, float4* rec,
-                                uint32_t* err) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.numAvpls) return;
+// One AVPL's 64-byte record (fields 0..15: p, n, w, L', A, 1/|w|).
+__device__ __forceinline__ void bf_record(const ArcAvplsGpuParam& a, const MaterialRecord* mats, int32_t num_mats,
+                                          int64_t i, uint32_t* err, float4* r) {
     const float3 p = ld3(a.position, i), nr = ld3(a.normal, i), w = ld3(a.incDirection, i);
     const float3 L = ld3(a.incRadiance, i), A = ld3(a.antiradiance, i);
     int m = a.materialIndex[i];
@@ -83,11 +85,38 @@ __global__ void pack_bf_records(ArcAvplsGpuParam a, const MaterialRecord* mats, 
     Lp.y = light ? L.y : rn_mul(L.y, rn_mul(kOneOverPi, dif.y));
     Lp.z = light ? L.z : rn_mul(L.z, rn_mul(kOneOverPi, dif.z));
     const float inv_w = light ? 0.0f : rn_div(1.0f, rn_sqrt(ww));
-    float4* r = rec + 4 * i;
     r[0] = make_float4(p.x, p.y, p.z, n.x);
     r[1] = make_float4(n.y, n.z, w.x, w.y);
     r[2] = make_float4(w.z, Lp.x, Lp.y, Lp.z);
     r[3] = make_float4(A.x, A.y, A.z, inv_w);
+}
+
+__global__ void pack_bf_records(ArcAvplsGpuParam a, const MaterialRecord* mats, int32_t num_mats, float4* rec,
+                                uint32_t* err) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.numAvpls) return;
+    float4 r[4];
+    bf_record(a, mats, num_mats, i, err, r);
+    float4* d = rec + 4 * i;
+    d[0] = r[0];
+    d[1] = r[1];
+    d[2] = r[2];
+    d[3] = r[3];
+}
+
+// The same records interleaved by AVPL pair: float pair * 32 + 2 f + h holds field f of AVPL
+// 2 pair + h; an odd count is padded with a zero record (it contributes exactly 0).
+__global__ void pack_bf_pairs(ArcAvplsGpuParam a, const MaterialRecord* mats, int32_t num_mats, float* rec,
+                              uint32_t* err) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.numAvpls + (a.numAvpls & 1)) return;
+    float4 r[4] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
+                   make_float4(0, 0, 0, 0)};
+    if (i < a.numAvpls) bf_record(a, mats, num_mats, i, err, r);
+    const float* f = reinterpret_cast<const float*>(r);
+    float* d = rec + (i >> 1) * 32 + (i & 1);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) d[2 * q] = f[q];
 }
 
 // PREC: 0 = chunk partials folded into Kahan sums, 1 = per-term Kahan, 2 = naive FP32, 3 = FP64.
@@ -279,6 +308,234 @@ __global__ void __launch_bounds__(kThreads) gather_bf_kernel(BfArgs k) {
     }
 }
 
+// Surface pixels of the G-buffer, compacted into a list (order within a warp arbitrary), for the
+// list form of the packed kernel; every other pixel gets here the outputs the gather gives a pixel
+// without a surface (0, w = 1).  Bad material indices are reported as the gather kernels do.
+__global__ void bf_compact_pixels(BfArgs k, int* list, int* count) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    bool valid = x < k.width;
+    if (valid) {
+        const int m = (int)k.gnrm[(int64_t)y * k.gpitch + x].w;
+        if (m <= 0 || m >= k.num_mats) {
+            if (m != 0) set_error(k.err, ARC_DEVERR_BAD_MATERIAL);
+            valid = false;
+        }
+    }
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);
+    int base = 0;
+    if (vm) {
+        const int leader = __ffs(vm) - 1;
+        if (lane == leader) base = atomicAdd(count, __popc(vm));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    if (valid) {
+        list[base + __popc(vm & ((1u << lane) - 1u))] = y * k.width + x;
+    } else if (x < k.width) {
+        const int64_t o = (int64_t)y * k.opitch + x;
+        const float4 z = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        if (k.out_res) k.out_res[o] = z;
+        if (k.out_rad) k.out_rad[o] = z;
+        if (k.out_ar) k.out_ar[o] = z;
+        if (k.out_res64) k.out_res64[3 * o] = k.out_res64[3 * o + 1] = k.out_res64[3 * o + 2] = 0.0;
+        if (k.out_ar64) k.out_ar64[3 * o] = k.out_ar64[3 * o + 1] = k.out_ar64[3 * o + 2] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Packed FP32x2 variant of the default path (per-chunk partials folded into Kahan sums, no or cone
+// antiradiance).  Records come from pack_bf_pairs, so one 16-byte shared load brings two fields of
+// two AVPLs, and each thread evaluates two AVPLs per step for each of its PX pixels with
+// add/mul/fma.rn.f32x2 (sm_100).  Same terms as pair_terms; within a chunk the even and odd AVPLs
+// are summed apart and added before the chunk's Kahan step.
+// ---------------------------------------------------------------------------------------
+// LIST: the block takes kThreads * PX consecutive entries of the compacted list of surface pixels
+// (bf_compact_pixels) instead of a 16 x 16 PX rectangle.
+template <int AR, int PX, bool LIST>
+__global__ void __launch_bounds__(kThreads) gather_bf_packed_kernel(BfArgs k) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    float* stage = reinterpret_cast<float*>(smem);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)kStages * k.chunk * 64);
+
+    const int tid = threadIdx.x;
+    const int tx = tid % kTileW, ty = tid / kTileW;
+    const int rows = kThreads / kTileW;  // 16
+    const int64_t lbase = (int64_t)blockIdx.x * kThreads * PX;
+    int list_n = 0;
+    if (LIST) {
+        list_n = *k.pixel_count;
+        if (lbase >= list_n) return;  // uniform: before any barrier
+    }
+    // pixel j of this thread
+    auto pixel_xy = [&](int j, int& px_, int& py_) {
+        if (LIST) {
+            const int64_t e = lbase + (int64_t)j * kThreads + tid;
+            const int idx = e < list_n ? k.pixel_list[e] : -1;
+            px_ = idx >= 0 ? idx % k.width : k.width;  // past the image: no pixel
+            py_ = idx >= 0 ? idx / k.width : 0;
+        } else {
+            px_ = blockIdx.x * kTileW + tx;
+            py_ = blockIdx.y * rows * PX + ty + j * rows;
+        }
+    };
+
+    const int npad = k.n + (k.n & 1);  // records incl. the zero pad; k.chunk is even
+    const int nchunks = (npad + k.chunk - 1) / k.chunk;
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int c = 0; c < kStages && c < nchunks; ++c) {
+            const int cnt = min(k.chunk, npad - c * k.chunk);
+            mbar_arrive_expect_tx(&bars[c], (uint32_t)cnt * 64u);
+            bulk_g2s(stage + (size_t)c * k.chunk * 16, k.records + (size_t)c * k.chunk * 4, (uint32_t)cnt * 64u,
+                     &bars[c]);
+        }
+    }
+
+    uint64_t PXc[PX], PYc[PX], PZc[PX], NXc[PX], NYc[PX], NZc[PX];
+    float sc[PX][6], ss[PX][6];
+    bool valid[PX];
+    int mat[PX];
+#pragma unroll
+    for (int j = 0; j < PX; ++j) {
+        int x, y;
+        pixel_xy(j, x, y);
+        valid[j] = (x < k.width && y < k.height);
+        mat[j] = 0;
+        float4 gp = make_float4(0, 0, 0, 0), gn = make_float4(0, 0, 0, 0);
+        if (valid[j]) {
+            gp = k.gpos[(int64_t)y * k.gpitch + x];
+            gn = k.gnrm[(int64_t)y * k.gpitch + x];
+            mat[j] = (int)gn.w;
+            if (mat[j] <= 0 || mat[j] >= k.num_mats) {
+                if (mat[j] != 0) set_error(k.err, ARC_DEVERR_BAD_MATERIAL);
+                valid[j] = false;
+            }
+        }
+        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+        if (valid[j]) {
+            const float l = rsqrtf(gn.x * gn.x + gn.y * gn.y + gn.z * gn.z);
+            nx = gn.x * l;
+            ny = gn.y * l;
+            nz = gn.z * l;
+        }
+        PXc[j] = f2(-gp.x, -gp.x);
+        PYc[j] = f2(-gp.y, -gp.y);
+        PZc[j] = f2(-gp.z, -gp.z);
+        NXc[j] = f2(nx, nx);
+        NYc[j] = f2(ny, ny);
+        NZc[j] = f2(nz, nz);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) sc[j][c] = ss[j][c] = 0.0f;
+    }
+    const float cos_thr = k.pc.cos_thr, eps = k.pc.eps, inv_clamp2 = k.pc.inv_clamp2;
+
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+        const int s = c % kStages;
+        const uint32_t parity = (uint32_t)((c / kStages) & 1);
+        if (ok) ok = mbar_wait_bounded(&bars[s], parity, k.err);
+        if (ok) {
+            const int pairs = min(k.chunk, npad - c * k.chunk) >> 1;
+            const float* st = stage + (size_t)s * k.chunk * 16;
+            uint64_t acc[PX][6];
+#pragma unroll
+            for (int j = 0; j < PX; ++j)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) acc[j][q] = 0;  // packed zeros
+#pragma unroll 2
+            for (int pr = 0; pr < pairs; ++pr) {
+                const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(st + pr * 32);
+                const ulonglong2 f01 = s2[0], f23 = s2[1], f45 = s2[2], f89 = s2[4], f1011 = s2[5];
+#pragma unroll
+                for (int j = 0; j < PX; ++j) {
+                    const uint64_t dx = f2_add(f01.x, PXc[j]), dy = f2_add(f01.y, PYc[j]), dz = f2_add(f23.x, PZc[j]);
+                    const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+                    float l2a, l2b;
+                    f2_split(l2, l2a, l2b);
+                    const uint64_t r = f2(rsqrtf(fmaxf(l2a, 1e-30f)), rsqrtf(fmaxf(l2b, 1e-30f)));
+                    const uint64_t c1 = f2_mul(f2_fma(NZc[j], dz, f2_fma(NYc[j], dy, f2_mul(NXc[j], dx))), r);
+                    const uint64_t c2n = f2_mul(f2_fma(f45.y, dz, f2_fma(f45.x, dy, f2_mul(f23.y, dx))), r);
+                    float c1a, c1b, c2a, c2b, rra, rrb;
+                    f2_split(c1, c1a, c1b);
+                    f2_split(c2n, c2a, c2b);
+                    f2_split(f2_mul(r, r), rra, rrb);
+                    const uint64_t inv = f2(fminf(rra, inv_clamp2), fminf(rrb, inv_clamp2));
+                    const uint64_t g =
+                        f2_mul(f2(fmaxf(c1a, 0.0f) * fmaxf(-c2a, 0.0f), fmaxf(c1b, 0.0f) * fmaxf(-c2b, 0.0f)), inv);
+                    acc[j][0] = f2_fma(f89.y, g, acc[j][0]);
+                    acc[j][1] = f2_fma(f1011.x, g, acc[j][1]);
+                    acc[j][2] = f2_fma(f1011.y, g, acc[j][2]);
+                    if (AR == ARC_AR_CONE) {
+                        const ulonglong2 f67 = s2[3], f1213 = s2[6], f1415 = s2[7];
+                        const uint64_t wdr = f2_mul(f2_fma(f89.x, dz, f2_fma(f67.y, dy, f2_mul(f67.x, dx))), r);
+                        float wa, wb, ia, ib;
+                        f2_split(wdr, wa, wb);
+                        f2_split(f2_mul(c1, inv), ia, ib);
+                        const uint64_t ga = f2((-wa > cos_thr && c1a > eps) ? ia : 0.0f,
+                                               (-wb > cos_thr && c1b > eps) ? ib : 0.0f);
+                        acc[j][3] = f2_fma(f1213.x, ga, acc[j][3]);
+                        acc[j][4] = f2_fma(f1213.y, ga, acc[j][4]);
+                        acc[j][5] = f2_fma(f1415.x, ga, acc[j][5]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < PX; ++j)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    float lo, hi;
+                    f2_split(acc[j][q], lo, hi);
+                    kahan_add(ss[j][q], sc[j][q], lo + hi);
+                }
+        }
+        __syncthreads();  // every thread is done reading stage s before it is refilled
+        if (tid == 0 && ok && c + kStages < nchunks) {
+            fence_proxy_async_smem();
+            const int cn = c + kStages;
+            const int cnt = min(k.chunk, npad - cn * k.chunk);
+            mbar_arrive_expect_tx(&bars[s], (uint32_t)cnt * 64u);
+            bulk_g2s(stage + (size_t)s * k.chunk * 16, k.records + (size_t)cn * k.chunk * 4, (uint32_t)cnt * 64u,
+                     &bars[s]);
+        }
+    }
+
+    // epilogue: receiver BRDF, FP64 signed combine, stores
+#pragma unroll
+    for (int j = 0; j < PX; ++j) {
+        int x, y;
+        pixel_xy(j, x, y);
+        if (x >= k.width || y >= k.height) continue;
+        double rad[3] = {0, 0, 0}, ar[3] = {0, 0, 0}, res[3] = {0, 0, 0};
+        if (valid[j]) {
+            const float4 d = k.mats[mat[j]].diffuse_exp;
+            const float kd[3] = {kOneOverPi * d.x, kOneOverPi * d.y, kOneOverPi * d.z};
+            for (int c = 0; c < 3; ++c) {
+                rad[c] = (double)kd[c] * ((double)ss[j][c] - (double)sc[j][c]);
+                ar[c] = (double)kd[c] * ((double)ss[j][3 + c] - (double)sc[j][3 + c]);
+                res[c] = rad[c] - ar[c];
+            }
+        }
+        const int64_t o = (int64_t)y * k.opitch + x;
+        if (k.out_res) k.out_res[o] = make_float4((float)res[0], (float)res[1], (float)res[2], 1.0f);
+        if (k.out_rad) k.out_rad[o] = make_float4((float)rad[0], (float)rad[1], (float)rad[2], 1.0f);
+        if (k.out_ar) k.out_ar[o] = make_float4((float)ar[0], (float)ar[1], (float)ar[2], 1.0f);
+        if (k.out_res64) {
+            k.out_res64[3 * o + 0] = res[0];
+            k.out_res64[3 * o + 1] = res[1];
+            k.out_res64[3 * o + 2] = res[2];
+        }
+        if (k.out_ar64) {
+            k.out_ar64[3 * o + 0] = ar[0];
+            k.out_ar64[3 * o + 1] = ar[1];
+            k.out_ar64[3 * o + 2] = ar[2];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // General path: full f_r on both sides (cudaGather.cu:59-95), geometry-term limits
 // (Gather.frag:182, 190-194); one thread per pixel over the raw SoA arrays.
@@ -453,8 +710,49 @@ arc_status launch_fast_prec(const BfArgs& a, int prec, int px, cudaStream_t st) 
     }
 }
 
+// the packed kernel serves the default precision with no or cone antiradiance
+bool use_packed(const ArcGatherParams& p) { return p.precision == ARC_PREC_KAHAN && p.ar_kind != ARC_AR_DISK; }
+
+template <int AR, int PX>
+arc_status launch_packed(const BfArgs& a, cudaStream_t st) {
+    const size_t smem = (size_t)kStages * a.chunk * 64 + kStages * sizeof(uint64_t);
+    if (a.pixel_list) {  // one block per kThreads * PX listed pixels; blocks past the count return
+        auto fn = gather_bf_packed_kernel<AR, PX, true>;
+        if (smem > 48 * 1024)
+            ARC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int64_t pixels = (int64_t)a.width * a.height;
+        fn<<<(unsigned)((pixels + kThreads * PX - 1) / (kThreads * PX)), kThreads, smem, st>>>(a);
+    } else {
+        auto fn = gather_bf_packed_kernel<AR, PX, false>;
+        if (smem > 48 * 1024)
+            ARC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 grid((a.width + kTileW - 1) / kTileW, (a.height + 16 * PX - 1) / (16 * PX));
+        fn<<<grid, kThreads, smem, st>>>(a);
+    }
+    ARC_TRY_CUDA(cudaGetLastError());
+    return ARC_OK;
+}
+
+template <int AR>
+arc_status launch_packed_px(const BfArgs& a, int px, cudaStream_t st) {
+    if (px == 1) return launch_packed<AR, 1>(a, st);
+    if (px == 2) return launch_packed<AR, 2>(a, st);
+    return launch_packed<AR, 4>(a, st);
+}
+
+// dispatch of the fast path (records packed by pack_bf_pairs when use_packed(p), else by
+// pack_bf_records)
+arc_status launch_fast_path(const BfArgs& a, const ArcGatherParams& p, int px, cudaStream_t st) {
+    if (use_packed(p)) return p.ar_kind == ARC_AR_NONE ? launch_packed_px<0>(a, px, st) : launch_packed_px<2>(a, px, st);
+    switch (p.ar_kind) {
+        case 0: return launch_fast_prec<0>(a, p.precision, px, st);
+        case 1: return launch_fast_prec<1>(a, p.precision, px, st);
+        default: return launch_fast_prec<2>(a, p.precision, px, st);
+    }
+}
+
 BfArgs make_args(arc_context* ctx, const GatherLaunch& g);
-arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a);
+arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a, bool pairs);
 
 }  // namespace
 
@@ -496,16 +794,24 @@ arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g) {
         ARC_TRY_CUDA(cudaGetLastError());
         return ARC_OK;
     }
-    ARC_TRY(pack_records(ctx, g, a));
+    ARC_TRY(pack_records(ctx, g, a, use_packed(p)));
     const TileShape ts = kTileShapes[p.tile_config < 0 ? kDefaultTileShape : p.tile_config];
     a.chunk = ts.chunk;
-    stage_begin(ctx, "bf_gather");
-    arc_status s;
-    switch (p.ar_kind) {
-        case 0: s = launch_fast_prec<0>(a, p.precision, ts.px, st); break;
-        case 1: s = launch_fast_prec<1>(a, p.precision, ts.px, st); break;
-        default: s = launch_fast_prec<2>(a, p.precision, ts.px, st); break;
+    if (use_packed(p)) {  // only surface pixels are gathered
+        int *list = nullptr, *count = nullptr;
+        ARC_TRY(ctx->arena.get("bf_pixel_list", sizeof(int) * (size_t)gb.width * gb.height,
+                               reinterpret_cast<void**>(&list)));
+        ARC_TRY(ctx->arena.get("bf_pixel_count", sizeof(int), reinterpret_cast<void**>(&count)));
+        ARC_TRY_CUDA(cudaMemsetAsync(count, 0, sizeof(int), st));
+        stage_begin(ctx, "bf_pixels");
+        bf_compact_pixels<<<dim3((gb.width + 255) / 256, gb.height), 256, 0, st>>>(a, list, count);
+        stage_end(ctx, 1);
+        ARC_TRY_CUDA(cudaGetLastError());
+        a.pixel_list = list;
+        a.pixel_count = count;
     }
+    stage_begin(ctx, "bf_gather");
+    const arc_status s = launch_fast_path(a, p, ts.px, st);
     stage_end(ctx, 1);
     return s;
 }
@@ -518,7 +824,7 @@ arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, dou
     a.out_res64 = nullptr;
     a.out_ar64 = ar64;
     cudaStream_t st = ctx->stream;
-    ARC_TRY(pack_records(ctx, g, a));
+    ARC_TRY(pack_records(ctx, g, a, false));
     a.chunk = kTileShapes[kDefaultTileShape].chunk;
     stage_begin(ctx, "bf_antiradiance");
     const arc_status s = p.ar_kind == ARC_AR_DISK ? launch_fast<ARC_AR_DISK, 0, 2, false>(a, st)
@@ -568,13 +874,17 @@ BfArgs make_args(arc_context* ctx, const GatherLaunch& g) {
 }
 
 // Pack the AVPL records into the context arena.
-arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a) {
+arc_status pack_records(arc_context* ctx, const GatherLaunch& g, BfArgs& a, bool pairs) {
     float4* rec = nullptr;
-    ARC_TRY(ctx->arena.get("bf_records", (size_t)(a.n > 0 ? a.n : 1) * 64, reinterpret_cast<void**>(&rec)));
+    ARC_TRY(ctx->arena.get("bf_records", (size_t)(a.n + 1) * 64, reinterpret_cast<void**>(&rec)));
     if (a.n > 0) {
         stage_begin(ctx, "bf_pack");
-        pack_bf_records<<<(a.n + 255) / 256, 256, 0, ctx->stream>>>(*g.avpls, ctx->d_materials, ctx->num_materials,
-                                                                     rec, ctx->d_error);
+        if (pairs)
+            pack_bf_pairs<<<(a.n + 1 + 255) / 256, 256, 0, ctx->stream>>>(
+                *g.avpls, ctx->d_materials, ctx->num_materials, reinterpret_cast<float*>(rec), ctx->d_error);
+        else
+            pack_bf_records<<<(a.n + 255) / 256, 256, 0, ctx->stream>>>(*g.avpls, ctx->d_materials,
+                                                                         ctx->num_materials, rec, ctx->d_error);
         stage_end(ctx, 1);
         ARC_TRY_CUDA(cudaGetLastError());
     }
@@ -729,18 +1039,17 @@ extern "C" arc_status arc_gather_bruteforce_noalloc(void* cuda_stream, const Arc
         ARC_TRY_CUDA(cudaGetLastError());
     } else {
         if (a.n > 0) {
-            pack_bf_records<<<(a.n + 255) / 256, 256, 0, st>>>(*avpls, mats, num_materials, records, err);
+            // an odd count's zero pad record still fits: the scratch holds kNoAllocMaxAvpls (even)
+            if (use_packed(p))
+                pack_bf_pairs<<<(a.n + 1 + 255) / 256, 256, 0, st>>>(*avpls, mats, num_materials,
+                                                                    reinterpret_cast<float*>(records), err);
+            else
+                pack_bf_records<<<(a.n + 255) / 256, 256, 0, st>>>(*avpls, mats, num_materials, records, err);
             ARC_TRY_CUDA(cudaGetLastError());
         }
         const TileShape ts = kTileShapes[p.tile_config < 0 ? kDefaultTileShape : p.tile_config];
         a.chunk = ts.chunk;
-        arc_status s;
-        switch (p.ar_kind) {
-            case 0: s = launch_fast_prec<0>(a, p.precision, ts.px, st); break;
-            case 1: s = launch_fast_prec<1>(a, p.precision, ts.px, st); break;
-            default: s = launch_fast_prec<2>(a, p.precision, ts.px, st); break;
-        }
-        ARC_TRY(s);
+        ARC_TRY(launch_fast_path(a, p, ts.px, st));
     }
     if (device_error_word) {
         uint32_t w = 0;

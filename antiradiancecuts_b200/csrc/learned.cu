@@ -69,9 +69,9 @@ __device__ __forceinline__ float safe_log2(float v) { return __log2f(fmaxf(v, 1e
 
 // Radiance and antiradiance luminance of one packed record at a point p with unit normal n
 // (receiver albedo folded into kdl by the caller).
-__device__ __forceinline__ void record_at(const float4* rec, float px, float py, float pz, float nx, float ny, float nz,
-                                          float clamp2, float cos_thr, float& rad, float& ar) {
-    const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+__device__ __forceinline__ void record_at(float4 q0, float4 q1, float4 q2, float4 q3, float px, float py, float pz,
+                                          float nx, float ny, float nz, float clamp2, float cos_thr, float& rad,
+                                          float& ar) {
     const float dx = q0.x - px, dy = q0.y - py, dz = q0.z - pz;
     const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
     const float r = rsqrtf(l2);
@@ -88,10 +88,10 @@ __device__ __forceinline__ void record_at(const float4* rec, float px, float py,
 // the records of its two children (a one-level lookahead at the tile centre), its depth, and the
 // analytic bound M against tau.
 __device__ __forceinline__ void node_features(const TileInfo& t, float mean, const NodeGeom& g, float M, float4 nc,
-                                              float4 wc, const float4* rec, const float4* rec_l, const float4* rec_r,
-                                              float4 ds, int depth, float clamp2, float cos_thr, float* f) {
+                                              float4 wc, float4 q0, float4 q1, float4 q2, float4 q3,
+                                              const float4* rec_l, const float4* rec_r, float4 ds, int depth,
+                                              float clamp2, float cos_thr, float* f) {
     const float E = fmaxf(mean, 1e-30f);
-    const float4 q2 = rec[2], q3 = rec[3];
     const float Ls = lum3(q2.y, q2.z, q2.w), As = lum3(q3.x, q3.y, q3.z);
     const float inv_dc = __fdividef(1.0f, fmaxf(g.dc, 1e-6f));
     const float rt = g.rs - g.rn;
@@ -106,9 +106,9 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
         nz *= s;
     }
     float rad, ar, radl, arl, radr, arr;
-    record_at(rec, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, rad, ar);
-    record_at(rec_l, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radl, arl);
-    record_at(rec_r, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radr, arr);
+    record_at(q0, q1, q2, q3, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, rad, ar);
+    record_at(rec_l[0], rec_l[1], rec_l[2], rec_l[3], cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radl, arl);
+    record_at(rec_r[0], rec_r[1], rec_r[2], rec_r[3], cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radr, arr);
     const float s = __fdividef(t.kdl, E);
     f[0] = clampf((M > 0.0f ? safe_log2(M / fmaxf(t.tau, 1e-30f)) : -32.0f) * 0.125f, -4.0f, 4.0f);
     f[1] = clampf(safe_log2(Ls * s) * 0.125f, -4.0f, 4.0f);
@@ -152,6 +152,7 @@ __device__ __forceinline__ int child_index(int c, int n) { return c >= 0 ? c : n
 // ---------------------------------------------------------------------------------------
 struct LevelArgs {
     int n;
+    int tiles;
     const float4* bounds;
     const float4* records;
     const float4* dirstat;
@@ -179,6 +180,13 @@ constexpr int kDepthShift = 26;  // node ids < 2^26 (trees of up to 32M leaves),
 
 __device__ __forceinline__ int2 entry(int tile, int node, int depth) {
     return make_int2(tile, node | (min(depth, 31) << kDepthShift));
+}
+
+// A frontier entry names a tile of the frame and a node of the tree; anything else (a slot that an
+// overflowing level could not fill) is skipped and reported.
+__device__ __forceinline__ bool valid_entry(int2 en, int tiles, int n) {
+    const int node = en.y & ((1 << kDepthShift) - 1);
+    return en.x >= 0 && en.x < tiles && en.y >= 0 && node < 2 * n - 1;
 }
 
 enum Action : int { kNone = 0, kAccept = 1, kRefine = 2, kScore = 3 };
@@ -217,8 +225,9 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, in
     }
     __syncthreads();
     if (action == kAccept) {
+        // unsigned: the shared counter keeps counting past the capacity and may wrap past 2^31
         const int pos = se[2 * kW] + se[w] + __popc(am & lt);
-        const bool ok = pos < a.acc_capacity;
+        const bool ok = (unsigned)pos < (unsigned)a.acc_capacity;
         if (ok)
             a.accepted[pos] = make_int2(tile, node);
         else
@@ -228,10 +237,11 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, in
         if (ok && lane == __ffs(grp) - 1) atomicAdd(&a.tile_counts[tile], __popc(grp));
     } else if (action == kRefine) {
         const int pos = se[2 * kW + 1] + se[kW + w] + 2 * __popc(pm & lt);
-        if (pos + 1 < a.capacity) {
+        if ((unsigned)pos + 1u < (unsigned)a.capacity) {
             a.out[pos] = entry(tile, lc, depth + 1);
             a.out[pos + 1] = entry(tile, rc, depth + 1);
         } else {
+            if ((unsigned)pos < (unsigned)a.capacity) a.out[pos] = make_int2(-1, -1);  // the next level skips it
             set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
         }
     }
@@ -289,17 +299,23 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
         int action = kNone, tile = 0, node = 0, lc = 0, rc = 0, depth = 0;
         if (!done && e < count) {
             const int2 en = a.in[e];
-            tile = en.x;
-            node = en.y & ((1 << kDepthShift) - 1);
-            depth = en.y >> kDepthShift;
-            action = kAccept;
-            if (node >= a.n) {
+            const bool good = valid_entry(en, a.tiles, a.n);
+            if (!good) set_error(a.err, en.x == -1 ? ARC_DEVERR_CUT_OVERFLOW : ARC_DEVERR_BAD_NODE);
+            tile = good ? en.x : 0;
+            node = good ? en.y & ((1 << kDepthShift) - 1) : 0;
+            depth = good ? en.y >> kDepthShift : 0;
+            action = good ? kAccept : kNone;
+            if (good && node >= a.n) {
                 const int k = node - a.n;
                 float mean;
                 const TileInfo ti = load_tile_info(a.info, tile, &mean);
                 const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
                 const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
-                const float4 q2 = a.records[4 * (size_t)node + 2], q3 = a.records[4 * (size_t)node + 3];
+                // the node's whole record and direction statistics depend only on the pair: load them
+                // with the bounds (the features need them when the network scores the node)
+                const float4* rec = a.records + 4 * (size_t)node;
+                const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
+                const float4 ds = a.dirstat[node];
                 const NodeGeom g = node_geom(ti, b0, b1, nc, wc, a.bp);
                 const float M = node_bound(ti, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
                 lc = child_index(__float_as_int(b0.w), a.n);
@@ -307,8 +323,8 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 if (M > ti.tau) action = M > a.band * ti.tau ? kRefine : kScore;
                 if (action == kScore) {
                     float f[kFeat];
-                    node_features(ti, mean, g, M, nc, wc, a.records + 4 * (size_t)node, a.records + 4 * (size_t)lc,
-                                  a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
+                    node_features(ti, mean, g, M, nc, wc, q0, q1, q2, q3, a.records + 4 * (size_t)lc,
+                                  a.records + 4 * (size_t)rc, ds, depth, a.clamp2, a.cos_thr, f);
                     // < kStageRows: fewer than kLevelThreads rows are left over from the last round
                     const int slot = atomicAdd(&s_staged, 1);
                     uint4 x0, x1;
@@ -326,8 +342,8 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 }
             }
         }
+        // emit's barriers also order every staging of this chunk before s_staged is read
         emit(a, s_emit, action, tile, node, lc, rc, depth);
-        __syncthreads();
         int staged = s_staged;
         // score full tiles now, and whatever is left once the level is exhausted
         while (staged >= kLevelThreads || (done && staged > 0)) {
@@ -350,8 +366,8 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 mlc = child_index(__float_as_int(a.bounds[4 * k].w), a.n);
                 mrc = child_index(__float_as_int(a.bounds[4 * k + 1].w), a.n);
             }
+            // after emit's barriers every thread has read its pair: the rows can be moved
             emit(a, s_emit, act, m.x, mnode, mlc, mrc, mdepth);
-            __syncthreads();  // the scored rows and their pairs are consumed
             const int rest = staged - n_rows;
             if (t < rest) {
                 const int r = kLevelThreads + t;
@@ -362,7 +378,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 meta[t] = meta[r];
             }
             if (t == 0) s_staged = rest;
-            __syncthreads();
+            // the next round's first barrier (in infer_tiles) or the next chunk's orders these moves
             staged = rest;
         }
         if (!ok || done) break;
@@ -378,8 +394,12 @@ __global__ void accept_frontier(LevelArgs a) {
     const int count = min(*a.in_count, a.capacity);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
         const int2 en = a.in[e];
+        if (!valid_entry(en, a.tiles, a.n)) {
+            set_error(a.err, en.x == -1 ? ARC_DEVERR_CUT_OVERFLOW : ARC_DEVERR_BAD_NODE);
+            continue;
+        }
         const int pos = atomicAdd(a.acc_count, 1);
-        if (pos < a.acc_capacity) {
+        if ((unsigned)pos < (unsigned)a.acc_capacity) {
             a.accepted[pos] = make_int2(en.x, en.y & ((1 << kDepthShift) - 1));
             atomicAdd(&a.tile_counts[en.x], 1);
         } else {
@@ -473,7 +493,8 @@ __global__ void scatter_tables(ScatterArgs s, int tiles) {
 
 // (blockDim a multiple of 32: every lane of a warp takes the same loop trips)
 __global__ void scatter_nodes(ScatterArgs s) {
-    const int count = min(*s.acc_count, s.acc_capacity);
+    // every reserved slot below the capacity was written; the counter may have wrapped past 2^31
+    const int count = (int)min((unsigned)*s.acc_count, (unsigned)s.acc_capacity);
     const int lane = threadIdx.x & 31;
     for (int b = blockIdx.x * blockDim.x; b < count; b += gridDim.x * blockDim.x) {
         const int e = b + threadIdx.x;
@@ -689,7 +710,8 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
             const int r = atomicAdd(a.count, 1);
             if (r < a.capacity) {
                 float f[kFeat];
-                node_features(t, mean, g, M, nc, wc, rec, a.records + 4 * (size_t)c0, a.records + 4 * (size_t)c1,
+                node_features(t, mean, g, M, nc, wc, rec[0], rec[1], rec[2], rec[3], a.records + 4 * (size_t)c0,
+                              a.records + 4 * (size_t)c1,
                               a.dirstat[node], depth,
                               a.bp.clamp2, a.bp.cos_thr, f);
                 store_features(a.feats + (size_t)r * kFeat, f);
@@ -760,6 +782,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     const float p = cp->mlp_threshold;
     LevelArgs la{};
     la.n = n;
+    la.tiles = tiles;
     la.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
     la.records = reinterpret_cast<const float4*>(bvh->view.records);
     la.dirstat = reinterpret_cast<const float4*>(bvh->view.dirstat);

@@ -61,6 +61,24 @@ def test_band_only_cut_equals_scaled_error_bound_cut(ctx, scene_, band):
     model.close()
 
 
+def test_learned_cut_overflow_is_reported(ctx, scene_):
+    """A cut pool too small for the cut: the selection keeps what fits, reports
+    ARC_DEVERR_CUT_OVERFLOW in the device error word, and the frame still completes."""
+    d, dv, bvh, tree, gb = scene_
+    model = learned.Model(ctx, seed=6, loss=L.ARC_MLP_LOSS_BCE)
+    cut = api.cut_params(L.ARC_CUT_LEARNED, error_bound=0.01, model=model.handle.value, mlp_threshold=0.0,
+                         cut_pool_entries=2048)
+    prm = api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
+    h, w = d["pos"].shape[:2]
+    out = api.Outputs(w, h)
+    api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, cut, out)
+    assert ctx.synchronize() & L.ARC_DEVERR_CUT_OVERFLOW
+    # the next frame with room is unaffected
+    img, _ = _gather(ctx, d, bvh, gb, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01))
+    assert np.isfinite(img).all()
+    model.close()
+
+
 def test_learned_cut_evaluation_matches_oracle(ctx, scene_):
     d, dv, bvh, tree, gb = scene_
     model = learned.Model(ctx, seed=4)
