@@ -136,6 +136,16 @@ class ArcSceneDesc(C.Structure):
                 ("scene_min", ArcFloat3), ("scene_max", ArcFloat3)]
 
 
+class ArcBatchView(C.Structure):
+    _fields_ = [("avpls", ArcAvplsGpuParam), ("gbuffer", ArcGBufferView), ("camera_position", ArcFloat3),
+                ("out", ArcOutputView)]
+
+
+class ArcBatchViewDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("num_avpls", C.c_int32), ("avpl_seed", C.c_uint64),
+                ("camera_position", ArcFloat3), ("camera_target", ArcFloat3)]
+
+
 P = C.POINTER
 _vp = C.c_void_p
 _st = C.c_int32
@@ -194,6 +204,18 @@ SIGNATURES = {
     "arc_scene_trace_avpls": (_st, [P(ArcSceneDesc), C.c_uint64, C.c_int32, C.c_int32, C.c_int32, P(ArcAvplHost),
                                     P(C.c_int64)]),
     "arc_scene_gbuffer": (_st, [P(ArcSceneDesc), C.c_int32, C.c_int32, _vp, _vp]),
+    "arc_scene_batch_views": (_st, [P(ArcSceneDesc), C.c_uint64, C.c_int32, P(ArcBatchViewDesc)]),
+    "arc_batch_create": (_st, [_vp, P(_vp)]),
+    "arc_batch_destroy": (_st, [_vp]),
+    "arc_batch_render": (_st, [_vp, P(ArcBatchView), C.c_int32, P(ArcLbvhParams), P(ArcGatherParams),
+                               P(ArcCutParams)]),
+    "arc_batch_capture": (_st, [_vp, P(ArcBatchView), C.c_int32, P(ArcLbvhParams), P(ArcGatherParams),
+                                P(ArcCutParams)]),
+    "arc_batch_launch": (_st, [_vp]),
+    "arc_bruteforce_num_tile_shapes": (C.c_int32, []),
+    "arc_context_set_tile_config": (_st, [_vp, C.c_int32]),
+    "arc_autotune_bruteforce": (_st, [_vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcGatherParams),
+                                      P(ArcOutputView), P(C.c_int32), P(C.c_float), C.c_int32]),
 }
 
 _lib = None

@@ -283,3 +283,97 @@ class CudaGather:
                                      L.f3(camera_position), float(scene_extent), C.byref(config), C.byref(gv),
                                      C.byref(ov)), "arc_run")
         return self.outputs
+
+
+class Batch:
+    """Multi-view batch renderer (arc_batch_*): per view an LBVH build and a cut gather, eagerly
+    (render) or recorded once into a CUDA graph (capture) and replayed with one launch (launch)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = C.c_void_p()
+        L.check(ctx.lib.arc_batch_create(ctx.handle, C.byref(h)), "arc_batch_create")
+        self.handle = h
+        self._views = None
+        ctx._children.add(self)
+
+    @staticmethod
+    def views(items) -> C.Array:
+        """items: (ArcAvplsGpuParam, GBuffer, camera, Outputs) per view."""
+        arr = (L.ArcBatchView * len(items))()
+        for i, (av, gb, cam, out) in enumerate(items):
+            arr[i].avpls = av
+            arr[i].gbuffer = gb.view()
+            arr[i].camera_position = L.f3(cam)
+            arr[i].out = out.view()
+        return arr
+
+    def render(self, views, lbvh: L.ArcLbvhParams, gather: L.ArcGatherParams, cut: L.ArcCutParams) -> None:
+        L.check(self.ctx.lib.arc_batch_render(self.handle, views, len(views), C.byref(lbvh), C.byref(gather),
+                                              C.byref(cut)), "arc_batch_render")
+
+    def capture(self, views, lbvh: L.ArcLbvhParams, gather: L.ArcGatherParams, cut: L.ArcCutParams) -> None:
+        self._views = views  # the recorded graph refers to these views' buffers
+        L.check(self.ctx.lib.arc_batch_capture(self.handle, views, len(views), C.byref(lbvh), C.byref(gather),
+                                               C.byref(cut)), "arc_batch_capture")
+
+    def launch(self) -> None:
+        L.check(self.ctx.lib.arc_batch_launch(self.handle), "arc_batch_launch")
+
+    def close(self):
+        if self.handle and self.ctx.handle:
+            self.ctx.lib.arc_batch_destroy(self.handle)
+        self.handle = None
+
+
+class DeviceAvpls:
+    """AVPLs in caller-owned device memory (a torch buffer) in the AvplsGpuParam layout: every
+    instance keeps its own arrays, unlike Context.upload_avpls, which reuses one context buffer.
+    `param` is the ArcAvplsGpuParam view."""
+
+    def __init__(self, avpls: np.ndarray, device: int = 0):
+        torch = _torch()
+        a = np.ascontiguousarray(avpls, dtype=AVPL_DTYPE)
+        n = len(a)
+        f3 = [np.ascontiguousarray(a[k], np.float32).reshape(-1) for k in
+              ("position", "normal", "incDirection", "incRadiance", "antiradiance")]
+        i2 = [np.ascontiguousarray(a[k], np.int32) for k in ("materialIndex", "bounce")]
+        host = np.concatenate([x.view(np.uint8) for x in f3 + i2]) if n else np.zeros(64, np.uint8)
+        self.buf = torch.from_numpy(host).to(f"cuda:{device}")
+        base = self.buf.data_ptr()
+        p = L.ArcAvplsGpuParam()
+        off = [0]
+        def take(nbytes):  # noqa: E306
+            ptr = base + off[0]
+            off[0] += nbytes
+            return ptr
+        p.position = take(12 * n)
+        p.normal = take(12 * n)
+        p.incDirection = take(12 * n)
+        p.incRadiance = take(12 * n)
+        p.antiradiance = take(12 * n)
+        p.materialIndex = take(4 * n)
+        p.bounce = take(4 * n)
+        p.numAvpls = n
+        self.param = p
+
+
+def lbvh_params(**kw) -> L.ArcLbvhParams:
+    p = L.ArcLbvhParams()
+    L.load().arc_lbvh_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def autotune_bruteforce(ctx: Context, avpls: L.ArcAvplsGpuParam, gb: GBuffer, cam, params: L.ArcGatherParams,
+                        out: Outputs) -> tuple[int, np.ndarray]:
+    """arc_autotune_bruteforce: (chosen tile_config, time of every shape in ms)."""
+    n = ctx.lib.arc_bruteforce_num_tile_shapes()
+    times = np.zeros(n, np.float32)
+    best = C.c_int32()
+    gv, ov = gb.view(), out.view()
+    L.check(ctx.lib.arc_autotune_bruteforce(ctx.handle, C.byref(avpls), C.byref(gv), L.f3(cam), C.byref(params),
+                                            C.byref(ov), C.byref(best), times.ctypes.data_as(C.POINTER(C.c_float)),
+                                            n), "arc_autotune_bruteforce")
+    return int(best.value), times

@@ -109,6 +109,7 @@ struct arc_context {
     arc::StageTimer timer;
     uint64_t launches = 0;  // kernels launched by this context
     uint64_t learned_rows = 0;  // rows scored by the cut network so far
+    int32_t bf_tile_config = -1;  // brute-force launch shape for tile_config = -1 (arc_autotune_bruteforce)
 };
 
 struct arc_lbvh {

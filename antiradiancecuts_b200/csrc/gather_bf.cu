@@ -678,7 +678,8 @@ struct TileShape {
     int px;
     int chunk;
 };
-constexpr TileShape kTileShapes[] = {{1, 128}, {2, 128}, {2, 256}, {4, 128}, {4, 256}, {1, 256}, {2, 64}, {4, 64}};
+constexpr TileShape kTileShapes[] = {{1, 128}, {2, 128}, {2, 256}, {4, 128}, {4, 256}, {1, 256},
+                                     {2, 64},  {4, 64},  {1, 512}, {2, 512}};
 constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
 constexpr int kDefaultTileShape = 2;
 
@@ -795,7 +796,8 @@ arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g) {
         return ARC_OK;
     }
     ARC_TRY(pack_records(ctx, g, a, use_packed(p)));
-    const TileShape ts = kTileShapes[p.tile_config < 0 ? kDefaultTileShape : p.tile_config];
+    const int shape = p.tile_config >= 0 ? p.tile_config : (ctx->bf_tile_config >= 0 ? ctx->bf_tile_config : kDefaultTileShape);
+    const TileShape ts = kTileShapes[shape];
     a.chunk = ts.chunk;
     if (use_packed(p)) {  // only surface pixels are gathered
         int *list = nullptr, *count = nullptr;
@@ -1059,3 +1061,62 @@ extern "C" arc_status arc_gather_bruteforce_noalloc(void* cuda_stream, const Arc
     }
     return ARC_OK;
 }
+
+// Brute-force launch-shape autotuner (no counterpart in the reference): times every shape of
+// kTileShapes on the caller's workload (one warm-up and one timed run each, CUDA events on the
+// context's stream) and makes the fastest the context's default for tile_config = -1.
+extern "C" int32_t arc_bruteforce_num_tile_shapes(void) { return arc::kNumTileShapes; }
+
+extern "C" arc_status arc_context_set_tile_config(arc_context* ctx, int32_t tile_config) {
+    ARC_CHECK_ARG(ctx, "NULL context");
+    ARC_CHECK_ARG(tile_config >= -1 && tile_config < arc::kNumTileShapes, "tile_config out of range");
+    ctx->bf_tile_config = tile_config;
+    return ARC_OK;
+}
+
+extern "C" arc_status arc_autotune_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avpls,
+                                              const ArcGBufferView* gbuffer, ArcFloat3 camera_position,
+                                              const ArcGatherParams* params, const ArcOutputView* out, int32_t* best,
+                                              float* times_ms, int32_t num_shapes) {
+    using namespace arc;
+    ARC_CHECK_ARG(ctx && avpls && gbuffer && params && out && best, "NULL argument");
+    ARC_CHECK_ARG(!times_ms || num_shapes >= kNumTileShapes, "times_ms holds fewer entries than there are shapes");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ARC_TRY_CUDA(cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        ARC_TRY_CUDA(ce);
+    }
+    arc_status s = ARC_OK;
+    float best_ms = 0.0f;
+    int best_i = -1;
+    for (int i = 0; i < kNumTileShapes && s == ARC_OK; ++i) {
+        ArcGatherParams p = *params;
+        p.tile_config = i;
+        s = arc_gather_bruteforce(ctx, avpls, gbuffer, camera_position, &p, out);  // warm-up
+        if (s == ARC_OK) ce = cudaEventRecord(e0, ctx->stream);
+        if (s == ARC_OK && ce == cudaSuccess) s = arc_gather_bruteforce(ctx, avpls, gbuffer, camera_position, &p, out);
+        if (s == ARC_OK && ce == cudaSuccess) ce = cudaEventRecord(e1, ctx->stream);
+        if (s == ARC_OK && ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float ms = -1.0f;
+        if (s == ARC_OK && ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+        if (ce != cudaSuccess && s == ARC_OK) {
+            set_last_error(std::string("arc_autotune_bruteforce: ") + cudaGetErrorString(ce));
+            s = ARC_ERR_CUDA;
+        }
+        if (times_ms) times_ms[i] = ms;
+        if (s == ARC_OK && (best_i < 0 || ms < best_ms)) {
+            best_ms = ms;
+            best_i = i;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ARC_TRY(s);
+    ctx->bf_tile_config = best_i;
+    *best = best_i;
+    return ARC_OK;
+}
+

@@ -332,3 +332,43 @@ extern "C" arc_status arc_scene_gbuffer(const ArcSceneDesc* scene, int32_t width
     }
     return ARC_OK;
 }
+
+extern "C" arc_status arc_scene_batch_views(const ArcSceneDesc* scene, uint64_t seed, int32_t count,
+                                            ArcBatchViewDesc* out) {
+    if (!scene || !out || count < 0) return ARC_ERR_INVALID_ARG;
+    static const int32_t kRes[4][2] = {{256, 256}, {512, 512}, {1280, 720}, {1920, 1080}};
+    arc_pcg32 rng;
+    arc_pcg32_seed(&rng, seed, 0);
+    const float lo[3] = {scene->scene_min.x, scene->scene_min.y, scene->scene_min.z};
+    const float hi[3] = {scene->scene_max.x, scene->scene_max.y, scene->scene_max.z};
+    auto inside_box = [&](const float* p) {
+        for (int b = 0; b < scene->num_boxes; ++b) {
+            const ArcBox& x = scene->boxes[b];
+            if (p[0] > x.lo.x && p[0] < x.hi.x && p[1] > x.lo.y && p[1] < x.hi.y && p[2] > x.lo.z && p[2] < x.hi.z)
+                return true;
+        }
+        return false;
+    };
+    for (int32_t v = 0; v < count; ++v) {
+        ArcBatchViewDesc& d = out[v];
+        const int r = (int)(arc_pcg32_next(&rng) % 4u);
+        d.width = kRes[r][0];
+        d.height = kRes[r][1];
+        // log-uniform in [2^13, 2^18]
+        d.num_avpls = (int32_t)std::lround(std::exp2(13.0 + 5.0 * (double)arc_pcg32_float(&rng)));
+        d.avpl_seed = ((uint64_t)arc_pcg32_next(&rng) << 32) | arc_pcg32_next(&rng);
+        float c[3], t[3];
+        for (int tries = 0; tries < 1000; ++tries) {  // a camera outside every box, 10% in from the walls
+            for (int k = 0; k < 3; ++k) c[k] = lo[k] + (hi[k] - lo[k]) * (0.1f + 0.8f * arc_pcg32_float(&rng));
+            if (!inside_box(c)) break;
+        }
+        for (int tries = 0; tries < 1000; ++tries) {  // a target at least 0.3 away
+            for (int k = 0; k < 3; ++k) t[k] = lo[k] + (hi[k] - lo[k]) * arc_pcg32_float(&rng);
+            const float dx = t[0] - c[0], dy = t[1] - c[1], dz = t[2] - c[2];
+            if (dx * dx + dy * dy + dz * dz >= 0.09f) break;
+        }
+        d.camera_position = ArcFloat3{c[0], c[1], c[2]};
+        d.camera_target = ArcFloat3{t[0], t[1], t[2]};
+    }
+    return ARC_OK;
+}

@@ -98,3 +98,24 @@ WORKLOADS = {
     "variant500_1080p_1m": Workload("variant500_1080p_1m", L.ARC_SCENE_TRAIN_VARIANT, 500, 0, 500, 1920, 1080,
                                     1 << 20, 3),
 }
+
+
+def batch_views(desc: L.ArcSceneDesc, seed: int, count: int) -> list[L.ArcBatchViewDesc]:
+    """Views of a multi-view batch in `desc` (arc_scene_batch_views): resolution, AVPL count and
+    seed, camera pose inside the room."""
+    out = (L.ArcBatchViewDesc * count)()
+    L.check(L.load().arc_scene_batch_views(C.byref(desc), int(seed), int(count), out), "arc_scene_batch_views")
+    return list(out)
+
+
+def view_inputs(desc: L.ArcSceneDesc, view: L.ArcBatchViewDesc, max_bounces: int = 3, scale: float = 1.0):
+    """(AVPLs, position, normal) of one batch view: its own AVPL set and its camera's G-buffer
+    (resolution scaled by `scale`, for reduced test sizes)."""
+    d = L.ArcSceneDesc()
+    C.memmove(C.byref(d), C.byref(desc), C.sizeof(d))
+    d.camera_position = view.camera_position
+    d.camera_target = view.camera_target
+    avpls, _ = trace_avpls(d, view.avpl_seed, view.num_avpls, max_bounces)
+    w, h = max(8, int(view.width * scale)), max(8, int(view.height * scale))
+    pos, nrm = gbuffer(d, w, h)
+    return avpls, pos, nrm

@@ -167,6 +167,57 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
                       f"{dt:.1f} s, extrapolated to {len(valid)} surface pixels"}
 
 
+def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
+    """Multi-view batch: views of the room + 2 boxes scene drawn with seed 4 (resolutions from
+    {256^2, 512^2, 1280x720, 1920x1080}, 8,192 - 262,144 AVPLs each, log-uniform, camera inside the
+    room), each with its own AVPL set; per view an LBVH build and an error-bound cut gather (eps
+    0.01).  Timed eagerly (host loop over views) and as one recorded CUDA graph launch."""
+    import torch
+
+    desc = scene.scene_desc(L.ARC_SCENE_ROOM_2BOXES, 2, 2)
+    mats, _, _, _ = scene.materials(desc)
+    ctx.upload_materials(mats)
+    items, keep = [], []
+    pixels = avpl_total = 0
+    for v in scene.batch_views(desc, 4, num_views):
+        avpls, pos, nrm = scene.view_inputs(desc, v)
+        dv = api.DeviceAvpls(avpls)
+        out = api.Outputs(v.width, v.height, fp64=False, parts=False)
+        keep.append((dv, out))
+        items.append((dv.param, api.GBuffer(pos, nrm), (v.camera_position.x, v.camera_position.y, v.camera_position.z),
+                      out))
+        pixels += v.width * v.height
+        avpl_total += v.num_avpls
+    views = api.Batch.views(items)
+    lp, gp = api.lbvh_params(), api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
+    cp = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01)
+    b = api.Batch(ctx)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.render(views, lp, gp, cp)  # warm-up (sizes every buffer)
+    assert ctx.synchronize() == 0
+    reps = 3
+    e0.record(stream)
+    for _ in range(reps):
+        b.render(views, lp, gp, cp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    eager = e0.elapsed_time(e1) / reps
+    b.capture(views, lp, gp, cp)
+    b.launch()
+    assert ctx.synchronize() == 0
+    e0.record(stream)
+    for _ in range(reps):
+        b.launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    graph = e0.elapsed_time(e1) / reps
+    assert ctx.synchronize() == 0
+    b.close()
+    return {"views": num_views, "pixels": pixels, "avpls": avpl_total, "ms_per_batch_eager": eager,
+            "ms_per_batch_graph": graph, "graph_launches_per_batch": 1, "cut": "error bound 0.01",
+            "views_per_s": num_views * 1000.0 / graph}
+
+
 def run_reference(args):
     """--impl reference: the CPU gather on the host cores (rank 0 only)."""
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
@@ -210,6 +261,7 @@ def main():
     ap.add_argument("--small", action="store_true", help="640x360 / 262,144 AVPLs, no extras (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip exact / FP64 / CPU legs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--batch-views", type=int, default=32, help="views of the multi-view batch leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -436,6 +488,10 @@ def main():
                            ref64=ref64)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
+    batch = None
+    if not args.no_extras:
+        batch = batch_leg(ctx, api, scene, L, stream, args.batch_views)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -453,7 +509,7 @@ def main():
             "roofline": roof, "cut_eval_roofline": eval_roof, "lbvh_roofline": lbvh_roof, **result,
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
-            "cpu_baseline": cpu, "clocks": clk,
+            "cpu_baseline": cpu, "clocks": clk, "batch": batch,
         }
         if method != "learned" and args.method == "auto":
             line["config"]["learned_unavailable"] = model_error[:200]

@@ -452,6 +452,50 @@ arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcF
                    const ArcOutputView* out);
 
 /* ---------------------------------------------------------------------------------------- */
+/* Batched multi-view rendering and the brute-force tile-shape autotuner (no counterpart in  */
+/* the reference, whose CudaGather::run renders one view per call with fixed launch shapes)  */
+/* ---------------------------------------------------------------------------------------- */
+
+/* One view of a batch: its own AVPL set (device arrays), G-buffer, camera and output planes. */
+typedef struct ArcBatchView {
+    ArcAvplsGpuParam avpls;
+    ArcGBufferView gbuffer;
+    ArcFloat3 camera_position;
+    ArcOutputView out;
+} ArcBatchView;
+
+typedef struct arc_batch arc_batch;
+
+/* A batch renderer on `ctx`: it owns one LBVH that every view's build reuses in turn. */
+arc_status arc_batch_create(arc_context* ctx, arc_batch** out);
+arc_status arc_batch_destroy(arc_batch* batch);
+/* Per view, in order, on the context's stream: the LBVH build of its AVPLs (`lbvh`) and the cut
+ * gather (`cut`; SOLID_ANGLE, ERROR_BOUND or LEARNED) into its outputs.  Enqueued only. */
+arc_status arc_batch_render(arc_batch* batch, const ArcBatchView* views, int32_t num_views, const ArcLbvhParams* lbvh,
+                            const ArcGatherParams* gather, const ArcCutParams* cut);
+/* Records arc_batch_render of these views into one CUDA graph: it first renders them once eagerly
+ * (sizing every library buffer), then captures the same work from the context's stream.  The views'
+ * buffers must stay valid and in place while the graph is used.  ERROR_BOUND cuts only (the learned
+ * selection reads its frontier size on the host).  Replaces any previously recorded graph. */
+arc_status arc_batch_capture(arc_batch* batch, const ArcBatchView* views, int32_t num_views,
+                             const ArcLbvhParams* lbvh, const ArcGatherParams* gather, const ArcCutParams* cut);
+/* Replays the recorded graph on the context's stream: the whole batch in one launch.  Enqueued
+ * only; the device error word collects the views' device errors. */
+arc_status arc_batch_launch(arc_batch* batch);
+
+/* Times every brute-force launch shape (pixel tile 16 x 16 PX, PX in {1, 2, 4}, AVPL chunk 64 ...
+ * 512, ArcGatherParams.tile_config index) on this workload and makes the fastest the context's
+ * default for tile_config = -1.  times_ms[num_shapes] (optional) receives each shape's time
+ * (< 0 where it does not apply); *best the chosen index.  Waits for the stream; writes `out`. */
+int32_t arc_bruteforce_num_tile_shapes(void);
+/* Sets the context's default launch shape for tile_config = -1 (-1: the library's built-in one),
+ * e.g. to apply a shape tuned earlier. */
+arc_status arc_context_set_tile_config(arc_context* ctx, int32_t tile_config);
+arc_status arc_autotune_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avpls, const ArcGBufferView* gbuffer,
+                                   ArcFloat3 camera_position, const ArcGatherParams* params, const ArcOutputView* out,
+                                   int32_t* best, float* times_ms, int32_t num_shapes);
+
+/* ---------------------------------------------------------------------------------------- */
 /* Synthetic scenes (CPU): inputs for tests and benchmarks                                   */
 /* ---------------------------------------------------------------------------------------- */
 
@@ -501,6 +545,20 @@ arc_status arc_scene_trace_avpls(const ArcSceneDesc* scene, uint64_t seed, int32
  * Row 0 is the top of the image. */
 arc_status arc_scene_gbuffer(const ArcSceneDesc* scene, int32_t width, int32_t height, float* position,
                              float* normal);
+
+/* Views of a multi-view batch in `scene`: camera inside the room (outside every box) looking at a
+ * point of the room at least 0.3 away, resolution drawn uniformly from {256x256, 512x512,
+ * 1280x720, 1920x1080}, AVPL count log-uniform in [8192, 262144], and a seed for the view's own
+ * AVPL set; all drawn from the PCG32 stream (seed, 0). */
+typedef struct ArcBatchViewDesc {
+    int32_t width;
+    int32_t height;
+    int32_t num_avpls;
+    uint64_t avpl_seed;
+    ArcFloat3 camera_position;
+    ArcFloat3 camera_target;
+} ArcBatchViewDesc;
+arc_status arc_scene_batch_views(const ArcSceneDesc* scene, uint64_t seed, int32_t count, ArcBatchViewDesc* out);
 
 #ifdef __cplusplus
 }
