@@ -311,11 +311,8 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 const TileInfo ti = load_tile_info(a.info, tile, &mean);
                 const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
                 const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
-                // the node's whole record and direction statistics depend only on the pair: load them
-                // with the bounds (the features need them when the network scores the node)
                 const float4* rec = a.records + 4 * (size_t)node;
-                const float4 q0 = rec[0], q1 = rec[1], q2 = rec[2], q3 = rec[3];
-                const float4 ds = a.dirstat[node];
+                const float4 q2 = rec[2], q3 = rec[3];
                 const NodeGeom g = node_geom(ti, b0, b1, nc, wc, a.bp);
                 const float M = node_bound(ti, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
                 lc = child_index(__float_as_int(b0.w), a.n);
@@ -323,8 +320,8 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 if (M > ti.tau) action = M > a.band * ti.tau ? kRefine : kScore;
                 if (action == kScore) {
                     float f[kFeat];
-                    node_features(ti, mean, g, M, nc, wc, q0, q1, q2, q3, a.records + 4 * (size_t)lc,
-                                  a.records + 4 * (size_t)rc, ds, depth, a.clamp2, a.cos_thr, f);
+                    node_features(ti, mean, g, M, nc, wc, rec[0], rec[1], q2, q3, a.records + 4 * (size_t)lc,
+                                  a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
                     // < kStageRows: fewer than kLevelThreads rows are left over from the last round
                     const int slot = atomicAdd(&s_staged, 1);
                     uint4 x0, x1;
