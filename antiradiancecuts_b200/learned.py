@@ -51,7 +51,7 @@ class Model:
     threshold recommended for it (probability for a classifier, relative error for a regressor)."""
 
     def __init__(self, ctx: api.Context, params: np.ndarray | None = None, seed: int = 1,
-                 loss: int = L.ARC_MLP_LOSS_BCE, threshold: float | None = None):
+                 loss: int = L.ARC_MLP_LOSS_BCE, threshold: float | None = None, band: float = PREACCEPT_BAND):
         self.ctx = ctx
         h = C.c_void_p()
         L.check(ctx.lib.arc_mlp_create(ctx.handle, seed, C.byref(h)), "arc_mlp_create")
@@ -60,16 +60,19 @@ class Model:
         L.check(ctx.lib.arc_mlp_set_loss(h, int(loss)), "arc_mlp_set_loss")
         self.loss = int(loss)
         self.threshold = threshold if threshold is not None else (0.5 if loss == L.ARC_MLP_LOSS_BCE else 1e-4)
+        self.band = float(band)  # the analytic refine band the network was trained within
         if params is not None:
             self.set_params(params)
 
     def save(self, path: str) -> None:
-        np.savez(path, params=self.params(), loss=np.int32(self.loss), threshold=np.float32(self.threshold))
+        np.savez(path, params=self.params(), loss=np.int32(self.loss), threshold=np.float32(self.threshold),
+                 band=np.float32(self.band))
 
     @classmethod
     def load(cls, ctx: api.Context, path: str) -> "Model":
         z = np.load(path)
-        return cls(ctx, z["params"], loss=int(z["loss"]), threshold=float(z["threshold"]))
+        return cls(ctx, z["params"], loss=int(z["loss"]), threshold=float(z["threshold"]),
+                   band=float(z["band"]) if "band" in z else PREACCEPT_BAND)
 
     def set_params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, np.float32)
@@ -92,7 +95,7 @@ class Model:
 
 def cut_params(model: Model, threshold: float | None = None, **kw):
     """ArcCutParams of the learned cut with the pre-acceptance the model was trained with."""
-    kw.setdefault("mlp_band", PREACCEPT_BAND)
+    kw.setdefault("mlp_band", model.band)
     return api.cut_params(L.ARC_CUT_LEARNED, error_bound=PREACCEPT_EPS, ar_uncertain_factor=PREACCEPT_K,
                           model=model.handle.value,
                           mlp_threshold=model.threshold if threshold is None else threshold, **kw)
@@ -224,6 +227,7 @@ def main(argv=None):
     tr.add_argument("--epochs", type=float, default=4.0)
     tr.add_argument("--delta", type=float, default=LABEL_DELTA)
     tr.add_argument("--objective", choices=["regression", "classification"], default="classification")
+    tr.add_argument("--band", type=float, default=PREACCEPT_BAND)
     tr.add_argument("--threshold", type=float, default=None, help="selection threshold stored with the model")
     tr.add_argument("--out", default=DEFAULT_MODEL)
     a = ap.parse_args(argv)
@@ -236,7 +240,7 @@ def main(argv=None):
     t0 = time.time()
     seeds = list(TRAIN_SEEDS)[: a.scenes]
     for s in seeds:
-        f, l, e = scene_samples(ctx, s, capacity=24 * per_scene, delta=a.delta)
+        f, l, e = scene_samples(ctx, s, capacity=24 * per_scene, delta=a.delta, band=a.band)
         if regress:
             l = torch.log2(torch.clamp(e, min=2.0 ** LOG2_FLOOR))
         if f.shape[0] > per_scene:  # uniform subsample to the per-scene budget
@@ -255,6 +259,7 @@ def main(argv=None):
     val, trn = perm[:nv], perm[nv:]
     loss = L.ARC_MLP_LOSS_SQUARED if regress else L.ARC_MLP_LOSS_BCE
     model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs, loss=loss)
+    model.band = a.band
     # the shipped classifier refines at P(refine) >= 0.01: within 1% RMSE on the held-out scene
     model.threshold = a.threshold if a.threshold is not None else (0.01 if not regress else 1e-4)
     print("validation:", evaluate(ctx, model, feats[val].contiguous(), labels[val].contiguous(), a.delta), flush=True)
