@@ -43,7 +43,7 @@ LOG2_FLOOR = -30.0  # regression targets: log2 of the relative error, at least t
 # network; the network decides the nodes in between (it prunes refinements of the analytic cut)
 PREACCEPT_EPS = 2e-3
 PREACCEPT_K = 16.0
-PREACCEPT_BAND = 16.0
+PREACCEPT_BAND = 64.0
 
 
 class Model:
@@ -260,8 +260,8 @@ def main(argv=None):
     loss = L.ARC_MLP_LOSS_SQUARED if regress else L.ARC_MLP_LOSS_BCE
     model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs, loss=loss)
     model.band = a.band
-    # the shipped classifier refines at P(refine) >= 0.01: within 1% RMSE on the held-out scene
-    model.threshold = a.threshold if a.threshold is not None else (0.01 if not regress else 1e-4)
+    # the shipped classifier refines at P(refine) >= 0.05: within 1% RMSE on the held-out scene
+    model.threshold = a.threshold if a.threshold is not None else (0.05 if not regress else 1e-4)
     print("validation:", evaluate(ctx, model, feats[val].contiguous(), labels[val].contiguous(), a.delta), flush=True)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
     model.save(a.out)
