@@ -484,13 +484,41 @@ struct EvalArgs {
     float4* out_ar;
     double* out_res64;
     int64_t opitch;
+    const int* order;  // block b evaluates tile order[b]
 };
+
+// Tiles in decreasing order of cut size (buckets of floor(log2(count)), empty tiles last), so that
+// the blocks with the longest cuts start first and the short ones fill the tail of the launch.
+// One block; the order within a bucket is arbitrary (each tile's result does not depend on it).
+__global__ void __launch_bounds__(1024) tile_order_kernel(const int32_t* counts, int tiles, int* order) {
+    __shared__ int hist[33], off[33];
+    const int t = threadIdx.x;
+    if (t < 33) hist[t] = 0;
+    __syncthreads();
+    for (int i = t; i < tiles; i += blockDim.x) {
+        const int c = counts[i];
+        atomicAdd(&hist[c > 0 ? 32 - __clz(c) : 0], 1);
+    }
+    __syncthreads();
+    if (t == 0) {
+        int s = 0;
+        for (int b = 32; b >= 0; --b) {
+            off[b] = s;
+            s += hist[b];
+        }
+    }
+    __syncthreads();
+    for (int i = t; i < tiles; i += blockDim.x) {
+        const int c = counts[i];
+        order[atomicAdd(&off[c > 0 ? 32 - __clz(c) : 0], 1)] = i;
+    }
+}
 
 template <int AR>
 __global__ void __launch_bounds__(64) cut_eval_kernel(EvalArgs a) {
     constexpr int kChunk = 256;
     __shared__ float4 srec[kChunk * 4];
-    const int tile = blockIdx.x;
+    const int tile = a.order[blockIdx.x];
     const int i = threadIdx.x;
     const int x = (tile % a.tiles_x) * kTile + i % kTile, y = (tile / a.tiles_x) * kTile + i / kTile;
     bool valid = x < a.width && y < a.height;
@@ -586,7 +614,7 @@ template <int AR>
 __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
     constexpr int kChunk = 256;
     __shared__ __align__(16) float srec[kChunk * 16];
-    const int tile = blockIdx.x;
+    const int tile = a.order[blockIdx.x];
     const int i = threadIdx.x;
     const int x = (tile % a.tiles_x) * kTile + i % kTile, y = (tile / a.tiles_x) * kTile + i / kTile;
     bool valid = x < a.width && y < a.height;
@@ -870,11 +898,15 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ea.out_ar = reinterpret_cast<float4*>(out->antiradiance);
     ea.out_res64 = out->result_fp64;
     ea.opitch = out->pitch;
+    int* order = nullptr;
+    ARC_TRY(ctx->arena.get("cut_order", (size_t)tiles * sizeof(int), reinterpret_cast<void**>(&order)));
+    ea.order = order;
     stage_begin(ctx, "cut_eval");
+    tile_order_kernel<<<1, 1024, 0, st>>>(pool.counts, tiles, order);
     if (gp->ar_kind == 0) cut_eval_packed_kernel<0><<<tiles, 64, 0, st>>>(ea);
     if (gp->ar_kind == 1) cut_eval_kernel<1><<<tiles, 64, 0, st>>>(ea);
     if (gp->ar_kind == 2) cut_eval_packed_kernel<2><<<tiles, 64, 0, st>>>(ea);
-    stage_end(ctx, 1);
+    stage_end(ctx, 2);
     ARC_TRY_CUDA(cudaGetLastError());
     ctx->last_cut.num_tiles = tiles;
     ctx->last_cut.pool = pool;

@@ -290,15 +290,24 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     bool ok = __syncthreads_and(mbar_wait_bounded(&wbar, 0, a.err)) != 0;
     mlp::InferCta c{smem_u32(sm), fW, fH, sm, vec, tmem_base, &bar, 0u, a.err};
     unsigned long long scored = 0;
+    // The next chunk's index and entries are fetched one chunk ahead, so that neither the work
+    // counter's round trip nor the entry load sits on the chain of dependent loads of a chunk.
+    if (t == 0) s_chunk = atomicAdd(a.work, 1);
+    __syncthreads();
+    int chunk = s_chunk;
+    int2 en_next = make_int2(0, 0);
+    if ((int64_t)chunk * kLevelThreads + t < count) en_next = a.in[(int64_t)chunk * kLevelThreads + t];
     while (ok) {
-        if (t == 0) s_chunk = atomicAdd(a.work, 1);
-        __syncthreads();  // also: every thread has read s_staged before this chunk adds to it
-        const int64_t first = (int64_t)s_chunk * kLevelThreads;
+        // every thread has read s_chunk and s_staged before they change again
+        __syncthreads();
+        const int64_t first = (int64_t)chunk * kLevelThreads;
         const bool done = first >= count;
         const int64_t e = first + t;
+        int next = 0;
+        if (t == 0 && !done) next = atomicAdd(a.work, 1);
         int action = kNone, tile = 0, node = 0, lc = 0, rc = 0, depth = 0;
         if (!done && e < count) {
-            const int2 en = a.in[e];
+            const int2 en = en_next;
             const bool good = valid_entry(en, a.tiles, a.n);
             if (!good) set_error(a.err, en.x == -1 ? ARC_DEVERR_CUT_OVERFLOW : ARC_DEVERR_BAD_NODE);
             tile = good ? en.x : 0;
@@ -339,30 +348,39 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 }
             }
         }
+        if (t == 0 && !done) s_chunk = next;
         // emit's barriers also order every staging of this chunk before s_staged is read
         emit(a, s_emit, action, tile, node, lc, rc, depth);
+        if (!done) {
+            chunk = s_chunk;
+            const int64_t en = (int64_t)chunk * kLevelThreads + t;
+            if (en < count) en_next = a.in[en];
+        }
         int staged = s_staged;
         // score full tiles now, and whatever is left once the level is exhausted
         while (staged >= kLevelThreads || (done && staged > 0)) {
+            const int n_rows = min(staged, kLevelThreads);
+            // the children of every staged (inner) node are fetched while the network runs
+            int2 m = make_int2(0, 0);
+            int cl = 0, cr = 0;
+            if (t < n_rows) {
+                m = meta[t];
+                const int mn = m.y & ((1 << kDepthShift) - 1);
+                if (mn >= a.n) {
+                    const size_t k = (size_t)(mn - a.n);
+                    cl = __float_as_int(a.bounds[4 * k].w);
+                    cr = __float_as_int(a.bounds[4 * k + 1].w);
+                }
+            }
             float y = 0.0f;
             if (!mlp::infer_tiles<kLevelTiles>(c, fX, t, &y)) {
                 ok = false;
                 break;
             }
-            const int n_rows = min(staged, kLevelThreads);
             scored += n_rows;
-            int act = kNone, mlc = 0, mrc = 0;
-            int2 m = make_int2(0, 0);
-            if (t < n_rows) {
-                m = meta[t];
-                act = y >= a.thr_logit ? kRefine : kAccept;
-            }
+            const int act = t < n_rows ? (y >= a.thr_logit ? kRefine : kAccept) : kNone;
             const int mnode = m.y & ((1 << kDepthShift) - 1), mdepth = m.y >> kDepthShift;
-            if (act == kRefine) {  // an inner node: its children from the bounds
-                const size_t k = (size_t)(mnode - a.n);
-                mlc = child_index(__float_as_int(a.bounds[4 * k].w), a.n);
-                mrc = child_index(__float_as_int(a.bounds[4 * k + 1].w), a.n);
-            }
+            const int mlc = child_index(cl, a.n), mrc = child_index(cr, a.n);
             // after emit's barriers every thread has read its pair: the rows can be moved
             emit(a, s_emit, act, m.x, mnode, mlc, mrc, mdepth);
             const int rest = staged - n_rows;
