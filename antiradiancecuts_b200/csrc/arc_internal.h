@@ -145,9 +145,10 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
                              const ArcGBufferView* gb, float3 cam, const ArcGatherParams* gp, const ArcCutParams* cp,
                              const ArcOutputView* out);
 arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64);
-// per-tile set-up of the tile cuts (bounds, normal cone, albedo, coarse estimate, threshold)
+// per-tile set-up of the tile cuts (bounds, normal cone, albedo, coarse estimate, threshold) and
+// the per-node parts of the cut bound (NodeExtra, two float4 per inner node)
 arc_status launch_tile_setup(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gb, const ArcGatherParams* gp,
-                             const ArcCutParams* cp, float4** info_out);
+                             const ArcCutParams* cp, float4** info_out, float4** extra_out);
 
 }  // namespace arc
 

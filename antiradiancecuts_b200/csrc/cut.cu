@@ -27,8 +27,8 @@ namespace arc {
 
 arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64);
 arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, const ArcGatherParams* gp,
-                                     const ArcCutParams* cp, const float4* tiles_info, int tiles_x, int tiles_y,
-                                     const CutPool& pool);
+                                     const ArcCutParams* cp, const float4* tiles_info, const float4* extra,
+                                     int tiles_x, int tiles_y, const CutPool& pool);
 
 namespace {
 
@@ -358,8 +358,22 @@ __global__ void __launch_bounds__(32 * kSelWarps) cut_tile_setup(TileArgs a) {
         info[0] = make_float4(tmin[0], tmin[1], tmin[2], kdl);
         info[1] = make_float4(tmax[0], tmax[1], tmax[2], rn_mul(a.eps_bound, mean));
         info[2] = cone;
-        info[3] = make_float4(__int_as_float(nvalid), mean, 0.0f, 0.0f);
+        info[3] = make_float4(__int_as_float(nvalid), mean,
+                              half_diagonal(rn_sub(tmax[0], tmin[0]), rn_sub(tmax[1], tmin[1]), rn_sub(tmax[2], tmin[2])),
+                              cone_sine(cone.w));
     }
+}
+
+// NodeExtra of every inner node k (bounds at 4 k, record at 4 (n + k)), for node_geom / node_bound
+__global__ void cut_node_extra(int n, const float4* bounds, const float4* records, float4* ext) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n - 1) return;
+    const float4 b0 = bounds[4 * (size_t)k], b1 = bounds[4 * (size_t)k + 1];
+    const float4 nc = bounds[4 * (size_t)k + 2], wc = bounds[4 * (size_t)k + 3];
+    const float4 q2 = records[4 * ((size_t)n + k) + 2], q3 = records[4 * ((size_t)n + k) + 3];
+    const float rn = half_diagonal(rn_sub(b1.x, b0.x), rn_sub(b1.y, b0.y), rn_sub(b1.z, b0.z));
+    ext[2 * (size_t)k] = make_float4(rn, cone_sine(nc.w), cone_sine(wc.w), lum3(q2.y, q2.z, q2.w));
+    ext[2 * (size_t)k + 1] = make_float4(lum3(q3.x, q3.y, q3.z), 0.0f, 0.0f, 0.0f);
 }
 
 __device__ __forceinline__ TileInfo load_tile(const float4* info, int tile) {
@@ -370,6 +384,8 @@ __device__ __forceinline__ TileInfo load_tile(const float4* info, int tile) {
     t.tmax[0] = i1.x; t.tmax[1] = i1.y; t.tmax[2] = i1.z; t.tau = i1.w;
     t.ncone = i2;
     t.valid = __float_as_int(i3.x);
+    t.rt = i3.z;
+    t.sn = i3.w;
     return t;
 }
 
@@ -381,6 +397,7 @@ struct SelArgs {
     const float4* bounds;
     const float4* records;
     const float4* info;
+    const float4* extra;  // NodeExtra per inner node
     BoundParams bp;
     int tiles;
     CutPool pool;
@@ -425,9 +442,9 @@ __global__ void __launch_bounds__(32 * kSelWarps) cut_select_bound(SelArgs a) {
                 const int k = node - a.n;
                 const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
                 const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
-                const float4 q2 = a.records[4 * (size_t)node + 2], q3 = a.records[4 * (size_t)node + 3];
-                const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
-                const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
+                const NodeExtra ne = load_node_extra(a.extra, k);
+                const NodeGeom g = node_geom(t, b0, b1, nc, wc, ne, a.bp);
+                const float M = node_bound(t, g, ne.Ls, ne.As, a.bp);
                 if (M > t.tau) {
                     refine = true;
                     const int l = __float_as_int(b0.w), r = __float_as_int(b1.w);
@@ -740,7 +757,7 @@ __global__ void combine_kernel(const double* rad64, const double* ar64, int widt
 }  // namespace
 
 arc_status launch_tile_setup(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gb, const ArcGatherParams* gp,
-                             const ArcCutParams* cp, float4** info_out) {
+                             const ArcCutParams* cp, float4** info_out, float4** extra_out) {
     const int W = gb->width, H = gb->height;
     const int tiles_x = (W + kTile - 1) / kTile, tiles_y = (H + kTile - 1) / kTile, tiles = tiles_x * tiles_y;
     float4* info = nullptr;
@@ -761,11 +778,15 @@ arc_status launch_tile_setup(arc_context* ctx, const arc_lbvh* bvh, const ArcGBu
     ta.tiles_x = tiles_x;
     ta.tiles_y = tiles_y;
     ta.info = info;
+    float4* extra = nullptr;
+    ARC_TRY(ctx->arena.get("node_extra", (size_t)(bvh->n - 1) * 2 * sizeof(float4), reinterpret_cast<void**>(&extra)));
     stage_begin(ctx, "cut_setup");
     cut_tile_setup<<<(tiles + kSelWarps - 1) / kSelWarps, 32 * kSelWarps, 0, ctx->stream>>>(ta);
-    stage_end(ctx, 1);
+    cut_node_extra<<<(bvh->n - 1 + 255) / 256, 256, 0, ctx->stream>>>(bvh->n, ta.bounds, ta.records, extra);
+    stage_end(ctx, 2);
     ARC_TRY_CUDA(cudaGetLastError());
     *info_out = info;
+    *extra_out = extra;
     return ARC_OK;
 }
 
@@ -844,7 +865,8 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     ARC_TRY(ctx->arena.get("cut_pool_next", sizeof(int32_t), reinterpret_cast<void**>(&pool.next)));
     ARC_TRY_CUDA(cudaMemsetAsync(pool.next, 0, sizeof(int32_t), st));
     float4* info = nullptr;
-    ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info));
+    float4* extra = nullptr;
+    ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info, &extra));
     TileArgs ta;
     ta.gpos = reinterpret_cast<const float4*>(gb->position);
     ta.gnrm = reinterpret_cast<const float4*>(gb->normal);
@@ -857,6 +879,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
         sa.bounds = ta.bounds;
         sa.records = ta.records;
         sa.info = info;
+        sa.extra = extra;
         sa.bp.clamp2 = clamp2;
         sa.bp.ar_kind = gp->ar_kind;
         sa.bp.eps_cone = 0.001f;
@@ -874,7 +897,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
         ARC_TRY_CUDA(cudaGetLastError());
     } else {
         ARC_CHECK_ARG(cp->model != nullptr, "ARC_CUT_LEARNED needs a model");
-        ARC_TRY(launch_cut_select_learned(ctx, bvh, gp, cp, info, tiles_x, tiles_y, pool));
+        ARC_TRY(launch_cut_select_learned(ctx, bvh, gp, cp, info, extra, tiles_x, tiles_y, pool));
     }
 
     EvalArgs ea;

@@ -15,7 +15,25 @@ struct TileInfo {
     float kdl;               // max luminance of the receivers' diffuse/pi
     float tau;               // error threshold: eps * mean coarse estimate
     int valid;               // valid pixel count
+    float rt;                // half-diagonal of the box (half_diagonal)
+    float sn;                // sine of the normal cone's half-angle (cone_sine)
 };
+
+// Per inner node, the pair-independent parts of node_geom / node_bound, computed once per cut
+// selection (cut_node_extra) with the same rounded operations, so the results are unchanged.
+struct NodeExtra {
+    float rn;   // half-diagonal of the node's box
+    float snc;  // sine of the normal cone's half-angle
+    float swc;  // sine of the direction cone's half-angle
+    float Ls;   // luminance of the summed radiance
+    float As;   // luminance of the summed antiradiance
+};
+
+// two float4 per inner node: {rn, snc, swc, Ls}, {As, 0, 0, 0}
+__device__ __forceinline__ NodeExtra load_node_extra(const float4* ext, int k) {
+    const float4 e0 = ext[2 * (size_t)k], e1 = ext[2 * (size_t)k + 1];
+    return NodeExtra{e0.x, e0.y, e0.z, e0.w, e1.x};
+}
 
 struct BoundParams {
     float clamp2;    // dist clamp squared (0 = off)
@@ -30,16 +48,23 @@ __device__ __forceinline__ float lum3(float r, float g, float b) {
     return rn_add(rn_add(rn_mul(0.2126f, r), rn_mul(0.7152f, g)), rn_mul(0.0722f, b));
 }
 
+// sin of a cone's half-angle from its cosine
+__device__ __forceinline__ float cone_sine(float c) { return rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(c, c)))); }
+
+// half the length of a box's diagonal (extents ex, ey, ez)
+__device__ __forceinline__ float half_diagonal(float ex, float ey, float ez) {
+    return rn_mul(0.5f, rn_sqrt(rn_dot(ex, ey, ez, ex, ey, ez)));
+}
+
 // max over members of two cones of cos(angle between them), clamped to [0, 1] is left to the
-// caller; returns 1 when the cones overlap.  (a1, c1), (a2, c2): axis and cos half-angle.
-__device__ __forceinline__ float cone_max_cos(float a1x, float a1y, float a1z, float c1, float a2x, float a2y, float a2z,
-                                              float c2) {
+// caller; returns 1 when the cones overlap.  (a1, c1, s1), (a2, c2, s2): axis, cos and sin
+// (cone_sine) of the half-angle.
+__device__ __forceinline__ float cone_max_cos(float a1x, float a1y, float a1z, float c1, float s1, float a2x, float a2y,
+                                              float a2z, float c2, float s2) {
     if (c1 <= -1.0f || c2 <= -1.0f) return 1.0f;
     float cb = rn_dot(a1x, a1y, a1z, a2x, a2y, a2z);
     cb = fminf(fmaxf(cb, -1.0f), 1.0f);
-    const float sb = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(cb, cb))));
-    const float s1 = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(c1, c1))));
-    const float s2 = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(c2, c2))));
+    const float sb = cone_sine(cb);
     const float cg = rn_sub(rn_mul(c1, c2), rn_mul(s1, s2));
     const float sg = rn_add(rn_mul(s1, c2), rn_mul(c1, s2));
     if (sg < 0.0f) return 1.0f;   // combined half-angles exceed pi
@@ -48,14 +73,12 @@ __device__ __forceinline__ float cone_max_cos(float a1x, float a1y, float a1z, f
 }
 
 // min over members of two cones of cos(angle between them); -1 when they can point opposite.
-__device__ __forceinline__ float cone_min_cos(float a1x, float a1y, float a1z, float c1, float a2x, float a2y, float a2z,
-                                              float c2) {
+__device__ __forceinline__ float cone_min_cos(float a1x, float a1y, float a1z, float c1, float s1, float a2x, float a2y,
+                                              float a2z, float c2, float s2) {
     if (c1 <= -1.0f || c2 <= -1.0f) return -1.0f;
     float cb = rn_dot(a1x, a1y, a1z, a2x, a2y, a2z);
     cb = fminf(fmaxf(cb, -1.0f), 1.0f);
-    const float sb = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(cb, cb))));
-    const float s1 = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(c1, c1))));
-    const float s2 = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(c2, c2))));
+    const float sb = cone_sine(cb);
     const float cg = rn_sub(rn_mul(c1, c2), rn_mul(s1, s2));
     const float sg = rn_add(rn_mul(s1, c2), rn_mul(c1, s2));
     if (sg < 0.0f) return -1.0f;
@@ -75,7 +98,7 @@ struct NodeGeom {
 };
 
 __device__ __forceinline__ NodeGeom node_geom(const TileInfo& t, float4 b0, float4 b1, float4 nc, float4 wc,
-                                              const BoundParams& bp) {
+                                              const NodeExtra& ne, const BoundParams& bp) {
     NodeGeom g;
     const float bmin[3] = {b0.x, b0.y, b0.z}, bmax[3] = {b1.x, b1.y, b1.z};
     float d2 = 0.0f;
@@ -86,19 +109,16 @@ __device__ __forceinline__ NodeGeom node_geom(const TileInfo& t, float4 b0, floa
     }
     g.d2c = fmaxf(d2, bp.clamp2);
     // direction cone node -> tile
-    float v[3], en[3], et[3];
+    float v[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float cn = rn_mul(0.5f, rn_add(bmin[k], bmax[k]));
         const float ct = rn_mul(0.5f, rn_add(t.tmin[k], t.tmax[k]));
         v[k] = rn_sub(ct, cn);
-        en[k] = rn_sub(bmax[k], bmin[k]);
-        et[k] = rn_sub(t.tmax[k], t.tmin[k]);
     }
     const float dc = rn_sqrt(rn_dot(v[0], v[1], v[2], v[0], v[1], v[2]));
-    const float rn = rn_mul(0.5f, rn_sqrt(rn_dot(en[0], en[1], en[2], en[0], en[1], en[2])));
-    const float rt = rn_mul(0.5f, rn_sqrt(rn_dot(et[0], et[1], et[2], et[0], et[1], et[2])));
-    const float rs = rn_add(rn, rt);
+    const float rn = ne.rn;
+    const float rs = rn_add(rn, t.rt);
     g.dc = dc;
     g.rs = rs;
     g.rn = rn;
@@ -111,18 +131,19 @@ __device__ __forceinline__ NodeGeom node_geom(const TileInfo& t, float4 b0, floa
         ay = rn_mul(v[1], inv);
         az = rn_mul(v[2], inv);
     }
-    const float c2 = cone_max_cos(nc.x, nc.y, nc.z, nc.w, ax, ay, az, ca);
-    const float c1 = cone_max_cos(t.ncone.x, t.ncone.y, t.ncone.z, t.ncone.w, -ax, -ay, -az, ca);
+    const float sa2 = cone_sine(ca);
+    const float c2 = cone_max_cos(nc.x, nc.y, nc.z, nc.w, ne.snc, ax, ay, az, ca, sa2);
+    const float c1 = cone_max_cos(t.ncone.x, t.ncone.y, t.ncone.z, t.ncone.w, t.sn, -ax, -ay, -az, ca, sa2);
     g.cos2 = fminf(fmaxf(c2, 0.0f), 1.0f);
     g.cos1 = fminf(fmaxf(c1, 0.0f), 1.0f);
     g.ar_ok = 0.0f;
     if (bp.ar_kind == ARC_AR_CONE) {
-        const float cw = cone_max_cos(wc.x, wc.y, wc.z, wc.w, ax, ay, az, ca);
+        const float cw = cone_max_cos(wc.x, wc.y, wc.z, wc.w, ne.swc, ax, ay, az, ca, sa2);
         if (cw > bp.cos_thr && g.cos1 > bp.eps_cone) {
             // 1 when every (pixel, AVPL) pair of the two boxes passes the cone test, else the
             // uncertainty multiplier: the representative's test then stands for a mixed set
-            const float cwmin = cone_min_cos(wc.x, wc.y, wc.z, wc.w, ax, ay, az, ca);
-            const float c1min = cone_min_cos(t.ncone.x, t.ncone.y, t.ncone.z, t.ncone.w, -ax, -ay, -az, ca);
+            const float cwmin = cone_min_cos(wc.x, wc.y, wc.z, wc.w, ne.swc, ax, ay, az, ca, sa2);
+            const float c1min = cone_min_cos(t.ncone.x, t.ncone.y, t.ncone.z, t.ncone.w, t.sn, -ax, -ay, -az, ca, sa2);
             g.ar_ok = (cwmin > bp.cos_thr && c1min > bp.eps_cone) ? 1.0f : bp.ar_uncertain;
         }
     } else if (bp.ar_kind == ARC_AR_DISK) {

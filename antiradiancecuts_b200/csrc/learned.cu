@@ -59,40 +59,55 @@ __device__ __forceinline__ TileInfo load_tile_info(const float4* info, int tile,
     t.ncone = i2;
     t.valid = __float_as_int(i3.x);
     *mean = i3.y;
+    t.rt = i3.z;
+    t.sn = i3.w;
     return t;
 }
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
-// features are coarse network inputs: fast hardware log2 / division
+// features are coarse network inputs: fast hardware log2 / division / square root
 __device__ __forceinline__ float safe_log2(float v) { return __log2f(fmaxf(v, 1e-30f)); }
 
+__device__ __forceinline__ float fast_sqrt(float v) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+    return r;
+}
+
 // Radiance and antiradiance luminance of one packed record at a point p with unit normal n
-// (receiver albedo folded into kdl by the caller).
-__device__ __forceinline__ void record_at(float4 q0, float4 q1, float4 q2, float4 q3, float px, float py, float pz,
-                                          float nx, float ny, float nz, float clamp2, float cos_thr, float& rad,
-                                          float& ar) {
+// (receiver albedo folded into kdl by the caller): position q0.xyz, normal (q0.w, q1.x, q1.y),
+// direction (q1.z, q1.w, wz), luminances L and A of the record's radiance and antiradiance.
+__device__ __forceinline__ void record_at(float4 q0, float4 q1, float wz, float L, float A, float px, float py,
+                                          float pz, float nx, float ny, float nz, float clamp2, float cos_thr,
+                                          float& rad, float& ar) {
     const float dx = q0.x - px, dy = q0.y - py, dz = q0.z - pz;
     const float l2 = fmaxf(dx * dx + dy * dy + dz * dz, 1e-12f);
     const float r = rsqrtf(l2);
     const float c1 = (nx * dx + ny * dy + nz * dz) * r;
     const float c2 = -(q0.w * dx + q1.x * dy + q1.y * dz) * r;
     const float inv = __fdividef(1.0f, fmaxf(l2, clamp2));
-    rad = lum3(q2.y, q2.z, q2.w) * fmaxf(c1, 0.0f) * fmaxf(c2, 0.0f) * inv;
-    const float cw = -(q1.z * dx + q1.w * dy + q2.x * dz) * r;
-    ar = (cw > cos_thr && c1 > 0.001f) ? lum3(q3.x, q3.y, q3.z) * c1 * inv : 0.0f;
+    rad = L * fmaxf(c1, 0.0f) * fmaxf(c2, 0.0f) * inv;
+    const float cw = -(q1.z * dx + q1.w * dy + wz * dz) * r;
+    ar = (cw > cos_thr && c1 > 0.001f) ? A * c1 * inv : 0.0f;
+}
+
+__device__ __forceinline__ void record_at(const float4* q, float px, float py, float pz, float nx, float ny, float nz,
+                                          float clamp2, float cos_thr, float& rad, float& ar) {
+    const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+    record_at(q0, q1, q2.x, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), px, py, pz, nx, ny, nz, clamp2, cos_thr,
+              rad, ar);
 }
 
 // The 16 features of (tile, inner node).  Every input is known at selection time: the tile's
-// geometry and coarse estimate (mean), the node's bounds / cones / record / direction statistics,
-// the records of its two children (a one-level lookahead at the tile centre), its depth, and the
-// analytic bound M against tau.
+// geometry and coarse estimate (mean), the node's bounds / cones / record (q0, q1, the direction's
+// z, the luminances Ls and As) / direction statistics, the records of its two children (a
+// one-level lookahead at the tile centre), its depth, and the analytic bound M against tau.
 __device__ __forceinline__ void node_features(const TileInfo& t, float mean, const NodeGeom& g, float M, float4 nc,
-                                              float4 wc, float4 q0, float4 q1, float4 q2, float4 q3,
+                                              float4 wc, float4 q0, float4 q1, float wz, float Ls, float As,
                                               const float4* rec_l, const float4* rec_r, float4 ds, int depth,
                                               float clamp2, float cos_thr, float* f) {
     const float E = fmaxf(mean, 1e-30f);
-    const float Ls = lum3(q2.y, q2.z, q2.w), As = lum3(q3.x, q3.y, q3.z);
     const float inv_dc = __fdividef(1.0f, fmaxf(g.dc, 1e-6f));
     const float rt = g.rs - g.rn;
     const float cx = 0.5f * (t.tmin[0] + t.tmax[0]), cy = 0.5f * (t.tmin[1] + t.tmax[1]),
@@ -106,16 +121,16 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
         nz *= s;
     }
     float rad, ar, radl, arl, radr, arr;
-    record_at(q0, q1, q2, q3, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, rad, ar);
-    record_at(rec_l[0], rec_l[1], rec_l[2], rec_l[3], cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radl, arl);
-    record_at(rec_r[0], rec_r[1], rec_r[2], rec_r[3], cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radr, arr);
+    record_at(q0, q1, wz, Ls, As, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, rad, ar);
+    record_at(rec_l, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radl, arl);
+    record_at(rec_r, cx, cy, cz, nx, ny, nz, clamp2, cos_thr, radr, arr);
     const float s = __fdividef(t.kdl, E);
-    f[0] = clampf((M > 0.0f ? safe_log2(M / fmaxf(t.tau, 1e-30f)) : -32.0f) * 0.125f, -4.0f, 4.0f);
+    f[0] = clampf((M > 0.0f ? safe_log2(__fdividef(M, fmaxf(t.tau, 1e-30f))) : -32.0f) * 0.125f, -4.0f, 4.0f);
     f[1] = clampf(safe_log2(Ls * s) * 0.125f, -4.0f, 4.0f);
     f[2] = clampf(safe_log2(As * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
     f[3] = clampf(g.rn * inv_dc, 0.0f, 4.0f);
     f[4] = clampf(rt * inv_dc, 0.0f, 4.0f);
-    f[5] = clampf(sqrtf(g.d2c) * inv_dc, 0.0f, 4.0f);
+    f[5] = clampf(fast_sqrt(g.d2c) * inv_dc, 0.0f, 4.0f);
     f[6] = g.cos1;
     f[7] = g.cos2;
     f[8] = g.ar_ok == 1.0f ? 1.0f : 0.0f;
@@ -126,7 +141,7 @@ __device__ __forceinline__ void node_features(const TileInfo& t, float mean, con
     f[13] = clampf(safe_log2(fabsf(ar - arl - arr) * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
     f[14] = depth * (1.0f / 32.0f);
     // mean resultant length of the antiradiance directions, in [-1, 1]
-    const float sl = sqrtf(ds.x * ds.x + ds.y * ds.y + ds.z * ds.z);
+    const float sl = fast_sqrt(ds.x * ds.x + ds.y * ds.y + ds.z * ds.z);
     f[15] = ds.w > 0.0f ? clampf(2.0f * __fdividef(sl, ds.w) - 1.0f, -1.0f, 1.0f) : -1.0f;
 }
 
@@ -157,6 +172,7 @@ struct LevelArgs {
     const float4* records;
     const float4* dirstat;
     const float4* info;
+    const float4* extra;    // NodeExtra per inner node
     BoundParams bp;
     const int2* in;         // {tile, node | depth << 26}
     const int* in_count;
@@ -321,15 +337,15 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
                 const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
                 const float4* rec = a.records + 4 * (size_t)node;
-                const float4 q2 = rec[2], q3 = rec[3];
-                const NodeGeom g = node_geom(ti, b0, b1, nc, wc, a.bp);
-                const float M = node_bound(ti, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
+                const NodeExtra ne = load_node_extra(a.extra, k);
+                const NodeGeom g = node_geom(ti, b0, b1, nc, wc, ne, a.bp);
+                const float M = node_bound(ti, g, ne.Ls, ne.As, a.bp);
                 lc = child_index(__float_as_int(b0.w), a.n);
                 rc = child_index(__float_as_int(b1.w), a.n);
                 if (M > ti.tau) action = M > a.band * ti.tau ? kRefine : kScore;
                 if (action == kScore) {
                     float f[kFeat];
-                    node_features(ti, mean, g, M, nc, wc, rec[0], rec[1], q2, q3, a.records + 4 * (size_t)lc,
+                    node_features(ti, mean, g, M, nc, wc, rec[0], rec[1], rec[2].x, ne.Ls, ne.As, a.records + 4 * (size_t)lc,
                                   a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
                     // < kStageRows: fewer than kLevelThreads rows are left over from the last round
                     const int slot = atomicAdd(&s_staged, 1);
@@ -544,6 +560,7 @@ struct LabelArgs {
     const float4* records;
     const float4* dirstat;
     const float4* info;
+    const float4* extra;
     BoundParams bp;
     PairConsts pc;
     float disk_scale;
@@ -691,9 +708,9 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
         const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
         const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
         const float4* rec = a.records + 4 * (size_t)node;
-        const float4 q2 = rec[2], q3 = rec[3];
-        const NodeGeom g = node_geom(t, b0, b1, nc, wc, a.bp);
-        const float M = node_bound(t, g, lum3(q2.y, q2.z, q2.w), lum3(q3.x, q3.y, q3.z), a.bp);
+        const NodeExtra ne = load_node_extra(a.extra, k);
+        const NodeGeom g = node_geom(t, b0, b1, nc, wc, ne, a.bp);
+        const float M = node_bound(t, g, ne.Ls, ne.As, a.bp);
         if (!(M > t.tau)) continue;  // the analytic bound accepts it: no decision to learn
         const int c0 = child_index(__float_as_int(b0.w), a.n), c1 = child_index(__float_as_int(b1.w), a.n);
         const int d1 = min(depth + 1, 127) << 24;
@@ -725,7 +742,7 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
             const int r = atomicAdd(a.count, 1);
             if (r < a.capacity) {
                 float f[kFeat];
-                node_features(t, mean, g, M, nc, wc, rec[0], rec[1], rec[2], rec[3], a.records + 4 * (size_t)c0,
+                node_features(t, mean, g, M, nc, wc, rec[0], rec[1], rec[2].x, ne.Ls, ne.As, a.records + 4 * (size_t)c0,
                               a.records + 4 * (size_t)c1,
                               a.dirstat[node], depth,
                               a.bp.clamp2, a.bp.cos_thr, f);
@@ -764,8 +781,8 @@ BoundParams bound_params(const ArcGatherParams* gp, const ArcCutParams* cp) {
 }  // namespace
 
 arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, const ArcGatherParams* gp,
-                                     const ArcCutParams* cp, const float4* info, int tiles_x, int tiles_y,
-                                     const CutPool& pool) {
+                                     const ArcCutParams* cp, const float4* info, const float4* extra, int tiles_x,
+                                     int tiles_y, const CutPool& pool) {
     cudaStream_t st = ctx->stream;
     const int tiles = tiles_x * tiles_y;
     const int n = bvh->n;
@@ -802,6 +819,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.records = reinterpret_cast<const float4*>(bvh->view.records);
     la.dirstat = reinterpret_cast<const float4*>(bvh->view.dirstat);
     la.info = info;
+    la.extra = extra;
     la.bp = bound_params(gp, cp);
     la.capacity = cap;
     la.rows_scored = rows_scored;
@@ -907,7 +925,8 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     const int tiles_x = (W + kTile - 1) / kTile, tiles = tiles_x * ((H + kTile - 1) / kTile);
     const int n = bvh->n;
     float4* info = nullptr;
-    ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info));
+    float4* extra = nullptr;
+    ARC_TRY(launch_tile_setup(ctx, bvh, gb, gp, cp, &info, &extra));
     // batch of tiles whose FP64 prefixes fit in ~8 GB
     const size_t per_tile = (size_t)(n + 1) * 64 * sizeof(double);
     const int batch = (int)std::max<size_t>(1, std::min<size_t>((size_t)tiles, ((size_t)8 << 30) / per_tile));
@@ -933,6 +952,7 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     a.records = reinterpret_cast<const float4*>(bvh->view.records);
     a.dirstat = reinterpret_cast<const float4*>(bvh->view.dirstat);
     a.info = info;
+    a.extra = extra;
     a.bp = bound_params(gp, cp);
     a.pc.cos_thr = fmaxf(cosf(gp->cone_half_angle), 0.001f);
     a.pc.eps = 0.001f;
