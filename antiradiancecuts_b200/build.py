@@ -21,7 +21,7 @@ LIB = os.path.join(PKG, "libarc.so")
 
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", f"-I{CSRC}",
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp", f"-I{INCLUDE}", f"-I{CSRC}",
                      "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O2", "-fPIC", "-fopenmp", "-std=c++17", f"-I{INCLUDE}", f"-I{CSRC}"]
 

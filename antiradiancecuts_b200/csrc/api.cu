@@ -207,7 +207,10 @@ arc_status arc_context_destroy(arc_context* ctx) {
     for (auto e : ctx->timer.end) cudaEventDestroy(e);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_materials) cudaFree(ctx->d_materials);
-    if (ctx->h_staging) cudaFreeHost(ctx->h_staging);
+    for (int i = 0; i < 2; ++i) {
+        if (ctx->h_staging[i]) cudaFreeHost(ctx->h_staging[i]);
+        if (ctx->staged[i]) cudaEventDestroy(ctx->staged[i]);
+    }
     if (ctx->owns_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ARC_OK;
@@ -311,21 +314,25 @@ arc_status arc_materials_upload(arc_context* ctx, const ArcMaterial* materials, 
 arc_status arc_avpls_upload(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcAvplsGpuParam* out) {
     ARC_CHECK_ARG(ctx && out && (avpls || num == 0), "NULL argument");
     ARC_CHECK_ARG(num >= 0, "negative AVPL count");
-    // AoS -> SoA on the host into pinned staging, one copy, then device views (data_gpu.cu:5-52)
+    // AoS -> SoA on the host (all cores) into pinned staging, one copy, then device views
+    // (data_gpu.cu:5-52).  The staging buffers alternate: this one was last read by the copy two
+    // uploads ago, which is all the host waits for.
     const size_t n = (size_t)num;
     const size_t bytes = n * (5 * sizeof(ArcFloat3) + 2 * sizeof(int32_t));
-    if (ctx->h_staging_bytes < bytes) {
-        if (ctx->h_staging) {
-            ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
-            ARC_TRY_CUDA(cudaFreeHost(ctx->h_staging));
-            ctx->h_staging = nullptr;
+    const int turn = ctx->staging_turn;
+    ctx->staging_turn ^= 1;
+    if (!ctx->staged[turn]) ARC_TRY_CUDA(cudaEventCreateWithFlags(&ctx->staged[turn], cudaEventDisableTiming));
+    ARC_TRY_CUDA(cudaEventSynchronize(ctx->staged[turn]));
+    if (ctx->h_staging_bytes[turn] < bytes) {
+        if (ctx->h_staging[turn]) {
+            ARC_TRY_CUDA(cudaFreeHost(ctx->h_staging[turn]));
+            ctx->h_staging[turn] = nullptr;
+            ctx->h_staging_bytes[turn] = 0;
         }
-        ARC_TRY_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ctx->h_staging), bytes > 0 ? bytes : 64));
-        ctx->h_staging_bytes = bytes;
-    } else {
-        ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));  // previous upload finished with the staging
+        ARC_TRY_CUDA(cudaMallocHost(&ctx->h_staging[turn], bytes > 0 ? bytes : 64));
+        ctx->h_staging_bytes[turn] = bytes;
     }
-    char* h = reinterpret_cast<char*>(ctx->h_staging);
+    char* h = reinterpret_cast<char*>(ctx->h_staging[turn]);
     ArcFloat3* hp = reinterpret_cast<ArcFloat3*>(h);
     ArcFloat3* hn = hp + n;
     ArcFloat3* hw = hn + n;
@@ -333,6 +340,7 @@ arc_status arc_avpls_upload(arc_context* ctx, const ArcAvplHost* avpls, int32_t 
     ArcFloat3* hA = hL + n;
     int32_t* hm = reinterpret_cast<int32_t*>(hA + n);
     int32_t* hb = hm + n;
+#pragma omp parallel for schedule(static) if (n >= 65536)
     for (size_t i = 0; i < n; ++i) {
         hp[i] = avpls[i].position;
         hn[i] = avpls[i].normal;
@@ -345,6 +353,7 @@ arc_status arc_avpls_upload(arc_context* ctx, const ArcAvplHost* avpls, int32_t 
     void* d = nullptr;
     ARC_TRY(ctx->arena.get("avpls_soa", bytes > 0 ? bytes : 64, &d));
     if (bytes) ARC_TRY_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ARC_TRY_CUDA(cudaEventRecord(ctx->staged[turn], ctx->stream));
     char* dc = reinterpret_cast<char*>(d);
     out->position = reinterpret_cast<ArcFloat3*>(dc);
     out->normal = out->position + n;

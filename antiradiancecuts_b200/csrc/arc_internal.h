@@ -100,9 +100,13 @@ struct arc_context {
     int32_t num_materials = 0;
     bool any_specular = false;
     std::vector<ArcMaterial> host_materials;
-    // AVPL upload buffers (AvplsGpu)
-    ArcAvplHost* h_staging = nullptr;  // pinned
-    size_t h_staging_bytes = 0;
+    // AVPL upload buffers (AvplsGpu): two pinned staging buffers used in turn, so that the host
+    // conversion of one upload overlaps the device work queued before it; staged[i] is recorded
+    // after the copy out of buffer i
+    void* h_staging[2] = {nullptr, nullptr};
+    size_t h_staging_bytes[2] = {0, 0};
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    int staging_turn = 0;
     arc::CutState last_cut;
     int sm_count = 148;
     arc_lbvh* run_bvh = nullptr;  // tree rebuilt by arc_run every frame

@@ -310,7 +310,7 @@ struct KarrasArgs {
     float4* records;   // [2N-1][4]
     float4* cones;     // [2N-1][2] {normal axis, cos}, {direction axis, cos}
     float4* dirstat;   // [2N-1] {S.xyz, a}: a = sum of antiradiance luminances, S = sum of a_i w_i / |w_i|
-    float* bbox;       // [2N-1][6] scratch: leaf boxes then inner boxes
+    float4* bbox;      // [2N-1][2] scratch: {min, 0}, {max, 0} of leaf boxes then inner boxes
     ArcAvplBvhNodeDataParam nd;
     ArcFloat3* sorted_pos;
     ArcFloat3* sorted_nrm;
@@ -383,10 +383,8 @@ __global__ void __launch_bounds__(256) lbvh_karras(KarrasArgs k) {
         c[1] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         k.dirstat[i] = make_float4(0.0f, 0.0f, 0.0f, a_lum);
     }
-    float* b = k.bbox + 6 * (size_t)i;
-    b[0] = b[3] = p.x;
-    b[1] = b[4] = p.y;
-    b[2] = b[5] = p.z;
+    k.bbox[2 * (size_t)i] = make_float4(p.x, p.y, p.z, 0.0f);
+    k.bbox[2 * (size_t)i + 1] = make_float4(p.x, p.y, p.z, 0.0f);
     // reference node-data layout (AvplBvhNodeData, bvh.cu:673-724, sorted as bvh.cu:793-808)
     k.nd.size[i] = 1;
     k.nd.materialIndex[i] = mat;
@@ -436,19 +434,105 @@ struct BottomUpArgs {
     const int32_t* left;
     const int32_t* right;
     const int32_t* parents;
+    const int32_t* range;  // [N-1][2]: first and last leaf of each inner node
     int32_t* visit;
     float4* records;
     float4* cones;
     float4* dirstat;
-    float* bbox;
+    float4* bbox;
     float4* bounds;  // [N-1][4]
     ArcAvplBvhNodeDataParam nd;
 };
 
-__device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
+// Loads of a child's data in the merge.  A child merged by a thread of the same block (LOCAL) was
+// published with a block-scope release, so the load goes through the SM's L1; a child merged in
+// another block was published with a device-scope release and is read from L2.
+template <bool LOCAL, typename T>
+__device__ __forceinline__ T ld_child(const T* p) {
+    if (LOCAL) return *p;
+    return __ldcg(p);
+}
 
-__global__ void __launch_bounds__(256) lbvh_bottom_up(BottomUpArgs b) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Merges the two children of inner node k (the second thread to arrive does it); same operations
+// and order as the CPU build's bottom-up pass.
+template <bool LOCAL>
+__device__ __forceinline__ void merge_node(const BottomUpArgs& b, int k, int lc, int rc) {
+    const int n = b.n;
+    const int t = n + k;
+    const int l = lc >= 0 ? lc : n - (lc + 1);
+    const int r = rc >= 0 ? rc : n - (rc + 1);
+    // bounding box
+    const float4 lmin = ld_child<LOCAL>(b.bbox + 2 * (size_t)l), lmax = ld_child<LOCAL>(b.bbox + 2 * (size_t)l + 1);
+    const float4 rmin = ld_child<LOCAL>(b.bbox + 2 * (size_t)r), rmax = ld_child<LOCAL>(b.bbox + 2 * (size_t)r + 1);
+    const float bt[6] = {fminf(lmin.x, rmin.x), fminf(lmin.y, rmin.y), fminf(lmin.z, rmin.z),
+                         fmaxf(lmax.x, rmax.x), fmaxf(lmax.y, rmax.y), fmaxf(lmax.z, rmax.z)};
+    b.bbox[2 * (size_t)t] = make_float4(bt[0], bt[1], bt[2], 0.0f);
+    b.bbox[2 * (size_t)t + 1] = make_float4(bt[3], bt[4], bt[5], 0.0f);
+    // representative (cluster, bvh.cu:726-744)
+    const float* Lf = reinterpret_cast<const float*>(b.nd.incRadiance);
+    const float Ll[3] = {ld_child<LOCAL>(Lf + 3 * l), ld_child<LOCAL>(Lf + 3 * l + 1), ld_child<LOCAL>(Lf + 3 * l + 2)};
+    const float Lr[3] = {ld_child<LOCAL>(Lf + 3 * r), ld_child<LOCAL>(Lf + 3 * r + 1), ld_child<LOCAL>(Lf + 3 * r + 2)};
+    const float i1 = rn_sqrt(rn_dot(Ll[0], Ll[1], Ll[2], Ll[0], Ll[1], Ll[2]));
+    const float i2 = rn_sqrt(rn_dot(Lr[0], Lr[1], Lr[2], Lr[0], Lr[1], Lr[2]));
+    const float rnd = arc_node_random(b.seed, (uint32_t)t);
+    const int repr = rnd > rn_div(i1, rn_add(i1, i2)) ? r : l;
+    const int sl = ld_child<LOCAL>(b.nd.size + l), sr = ld_child<LOCAL>(b.nd.size + r);
+    b.nd.randomNumbers[t] = rnd;
+    b.nd.size[t] = sl + sr;
+    b.nd.materialIndex[t] = ld_child<LOCAL>(b.nd.materialIndex + repr);
+    float* Lt = reinterpret_cast<float*>(b.nd.incRadiance);
+    float* P = reinterpret_cast<float*>(b.nd.position);
+    float* N = reinterpret_cast<float*>(b.nd.normal);
+    float* W = reinterpret_cast<float*>(b.nd.incDirection);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        Lt[3 * t + q] = rn_add(Ll[q], Lr[q]);
+        P[3 * t + q] = ld_child<LOCAL>(P + 3 * repr + q);
+        N[3 * t + q] = ld_child<LOCAL>(N + 3 * repr + q);
+        W[3 * t + q] = ld_child<LOCAL>(W + 3 * repr + q);
+    }
+    // direction statistics, and the antiradiance representative: drawn in proportion to
+    // antiradiance luminance with the same random number; its direction is the record's w
+    const float4 dl = ld_child<LOCAL>(b.dirstat + l), dr = ld_child<LOCAL>(b.dirstat + r);
+    const float4 dt = make_float4(rn_add(dl.x, dr.x), rn_add(dl.y, dr.y), rn_add(dl.z, dr.z), rn_add(dl.w, dr.w));
+    b.dirstat[t] = dt;
+    const int arep = dt.w > 0.0f ? (rnd > rn_div(dl.w, dt.w) ? r : l) : repr;
+    // packed record: representative p/n, antiradiance representative's w, summed L' and A, count
+    const float4* R = b.records;
+    const float4 p0 = ld_child<LOCAL>(R + 4 * (size_t)repr), p1 = ld_child<LOCAL>(R + 4 * (size_t)repr + 1);
+    const float4 w1 = ld_child<LOCAL>(R + 4 * (size_t)arep + 1), w2 = ld_child<LOCAL>(R + 4 * (size_t)arep + 2);
+    const float4 l2 = ld_child<LOCAL>(R + 4 * (size_t)l + 2), l3 = ld_child<LOCAL>(R + 4 * (size_t)l + 3);
+    const float4 r2 = ld_child<LOCAL>(R + 4 * (size_t)r + 2), r3 = ld_child<LOCAL>(R + 4 * (size_t)r + 3);
+    float4* rec = b.records + 4 * (size_t)t;
+    rec[0] = p0;
+    rec[1] = make_float4(p1.x, p1.y, w1.z, w1.w);
+    rec[2] = make_float4(w2.x, rn_add(l2.y, r2.y), rn_add(l2.z, r2.z), rn_add(l2.w, r2.w));
+    rec[3] = make_float4(rn_add(l3.x, r3.x), rn_add(l3.y, r3.y), rn_add(l3.z, r3.z), (float)(sl + sr));
+    // cones
+    const float4 cnl = ld_child<LOCAL>(b.cones + 2 * (size_t)l), cnr = ld_child<LOCAL>(b.cones + 2 * (size_t)r);
+    const float4 cwl = ld_child<LOCAL>(b.cones + 2 * (size_t)l + 1), cwr = ld_child<LOCAL>(b.cones + 2 * (size_t)r + 1);
+    const float4 cn = cone_union(cnl, cnr), cw = cone_union(cwl, cwr);
+    b.cones[2 * (size_t)t] = cn;
+    b.cones[2 * (size_t)t + 1] = cw;
+    float4* bd = b.bounds + 4 * (size_t)k;
+    bd[0] = make_float4(bt[0], bt[1], bt[2], __int_as_float(lc));
+    bd[1] = make_float4(bt[3], bt[4], bt[5], __int_as_float(rc));
+    bd[2] = cn;
+    bd[3] = cw;
+}
+
+// One thread per leaf climbs towards the root; at each inner node the first thread to arrive
+// stops and the second merges the two children.  Nodes whose leaf range lies inside the block's
+// kBottomUpThreads leaves are settled in shared memory with block-scope ordering (both arrivals
+// come from this block); the others through the global visit counters with device-scope fences.
+constexpr int kBottomUpThreads = 256;
+
+__global__ void __launch_bounds__(kBottomUpThreads) lbvh_bottom_up(BottomUpArgs b) {
+    __shared__ int arrivals[kBottomUpThreads];
+    arrivals[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kBottomUpThreads;
+    const int i = base + threadIdx.x;
     const int n = b.n;
     if (i >= n) return;
     int parent = b.parents[i];
@@ -458,82 +542,22 @@ __global__ void __launch_bounds__(256) lbvh_bottom_up(BottomUpArgs b) {
             set_error(b.err, ARC_DEVERR_BAD_NODE);
             return;
         }
-        __threadfence();  // release this thread's writes (the child it just finished)
-        if (atomicAdd(&b.visit[parent], 1) == 0) return;
-        __threadfence();  // acquire the sibling's writes
         const int k = parent;
-        const int t = n + k;
+        const int2 rg = *reinterpret_cast<const int2*>(b.range + 2 * (size_t)k);
         const int lc = b.left[k], rc = b.right[k];
-        const int l = lc >= 0 ? lc : n - (lc + 1);
-        const int r = rc >= 0 ? rc : n - (rc + 1);
-        // bounding box
-        float bl[6], br[6], bt[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            bl[q] = ldcg(b.bbox + 6 * (size_t)l + q);
-            br[q] = ldcg(b.bbox + 6 * (size_t)r + q);
+        // node k is one end of its own range, so a local node's slot k - base is in [0, 256)
+        const bool local = rg.x >= base && rg.y < base + kBottomUpThreads && k >= base && k < base + kBottomUpThreads;
+        if (local) {
+            __threadfence_block();  // release this thread's writes (the child it just finished)
+            if (atomicAdd(&arrivals[k - base], 1) == 0) return;
+            __threadfence_block();  // acquire the sibling's writes
+            merge_node<true>(b, k, lc, rc);
+        } else {
+            __threadfence();
+            if (atomicAdd(&b.visit[k], 1) == 0) return;
+            __threadfence();
+            merge_node<false>(b, k, lc, rc);
         }
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            bt[q] = fminf(bl[q], br[q]);
-            bt[3 + q] = fmaxf(bl[3 + q], br[3 + q]);
-        }
-#pragma unroll
-        for (int q = 0; q < 6; ++q) b.bbox[6 * (size_t)t + q] = bt[q];
-        // representative (cluster, bvh.cu:726-744)
-        const float* Lf = reinterpret_cast<const float*>(b.nd.incRadiance);
-        const float Ll[3] = {ldcg(Lf + 3 * l), ldcg(Lf + 3 * l + 1), ldcg(Lf + 3 * l + 2)};
-        const float Lr[3] = {ldcg(Lf + 3 * r), ldcg(Lf + 3 * r + 1), ldcg(Lf + 3 * r + 2)};
-        const float i1 = rn_sqrt(rn_dot(Ll[0], Ll[1], Ll[2], Ll[0], Ll[1], Ll[2]));
-        const float i2 = rn_sqrt(rn_dot(Lr[0], Lr[1], Lr[2], Lr[0], Lr[1], Lr[2]));
-        const float rnd = arc_node_random(b.seed, (uint32_t)t);
-        const int repr = rnd > rn_div(i1, rn_add(i1, i2)) ? r : l;
-        b.nd.randomNumbers[t] = rnd;
-        b.nd.size[t] = __ldcg(b.nd.size + l) + __ldcg(b.nd.size + r);
-        b.nd.materialIndex[t] = __ldcg(b.nd.materialIndex + repr);
-        float* Lt = reinterpret_cast<float*>(b.nd.incRadiance);
-        float* P = reinterpret_cast<float*>(b.nd.position);
-        float* N = reinterpret_cast<float*>(b.nd.normal);
-        float* W = reinterpret_cast<float*>(b.nd.incDirection);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            Lt[3 * t + q] = rn_add(Ll[q], Lr[q]);
-            P[3 * t + q] = ldcg(P + 3 * repr + q);
-            N[3 * t + q] = ldcg(N + 3 * repr + q);
-            W[3 * t + q] = ldcg(W + 3 * repr + q);
-        }
-        // direction statistics, and the antiradiance representative: drawn in proportion to
-        // antiradiance luminance with the same random number; its direction is the record's w
-        const float4 dl = __ldcg(b.dirstat + l), dr = __ldcg(b.dirstat + r);
-        const float4 dt = make_float4(rn_add(dl.x, dr.x), rn_add(dl.y, dr.y), rn_add(dl.z, dr.z), rn_add(dl.w, dr.w));
-        b.dirstat[t] = dt;
-        const int arep = dt.w > 0.0f ? (rnd > rn_div(dl.w, dt.w) ? r : l) : repr;
-        // packed record: representative p/n, antiradiance representative's w, summed L' and A, count
-        const float* R = reinterpret_cast<const float*>(b.records);
-        float rt[16];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) rt[q] = ldcg(R + 16 * (size_t)repr + q);
-#pragma unroll
-        for (int q = 6; q < 9; ++q) rt[q] = ldcg(R + 16 * (size_t)arep + q);
-#pragma unroll
-        for (int q = 9; q < 15; ++q) rt[q] = rn_add(ldcg(R + 16 * (size_t)l + q), ldcg(R + 16 * (size_t)r + q));
-        rt[15] = (float)(__ldcg(b.nd.size + l) + __ldcg(b.nd.size + r));
-        float4* rec = b.records + 4 * (size_t)t;
-        rec[0] = make_float4(rt[0], rt[1], rt[2], rt[3]);
-        rec[1] = make_float4(rt[4], rt[5], rt[6], rt[7]);
-        rec[2] = make_float4(rt[8], rt[9], rt[10], rt[11]);
-        rec[3] = make_float4(rt[12], rt[13], rt[14], rt[15]);
-        // cones
-        const float4 cnl = __ldcg(b.cones + 2 * (size_t)l), cnr = __ldcg(b.cones + 2 * (size_t)r);
-        const float4 cwl = __ldcg(b.cones + 2 * (size_t)l + 1), cwr = __ldcg(b.cones + 2 * (size_t)r + 1);
-        const float4 cn = cone_union(cnl, cnr), cw = cone_union(cwl, cwr);
-        b.cones[2 * (size_t)t] = cn;
-        b.cones[2 * (size_t)t + 1] = cw;
-        float4* bd = b.bounds + 4 * (size_t)k;
-        bd[0] = make_float4(bt[0], bt[1], bt[2], __int_as_float(lc));
-        bd[1] = make_float4(bt[3], bt[4], bt[5], __int_as_float(rc));
-        bd[2] = cn;
-        bd[3] = cw;
         parent = b.parents[n + k];
     }
 }
@@ -575,7 +599,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     uint32_t *keys0, *keys1, *hist, *status, *bb;
     int32_t *vals0, *vals1, *left, *right, *parents, *range, *visit;
     float4 *records, *cones, *bounds, *dirstat;
-    float* bbox;
+    float4* bbox;
     ARC_TRY(get(bvh, "keys0", n, &keys0));
     ARC_TRY(get(bvh, "keys1", n, &keys1));
     ARC_TRY(get(bvh, "vals0", n, &vals0));
@@ -592,7 +616,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     ARC_TRY(get(bvh, "cones", (size_t)2 * total, &cones));
     ARC_TRY(get(bvh, "dirstat", total, &dirstat));
     ARC_TRY(get(bvh, "bounds", (size_t)4 * (n - 1), &bounds));
-    ARC_TRY(get(bvh, "bbox", (size_t)6 * total, &bbox));
+    ARC_TRY(get(bvh, "bbox", (size_t)2 * total, &bbox));
     ArcAvplBvhNodeDataParam nd;
     ARC_TRY(get(bvh, "nd_size", total, &nd.size));
     ARC_TRY(get(bvh, "nd_mat", total, &nd.materialIndex));
@@ -689,6 +713,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     bu.left = left;
     bu.right = right;
     bu.parents = parents;
+    bu.range = range;
     bu.visit = visit;
     bu.records = records;
     bu.cones = cones;
@@ -698,7 +723,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     bu.nd = nd;
     bu.err = ctx->d_error;
     stage_begin(ctx, "lbvh_bottom_up");
-    lbvh_bottom_up<<<(n + 255) / 256, 256, 0, st>>>(bu);
+    lbvh_bottom_up<<<(n + kBottomUpThreads - 1) / kBottomUpThreads, kBottomUpThreads, 0, st>>>(bu);
     stage_end(ctx, 1);
     ARC_TRY_CUDA(cudaGetLastError());
 
