@@ -498,16 +498,21 @@ __device__ __forceinline__ void merge_node(const BottomUpArgs& b, int k, int lc,
     b.dirstat[t] = dt;
     const int arep = dt.w > 0.0f ? (rnd > rn_div(dl.w, dt.w) ? r : l) : repr;
     // packed record: representative p/n, antiradiance representative's w, summed L' and A, count
-    const float4* R = b.records;
-    const float4 p0 = ld_child<LOCAL>(R + 4 * (size_t)repr), p1 = ld_child<LOCAL>(R + 4 * (size_t)repr + 1);
-    const float4 w1 = ld_child<LOCAL>(R + 4 * (size_t)arep + 1), w2 = ld_child<LOCAL>(R + 4 * (size_t)arep + 2);
-    const float4 l2 = ld_child<LOCAL>(R + 4 * (size_t)l + 2), l3 = ld_child<LOCAL>(R + 4 * (size_t)l + 3);
-    const float4 r2 = ld_child<LOCAL>(R + 4 * (size_t)r + 2), r3 = ld_child<LOCAL>(R + 4 * (size_t)r + 3);
+    const float* R = reinterpret_cast<const float*>(b.records);
+    float rt[16];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) rt[q] = ld_child<LOCAL>(R + 16 * (size_t)repr + q);
+#pragma unroll
+    for (int q = 6; q < 9; ++q) rt[q] = ld_child<LOCAL>(R + 16 * (size_t)arep + q);
+#pragma unroll
+    for (int q = 9; q < 15; ++q)
+        rt[q] = rn_add(ld_child<LOCAL>(R + 16 * (size_t)l + q), ld_child<LOCAL>(R + 16 * (size_t)r + q));
+    rt[15] = (float)(sl + sr);
     float4* rec = b.records + 4 * (size_t)t;
-    rec[0] = p0;
-    rec[1] = make_float4(p1.x, p1.y, w1.z, w1.w);
-    rec[2] = make_float4(w2.x, rn_add(l2.y, r2.y), rn_add(l2.z, r2.z), rn_add(l2.w, r2.w));
-    rec[3] = make_float4(rn_add(l3.x, r3.x), rn_add(l3.y, r3.y), rn_add(l3.z, r3.z), (float)(sl + sr));
+    rec[0] = make_float4(rt[0], rt[1], rt[2], rt[3]);
+    rec[1] = make_float4(rt[4], rt[5], rt[6], rt[7]);
+    rec[2] = make_float4(rt[8], rt[9], rt[10], rt[11]);
+    rec[3] = make_float4(rt[12], rt[13], rt[14], rt[15]);
     // cones
     const float4 cnl = ld_child<LOCAL>(b.cones + 2 * (size_t)l), cnr = ld_child<LOCAL>(b.cones + 2 * (size_t)r);
     const float4 cwl = ld_child<LOCAL>(b.cones + 2 * (size_t)l + 1), cwr = ld_child<LOCAL>(b.cones + 2 * (size_t)r + 1);
