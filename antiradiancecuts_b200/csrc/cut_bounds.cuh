@@ -122,16 +122,18 @@ __device__ __forceinline__ NodeGeom node_geom(const TileInfo& t, float4 b0, floa
     g.dc = dc;
     g.rs = rs;
     g.rn = rn;
-    float ca = -1.0f, ax = 0.0f, ay = 0.0f, az = 0.0f;
+    // direction cone node -> tile: axis v / dc, sine rs / dc, cosine from the sine (ca = -1: the
+    // boxes are too close for a cone)
+    float ca = -1.0f, sa = 0.0f, ax = 0.0f, ay = 0.0f, az = 0.0f;
     if (dc > rs) {
-        const float sa = rn_div(rs, dc);
-        ca = rn_sqrt(fmaxf(0.0f, rn_sub(1.0f, rn_mul(sa, sa))));
         const float inv = rn_div(1.0f, dc);
+        sa = rn_mul(rs, inv);
+        ca = cone_sine(sa);
         ax = rn_mul(v[0], inv);
         ay = rn_mul(v[1], inv);
         az = rn_mul(v[2], inv);
     }
-    const float sa2 = cone_sine(ca);
+    const float sa2 = sa;
     const float c2 = cone_max_cos(nc.x, nc.y, nc.z, nc.w, ne.snc, ax, ay, az, ca, sa2);
     const float c1 = cone_max_cos(t.ncone.x, t.ncone.y, t.ncone.z, t.ncone.w, t.sn, -ax, -ay, -az, ca, sa2);
     g.cos2 = fminf(fmaxf(c2, 0.0f), 1.0f);
@@ -156,10 +158,11 @@ __device__ __forceinline__ NodeGeom node_geom(const TileInfo& t, float4 b0, floa
 __device__ __forceinline__ float node_bound(const TileInfo& t, const NodeGeom& g, float Ls, float As,
                                             const BoundParams& bp) {
     if (!(g.d2c > 0.0f)) return INFINITY;
-    const float grad = rn_div(rn_mul(g.cos1, g.cos2), g.d2c);
+    const float id2 = rn_div(1.0f, g.d2c);
+    const float grad = rn_mul(rn_mul(g.cos1, g.cos2), id2);
     float m = rn_mul(Ls, grad);
     if (bp.ar_kind == ARC_AR_CONE) {
-        m = rn_add(m, rn_mul(As, rn_mul(g.ar_ok, rn_div(g.cos1, g.d2c))));
+        m = rn_add(m, rn_mul(As, rn_mul(g.ar_ok, rn_mul(g.cos1, id2))));
     } else if (bp.ar_kind == ARC_AR_DISK) {
         m = rn_add(m, rn_mul(As, bp.disk_scale));
     }

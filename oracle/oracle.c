@@ -780,13 +780,13 @@ OR_EXPORT void oracle_cut_solid_angle(const float* gb_pos, const float* gb_nrm, 
 
 static float lum3f(float r, float g, float b) { return (0.2126f * r + 0.7152f * g) + 0.0722f * b; }
 
-static float cone_max_cos(const float* a1, float c1, const float* a2, float c2) {
+/* (a2, c2, s2): the second cone's axis, cosine and sine of its half-angle */
+static float cone_max_cos(const float* a1, float c1, const float* a2, float c2, float s2) {
     if (c1 <= -1.0f || c2 <= -1.0f) return 1.0f;
     float cb = dot3(a1, a2);
     cb = fminf(fmaxf(cb, -1.0f), 1.0f);
     const float sb = sqrtf(fmaxf(0.0f, 1.0f - cb * cb));
     const float s1 = sqrtf(fmaxf(0.0f, 1.0f - c1 * c1));
-    const float s2 = sqrtf(fmaxf(0.0f, 1.0f - c2 * c2));
     const float cg = c1 * c2 - s1 * s2;
     const float sg = s1 * c2 + c1 * s2;
     if (sg < 0.0f) return 1.0f;
@@ -898,13 +898,12 @@ typedef struct {
 } bound_params;
 
 /* min over members of two cones of cos(angle between them); -1 when they can point opposite. */
-static float cone_min_cos(const float* a1, float c1, const float* a2, float c2) {
+static float cone_min_cos(const float* a1, float c1, const float* a2, float c2, float s2) {
     if (c1 <= -1.0f || c2 <= -1.0f) return -1.0f;
     float cb = dot3(a1, a2);
     cb = fminf(fmaxf(cb, -1.0f), 1.0f);
     const float sb = sqrtf(fmaxf(0.0f, 1.0f - cb * cb));
     const float s1 = sqrtf(fmaxf(0.0f, 1.0f - c1 * c1));
-    const float s2 = sqrtf(fmaxf(0.0f, 1.0f - c2 * c2));
     const float cg = c1 * c2 - s1 * s2;
     const float sg = s1 * c2 + c1 * s2;
     if (sg < 0.0f) return -1.0f;
@@ -934,25 +933,25 @@ static float node_bound(const tile_info* t, const float* b, const float* rec, co
     const float rn = 0.5f * sqrtf(dot3(en, en));
     const float rt = 0.5f * sqrtf(dot3(et, et));
     const float rs = rn + rt;
-    float ca = -1.0f, ax[3] = {0, 0, 0}, nax[3];
+    float ca = -1.0f, sa = 0.0f, ax[3] = {0, 0, 0}, nax[3];
     if (dc > rs) {
-        const float sa = rs / dc;
-        ca = sqrtf(fmaxf(0.0f, 1.0f - sa * sa));
         const float inv = 1.0f / dc;
+        sa = rs * inv;
+        ca = sqrtf(fmaxf(0.0f, 1.0f - sa * sa));
         ax[0] = v[0] * inv; ax[1] = v[1] * inv; ax[2] = v[2] * inv;
     }
     nax[0] = -ax[0]; nax[1] = -ax[1]; nax[2] = -ax[2];
-    const float c2 = cone_max_cos(b + 8, b[11], ax, ca);
-    const float c1 = cone_max_cos(t->ncone, t->ncone[3], nax, ca);
+    const float c2 = cone_max_cos(b + 8, b[11], ax, ca, sa);
+    const float c1 = cone_max_cos(t->ncone, t->ncone[3], nax, ca, sa);
     const float cos2 = fminf(fmaxf(c2, 0.0f), 1.0f);
     const float cos1 = fminf(fmaxf(c1, 0.0f), 1.0f);
     float ar_ok = 0.0f;
     if (bp->ar_kind == 2) {
-        const float cw = cone_max_cos(b + 12, b[15], ax, ca);
+        const float cw = cone_max_cos(b + 12, b[15], ax, ca, sa);
         if (cw > bp->cos_thr && cos1 > bp->eps_cone) {
             /* every pair passes the cone test -> 1; some may fail -> the uncertainty factor */
-            const float cwmin = cone_min_cos(b + 12, b[15], ax, ca);
-            const float c1min = cone_min_cos(t->ncone, t->ncone[3], nax, ca);
+            const float cwmin = cone_min_cos(b + 12, b[15], ax, ca, sa);
+            const float c1min = cone_min_cos(t->ncone, t->ncone[3], nax, ca, sa);
             ar_ok = (cwmin > bp->cos_thr && c1min > bp->eps_cone) ? 1.0f : bp->ar_uncertain;
         }
     } else if (bp->ar_kind == 1) {
@@ -964,9 +963,10 @@ static float node_bound(const tile_info* t, const float* b, const float* rec, co
     if (!(d2c > 0.0f)) return INFINITY;
     const float Ls = lum3f(rec[9], rec[10], rec[11]);
     const float As = lum3f(rec[12], rec[13], rec[14]);
-    const float grad = (cos1 * cos2) / d2c;
+    const float id2 = 1.0f / d2c;
+    const float grad = (cos1 * cos2) * id2;
     float m = Ls * grad;
-    if (bp->ar_kind == 2) m = m + As * (ar_ok * (cos1 / d2c));
+    if (bp->ar_kind == 2) m = m + As * (ar_ok * (cos1 * id2));
     else if (bp->ar_kind == 1) m = m + As * bp->disk_scale;
     return t->kdl * m;
 }
