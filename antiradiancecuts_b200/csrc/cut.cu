@@ -653,6 +653,8 @@ __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
     const uint64_t PX = f2(-gp.x, -gp.x), PY = f2(-gp.y, -gp.y), PZ = f2(-gp.z, -gp.z);
     const uint64_t NX = f2(nx, nx), NY = f2(ny, ny), NZ = f2(nz, nz);
     const float cos_thr = a.pc.cos_thr, eps = a.pc.eps, inv_clamp2 = a.pc.inv_clamp2;
+    // distance floor folded into the FMA chain: l2 + 1e-30 equals max(l2, 1e-30) for l2 above ~1e-23
+    const uint64_t kTiny2 = f2(1e-30f, 1e-30f);
     float ss[6] = {0, 0, 0, 0, 0, 0}, sc[6] = {0, 0, 0, 0, 0, 0};
     const int count = a.pool.counts[tile];
     for (int base = 0; base < count; base += kChunk) {
@@ -678,10 +680,10 @@ __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
             const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(srec + pr * 32);
             const ulonglong2 f01 = s2[0], f23 = s2[1], f45 = s2[2], f67 = s2[3], f89 = s2[4], f1011 = s2[5];
             const uint64_t dx = f2_add(f01.x, PX), dy = f2_add(f01.y, PY), dz = f2_add(f23.x, PZ);
-            const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+            const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, kTiny2)));  // >= 1e-30
             float l2a, l2b;
             f2_split(l2, l2a, l2b);
-            const uint64_t r = f2(rsqrtf(fmaxf(l2a, 1e-30f)), rsqrtf(fmaxf(l2b, 1e-30f)));
+            const uint64_t r = f2(rsqrtf(l2a), rsqrtf(l2b));
             const uint64_t c1 = f2_mul(f2_fma(NZ, dz, f2_fma(NY, dy, f2_mul(NX, dx))), r);
             const uint64_t c2n = f2_mul(f2_fma(f45.y, dz, f2_fma(f45.x, dy, f2_mul(f23.y, dx))), r);  // -c2
             float c1a, c1b, c2a, c2b, rra, rrb;

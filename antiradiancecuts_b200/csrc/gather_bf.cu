@@ -432,6 +432,8 @@ __global__ void __launch_bounds__(kThreads) gather_bf_packed_kernel(BfArgs k) {
         for (int c = 0; c < 6; ++c) sc[j][c] = ss[j][c] = 0.0f;
     }
     const float cos_thr = k.pc.cos_thr, eps = k.pc.eps, inv_clamp2 = k.pc.inv_clamp2;
+    // distance floor folded into the FMA chain: l2 + 1e-30 equals max(l2, 1e-30) for l2 above ~1e-23
+    const uint64_t kTiny2 = f2(1e-30f, 1e-30f);
 
     bool ok = true;
     for (int c = 0; c < nchunks; ++c) {
@@ -453,10 +455,10 @@ __global__ void __launch_bounds__(kThreads) gather_bf_packed_kernel(BfArgs k) {
 #pragma unroll
                 for (int j = 0; j < PX; ++j) {
                     const uint64_t dx = f2_add(f01.x, PXc[j]), dy = f2_add(f01.y, PYc[j]), dz = f2_add(f23.x, PZc[j]);
-                    const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+                    const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, kTiny2)));  // >= 1e-30
                     float l2a, l2b;
                     f2_split(l2, l2a, l2b);
-                    const uint64_t r = f2(rsqrtf(fmaxf(l2a, 1e-30f)), rsqrtf(fmaxf(l2b, 1e-30f)));
+                    const uint64_t r = f2(rsqrtf(l2a), rsqrtf(l2b));
                     const uint64_t c1 = f2_mul(f2_fma(NZc[j], dz, f2_fma(NYc[j], dy, f2_mul(NXc[j], dx))), r);
                     const uint64_t c2n = f2_mul(f2_fma(f45.y, dz, f2_fma(f45.x, dy, f2_mul(f23.y, dx))), r);
                     float c1a, c1b, c2a, c2b, rra, rrb;

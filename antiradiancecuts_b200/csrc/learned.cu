@@ -11,8 +11,9 @@
 //     the CTA has 256 rows (two 128-row tiles, one set of weights) they are scored on the tensor
 //     cores (mlp_tile.cuh) and their pairs are refined or accepted by the logit, in the same
 //     launch.
-// Persistent CTAs take 256 pairs at a time from a per-level work counter; pushes and accepts use
-// warp-aggregated atomics.  The host checks the frontier size only every few levels.  Accepted
+// Persistent CTAs take 256 pairs at a time from a per-level work counter (the next chunk fetched
+// one ahead); pushes and accepts reserve their slots with one atomic per CTA and kind.  The host
+// checks the frontier size only every few levels.  Accepted
 // pairs are finally grouped by tile into the chunked cut pool (count, scan, scatter), which the
 // shared cut evaluation reads.
 //

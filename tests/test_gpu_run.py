@@ -37,3 +37,28 @@ def test_run_matches_oracle(ctx, use_cuts):
         crad, err = O.cut_solid_angle(d["pos"], d["nrm"], px, tree, d["dif"], d["spe"], d["ex"], d["cam"],
                                       math.pi / 10, 0.01)
         assert H.rel_rmse(got, crad - ar) < 1e-5
+
+
+def test_back_to_back_runs_keep_their_uploads(ctx):
+    """arc_run's upload converts into two pinned staging buffers in turn without waiting for the
+    previous frame: three runs queued back to back (AVPL sets A, B, A) give each set's own image."""
+    import torch
+
+    da = H.workload("room_256_4k", 64, 64, 4096)
+    avpls_b = da["avpls"].copy()
+    avpls_b["incRadiance"] *= 0.5  # a second AVPL set: half the radiance
+    gb = api.GBuffer(da["pos"], da["nrm"])
+    g = api.CudaGather(ctx, gb, da["mats"])
+    ext = scene.scene_extent(da["desc"])
+    cfg = api.run_config(useLightCuts=0, ar_kind=L.ARC_AR_DISK, dist_clamp=0.01)
+    ref = {}
+    for name, av in (("a", da["avpls"]), ("b", avpls_b)):
+        ref[name] = g.run(av, da["cam"], ext, cfg).result64.clone()
+        assert ctx.synchronize() == 0
+    got = []
+    for av in (da["avpls"], avpls_b, da["avpls"]):  # no synchronisation in between
+        got.append(g.run(av, da["cam"], ext, cfg).result64.clone())
+    torch.cuda.synchronize()
+    assert ctx.synchronize() == 0
+    assert torch.equal(got[0], ref["a"]) and torch.equal(got[1], ref["b"]) and torch.equal(got[2], ref["a"])
+    assert not torch.equal(ref["a"], ref["b"])
