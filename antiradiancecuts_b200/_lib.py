@@ -204,6 +204,9 @@ SIGNATURES = {
     "arc_scene_trace_avpls": (_st, [P(ArcSceneDesc), C.c_uint64, C.c_int32, C.c_int32, C.c_int32, P(ArcAvplHost),
                                     P(C.c_int64)]),
     "arc_scene_gbuffer": (_st, [P(ArcSceneDesc), C.c_int32, C.c_int32, _vp, _vp]),
+    "arc_scene_gbuffer_device": (_st, [_vp, P(ArcSceneDesc), P(ArcGBufferView)]),
+    "arc_scene_trace_avpls_device": (_st, [_vp, P(ArcSceneDesc), C.c_uint64, C.c_int32, C.c_int32,
+                                           P(ArcAvplsGpuParam), P(C.c_int64)]),
     "arc_scene_batch_views": (_st, [P(ArcSceneDesc), C.c_uint64, C.c_int32, P(ArcBatchViewDesc)]),
     "arc_batch_create": (_st, [_vp, P(_vp)]),
     "arc_batch_destroy": (_st, [_vp]),

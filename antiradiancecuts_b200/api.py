@@ -84,13 +84,23 @@ class Context:
 
 
 class GBuffer:
-    """Device G-buffer planes (float4 position, float4 normal with material in w)."""
+    """Device G-buffer planes (float4 position, float4 normal with material in w), uploaded from
+    host arrays or, with GBuffer.empty, left to be written on the device."""
 
-    def __init__(self, pos: np.ndarray, nrm: np.ndarray, device: int = 0):
+    def __init__(self, pos: np.ndarray | None, nrm: np.ndarray | None, device: int = 0, size=None):
         torch = _torch()
+        if pos is None:
+            self.width, self.height = size
+            self.pos = torch.zeros((self.height, self.width, 4), dtype=torch.float32, device=f"cuda:{device}")
+            self.nrm = torch.zeros_like(self.pos)
+            return
         self.height, self.width = pos.shape[:2]
         self.pos = torch.from_numpy(np.ascontiguousarray(pos)).to(f"cuda:{device}")
         self.nrm = torch.from_numpy(np.ascontiguousarray(nrm)).to(f"cuda:{device}")
+
+    @classmethod
+    def empty(cls, width: int, height: int, device: int = 0) -> "GBuffer":
+        return cls(None, None, device, (width, height))
 
     def view(self) -> L.ArcGBufferView:
         return L.ArcGBufferView(self.pos.data_ptr(), self.nrm.data_ptr(), self.width, self.height, self.width)
@@ -329,17 +339,25 @@ class Batch:
 class DeviceAvpls:
     """AVPLs in caller-owned device memory (a torch buffer) in the AvplsGpuParam layout: every
     instance keeps its own arrays, unlike Context.upload_avpls, which reuses one context buffer.
-    `param` is the ArcAvplsGpuParam view."""
+    `param` is the ArcAvplsGpuParam view.  DeviceAvpls(avpls) uploads host AVPLs;
+    DeviceAvpls.empty(n) leaves room for n (e.g. for the GPU light tracer)."""
 
-    def __init__(self, avpls: np.ndarray, device: int = 0):
+    _F3 = ("position", "normal", "incDirection", "incRadiance", "antiradiance")
+    _I = ("materialIndex", "bounce")
+
+    def __init__(self, avpls: np.ndarray | None, device: int = 0, count: int | None = None):
         torch = _torch()
-        a = np.ascontiguousarray(avpls, dtype=AVPL_DTYPE)
-        n = len(a)
-        f3 = [np.ascontiguousarray(a[k], np.float32).reshape(-1) for k in
-              ("position", "normal", "incDirection", "incRadiance", "antiradiance")]
-        i2 = [np.ascontiguousarray(a[k], np.int32) for k in ("materialIndex", "bounce")]
-        host = np.concatenate([x.view(np.uint8) for x in f3 + i2]) if n else np.zeros(64, np.uint8)
-        self.buf = torch.from_numpy(host).to(f"cuda:{device}")
+        if avpls is not None:
+            a = np.ascontiguousarray(avpls, dtype=AVPL_DTYPE)
+            n = len(a)
+            f3 = [np.ascontiguousarray(a[k], np.float32).reshape(-1) for k in self._F3]
+            i2 = [np.ascontiguousarray(a[k], np.int32) for k in self._I]
+            host = np.concatenate([x.view(np.uint8) for x in f3 + i2]) if n else np.zeros(64, np.uint8)
+            self.buf = torch.from_numpy(host).to(f"cuda:{device}")
+        else:
+            n = int(count)
+            self.buf = torch.zeros(max(68 * n, 64), dtype=torch.uint8, device=f"cuda:{device}")
+        self.n = n
         base = self.buf.data_ptr()
         p = L.ArcAvplsGpuParam()
         off = [0]
@@ -356,6 +374,24 @@ class DeviceAvpls:
         p.bounce = take(4 * n)
         p.numAvpls = n
         self.param = p
+
+    @classmethod
+    def empty(cls, count: int, device: int = 0) -> "DeviceAvpls":
+        return cls(None, device, count)
+
+    def to_host(self) -> np.ndarray:
+        """The AVPLs as a host array of AVPL_DTYPE (synchronises with torch's current stream)."""
+        raw = self.buf.cpu().numpy()
+        n = self.n
+        out = np.zeros(n, dtype=AVPL_DTYPE)
+        off = 0
+        for k in self._F3:
+            out[k] = raw[off:off + 12 * n].view(np.float32).reshape(n, 3)
+            off += 12 * n
+        for k in self._I:
+            out[k] = raw[off:off + 4 * n].view(np.int32)
+            off += 4 * n
+        return out
 
 
 def lbvh_params(**kw) -> L.ArcLbvhParams:

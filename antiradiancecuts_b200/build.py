@@ -66,7 +66,9 @@ def build(force: bool = False, verbose: bool = False, extra_nvcc=()) -> str:
         src, obj = os.path.join(CSRC, f), os.path.join(BUILD, f + ".o")
         objs.append(obj)
         if force or _needs(obj, src, hdr):
-            jobs.append([NVCC, *NVCC_FLAGS, *extra_nvcc, "-c", src, "-o", obj])
+            # the GPU scene generator reproduces the CPU one bit for bit: no FMA contraction
+            per_file = ["-fmad=false"] if f == "scene_gpu.cu" else []
+            jobs.append([NVCC, *NVCC_FLAGS, *per_file, *extra_nvcc, "-c", src, "-o", obj])
     for f in cpp:
         src, obj = os.path.join(CSRC, f), os.path.join(BUILD, f + ".o")
         objs.append(obj)

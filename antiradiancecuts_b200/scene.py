@@ -42,6 +42,31 @@ def gbuffer(desc: L.ArcSceneDesc, width: int, height: int) -> tuple[np.ndarray, 
     return pos, nrm
 
 
+def gbuffer_device(ctx, desc: L.ArcSceneDesc, width: int, height: int):
+    """The G-buffer of `desc` rendered on the GPU (arc_scene_gbuffer_device) into a new
+    api.GBuffer; the same bits as gbuffer()."""
+    from . import api
+
+    gb = api.GBuffer.empty(width, height)
+    L.check(ctx.lib.arc_scene_gbuffer_device(ctx.handle, C.byref(desc), C.byref(gb.view())), "arc_scene_gbuffer_device")
+    return gb
+
+
+def trace_avpls_device(ctx, desc: L.ArcSceneDesc, seed: int, num: int, max_bounces: int = 3,
+                       explicit_direct: bool = True):
+    """`num` AVPLs traced on the GPU (arc_scene_trace_avpls_device) into a new api.DeviceAvpls,
+    and the number of light paths; the AVPLs of trace_avpls(), in the same order, up to the
+    rounding of the azimuth's cos / sin."""
+    from . import api
+
+    dv = api.DeviceAvpls.empty(num)
+    paths = C.c_int64(0)
+    L.check(ctx.lib.arc_scene_trace_avpls_device(ctx.handle, C.byref(desc), int(seed), int(max_bounces),
+                                                 int(explicit_direct), C.byref(dv.param), C.byref(paths)),
+            "arc_scene_trace_avpls_device")
+    return dv, int(paths.value)
+
+
 def materials(desc: L.ArcSceneDesc):
     """(ctypes array of ArcMaterial, diffuse[m,3], specular[m,3], exponent[m])"""
     n = desc.num_materials

@@ -167,6 +167,45 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
                       f"{dt:.1f} s, extrapolated to {len(valid)} surface pixels"}
 
 
+def scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream) -> dict:
+    """The benchmark frame's inputs made on the GPU (arc_scene_trace_avpls_device,
+    arc_scene_gbuffer_device) against the CPU generator that made them (all host threads): times,
+    whether the G-buffers are the same bits, and how far the AVPLs are from the CPU's (the azimuth's
+    cos / sin come from different math libraries)."""
+    import torch
+
+    N, H, W = len(avpls), pos.shape[0], pos.shape[1]
+    t0 = time.perf_counter()
+    cpu_av, _ = scene.trace_avpls(desc, wl.avpl_seed, N, wl.max_bounces)
+    cpu_av_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    scene.gbuffer(desc, W, H)
+    cpu_gb_ms = (time.perf_counter() - t0) * 1e3
+    dv, _ = scene.trace_avpls_device(ctx, desc, wl.avpl_seed, N, wl.max_bounces)  # warm-up
+    gb = scene.gbuffer_device(ctx, desc, W, H)
+    assert ctx.synchronize() == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dv, _ = scene.trace_avpls_device(ctx, desc, wl.avpl_seed, N, wl.max_bounces)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    gpu_av_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    gb = scene.gbuffer_device(ctx, desc, W, H)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    gpu_gb_ms = e0.elapsed_time(e1)
+    assert ctx.synchronize() == 0
+    got = dv.to_host()
+    same_ints = all(np.array_equal(got[k], avpls[k]) for k in ("bounce", "materialIndex"))
+    pos_diff = float(np.abs(got["position"].astype(np.float64) - avpls["position"]).max()) if same_ints else None
+    gb_equal = np.array_equal(gb.pos.cpu().numpy(), pos) and np.array_equal(gb.nrm.cpu().numpy(), nrm)
+    return {"avpls": N, "resolution": [W, H], "gpu_ms_avpls": gpu_av_ms, "gpu_ms_gbuffer": gpu_gb_ms,
+            "cpu_ms_avpls": cpu_av_ms, "cpu_ms_gbuffer": cpu_gb_ms, "cpu_threads": os.cpu_count(),
+            "gbuffer_bit_equal": bool(gb_equal), "avpl_bounces_materials_equal": bool(same_ints),
+            "avpl_max_position_diff": pos_diff}
+
+
 def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
     """Multi-view batch: views of the room + 2 boxes scene drawn with seed 4 (resolutions from
     {256^2, 512^2, 1280x720, 1920x1080}, 8,192 - 262,144 AVPLs each, log-uniform, camera inside the
@@ -488,9 +527,10 @@ def main():
                            ref64=ref64)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
-    batch = None
+    batch = gen = None
     if not args.no_extras:
         batch = batch_leg(ctx, api, scene, L, stream, args.batch_views)
+        gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
 
     if rank == 0:
         line = {
@@ -509,7 +549,7 @@ def main():
             "roofline": roof, "cut_eval_roofline": eval_roof, "lbvh_roofline": lbvh_roof, **result,
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
-            "cpu_baseline": cpu, "clocks": clk, "batch": batch,
+            "cpu_baseline": cpu, "clocks": clk, "batch": batch, "scene_generation": gen,
         }
         if method != "learned" and args.method == "auto":
             line["config"]["learned_unavailable"] = model_error[:200]

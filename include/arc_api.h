@@ -546,6 +546,18 @@ arc_status arc_scene_trace_avpls(const ArcSceneDesc* scene, uint64_t seed, int32
 arc_status arc_scene_gbuffer(const ArcSceneDesc* scene, int32_t width, int32_t height, float* position,
                              float* normal);
 
+/* The same two generators on the GPU (csrc/scene_gpu.cu), on the context's stream: the same
+ * G-buffer bits, and the same AVPLs in the same order up to the rounding of the azimuth's
+ * cos / sin (device vs host math library).  arc_scene_gbuffer_device writes the
+ * caller's device planes `out` (out->width x out->height, row pitch out->pitch float4s; the view's
+ * planes are written).  arc_scene_trace_avpls_device writes out->numAvpls AVPLs into the caller's
+ * device SoA arrays `out` (AvplsGpuParam layout), in the CPU tracer's order; returns after the
+ * tracer has produced them (it reads the running count back between batches of paths). */
+arc_status arc_scene_gbuffer_device(arc_context* ctx, const ArcSceneDesc* scene, const ArcGBufferView* out);
+arc_status arc_scene_trace_avpls_device(arc_context* ctx, const ArcSceneDesc* scene, uint64_t seed,
+                                        int32_t max_bounces, int32_t explicit_direct_illum,
+                                        const ArcAvplsGpuParam* out, int64_t* num_paths);
+
 /* Views of a multi-view batch in `scene`: camera inside the room (outside every box) looking at a
  * point of the room at least 0.3 away, resolution drawn uniformly from {256x256, 512x512,
  * 1280x720, 1920x1080}, AVPL count log-uniform in [8192, 262144], and a seed for the view's own
