@@ -21,6 +21,7 @@ ARC_ERR_CUDA = 5
 ARC_ERR_OUT_OF_MEMORY = 6
 ARC_ERR_DEVICE = 7
 ARC_ERR_UNSUPPORTED = 8
+ARC_ERR_IO = 9
 
 ARC_DEVERR_STACK_OVERFLOW = 0x1
 ARC_DEVERR_TIMEOUT = 0x2
@@ -32,6 +33,7 @@ ARC_MAX_MATERIALS = 64
 ARC_SCENE_MAX_BOXES = 32
 
 ARC_AR_NONE, ARC_AR_DISK, ARC_AR_CONE = 0, 1, 2
+ARC_ERROR_REFERENCE, ARC_ERROR_RMSE = 0, 1
 ARC_PREC_KAHAN, ARC_PREC_KAHAN_STRICT, ARC_PREC_NAIVE, ARC_PREC_FP64 = 0, 1, 2, 3
 ARC_BBOX_SCENE, ARC_BBOX_AVPL_REFERENCE = 0, 1
 ARC_CUT_SOLID_ANGLE, ARC_CUT_ERROR_BOUND, ARC_CUT_LEARNED = 0, 1, 2
@@ -67,6 +69,10 @@ class ArcGBufferView(C.Structure):
 class ArcOutputView(C.Structure):
     _fields_ = [("result", C.c_void_p), ("radiance", C.c_void_p), ("antiradiance", C.c_void_p),
                 ("result_fp64", C.c_void_p), ("pitch", C.c_int64)]
+
+
+class ArcAccumView(C.Structure):
+    _fields_ = [("sum", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32), ("pitch", C.c_int64)]
 
 
 class ArcGatherParams(C.Structure):
@@ -205,6 +211,13 @@ SIGNATURES = {
                                     P(C.c_int64)]),
     "arc_scene_gbuffer": (_st, [P(ArcSceneDesc), C.c_int32, C.c_int32, _vp, _vp]),
     "arc_scene_gbuffer_device": (_st, [_vp, P(ArcSceneDesc), P(ArcGBufferView)]),
+    "arc_accumulate": (_st, [_vp, P(ArcOutputView), P(ArcAccumView)]),
+    "arc_accum_clear": (_st, [_vp, P(ArcAccumView)]),
+    "arc_accum_normalize": (_st, [_vp, P(ArcAccumView), C.c_int64, P(ArcOutputView)]),
+    "arc_image_error": (_st, [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int64, C.c_int32, P(C.c_double),
+                              P(C.c_double)]),
+    "arc_export_pfm": (_st, [C.c_char_p, _vp, C.c_int32, C.c_int32, C.c_int64]),
+    "arc_export_hdr": (_st, [C.c_char_p, _vp, C.c_int32, C.c_int32, C.c_int64]),
     "arc_scene_trace_avpls_device": (_st, [_vp, P(ArcSceneDesc), C.c_uint64, C.c_int32, C.c_int32,
                                            P(ArcAvplsGpuParam), P(C.c_int64)]),
     "arc_scene_batch_views": (_st, [P(ArcSceneDesc), C.c_uint64, C.c_int32, P(ArcBatchViewDesc)]),

@@ -336,6 +336,60 @@ class Batch:
         self.handle = None
 
 
+class Accumulator:
+    """FP64 running sums of the output planes over frames (arc_accumulate), normalised by the
+    number of light paths (arc_accum_normalize): Renderer::Add / Normalize (Render.cpp:298-316)."""
+
+    def __init__(self, ctx: Context, width: int, height: int, device: int = 0):
+        torch = _torch()
+        self.ctx, self.width, self.height = ctx, width, height
+        self.sum = torch.zeros((height, width, 9), dtype=torch.float64, device=f"cuda:{device}")
+        self.paths = 0
+
+    def view(self) -> L.ArcAccumView:
+        return L.ArcAccumView(self.sum.data_ptr(), self.width, self.height, self.width)
+
+    def add(self, frame: "Outputs", paths: int = 0) -> None:
+        L.check(self.ctx.lib.arc_accumulate(self.ctx.handle, C.byref(frame.view()), C.byref(self.view())),
+                "arc_accumulate")
+        self.paths += int(paths)
+
+    def clear(self) -> None:
+        L.check(self.ctx.lib.arc_accum_clear(self.ctx.handle, C.byref(self.view())), "arc_accum_clear")
+        self.paths = 0
+
+    def normalize(self, out: "Outputs", paths: int | None = None) -> "Outputs":
+        n = self.paths if paths is None else int(paths)
+        L.check(self.ctx.lib.arc_accum_normalize(self.ctx.handle, C.byref(self.view()), n, C.byref(out.view())),
+                "arc_accum_normalize")
+        return out
+
+
+def image_error(ctx: Context, reference, image, metric: int = L.ARC_ERROR_RMSE):
+    """(error, per-channel RMSE) of a device RGBA plane against a reference plane
+    (arc_image_error; CReferenceImage::GetError with metric ARC_ERROR_REFERENCE)."""
+    h, w = image.shape[:2]
+    err = C.c_double(0.0)
+    ch = (C.c_double * 3)()
+    L.check(ctx.lib.arc_image_error(ctx.handle, C.c_void_p(reference.data_ptr()), C.c_void_p(image.data_ptr()), w, h,
+                                    w, int(metric), C.byref(err), ch), "arc_image_error")
+    return err.value, np.array(list(ch))
+
+
+def export_pfm(path: str, rgba: np.ndarray) -> None:
+    """Host [H, W, 4] float32 plane (row 0 = top) to a PFM file (arc_export_pfm)."""
+    a = np.ascontiguousarray(rgba, np.float32)
+    L.check(L.load().arc_export_pfm(str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0], a.shape[1]),
+            "arc_export_pfm")
+
+
+def export_hdr(path: str, rgba: np.ndarray) -> None:
+    """Host [H, W, 4] float32 plane (row 0 = top) to a Radiance RGBE file (arc_export_hdr)."""
+    a = np.ascontiguousarray(rgba, np.float32)
+    L.check(L.load().arc_export_hdr(str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0], a.shape[1]),
+            "arc_export_hdr")
+
+
 class DeviceAvpls:
     """AVPLs in caller-owned device memory (a torch buffer) in the AvplsGpuParam layout: every
     instance keeps its own arrays, unlike Context.upload_avpls, which reuses one context buffer.

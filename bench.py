@@ -206,6 +206,42 @@ def scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream) -> dict:
             "avpl_max_position_diff": pos_diff}
 
 
+def post_leg(ctx, api, L, out, stream, hbm_gbs: float) -> dict:
+    """After the gather, at the frame's resolution: accumulating the frame's three planes into FP64
+    sums (arc_accumulate), normalising them (arc_accum_normalize) and the image error against
+    another plane (arc_image_error); device times and the accumulation's HBM roofline
+    (3 float4 read, 9 doubles read and written = 192 B per pixel)."""
+    import torch
+
+    W, H = out.width, out.height
+    acc = api.Accumulator(ctx, W, H)
+    norm = api.Outputs(W, H, fp64=False, parts=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    acc.add(out, paths=1)  # warm-up
+    reps = 10
+    e0.record(stream)
+    for _ in range(reps):
+        acc.add(out, paths=1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    acc_ms = e0.elapsed_time(e1) / reps
+    e0.record(stream)
+    acc.normalize(norm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    norm_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    err, _ = api.image_error(ctx, out.result, norm.result, L.ARC_ERROR_RMSE)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    err_ms = e0.elapsed_time(e1)
+    assert ctx.synchronize() == 0
+    gbs = 192.0 * W * H / (acc_ms * 1e-3) / 1e9
+    return {"accumulate_ms": acc_ms, "normalize_ms": norm_ms, "image_error_ms_incl_readback": err_ms,
+            "accumulate_roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_gbs, "unit": "GB/s",
+                                    "frac": gbs / hbm_gbs}, "frames_averaged_error": err}
+
+
 def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
     """Multi-view batch: views of the room + 2 boxes scene drawn with seed 4 (resolutions from
     {256^2, 512^2, 1280x720, 1920x1080}, 8,192 - 262,144 AVPLs each, log-uniform, camera inside the
@@ -527,10 +563,11 @@ def main():
                            ref64=ref64)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
-    batch = gen = None
+    batch = gen = post = None
     if not args.no_extras:
         batch = batch_leg(ctx, api, scene, L, stream, args.batch_views)
         gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
+        post = post_leg(ctx, api, L, out, stream, lbvh_roof["peak"])
 
     if rank == 0:
         line = {
@@ -549,7 +586,7 @@ def main():
             "roofline": roof, "cut_eval_roofline": eval_roof, "lbvh_roofline": lbvh_roof, **result,
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
-            "cpu_baseline": cpu, "clocks": clk, "batch": batch, "scene_generation": gen,
+            "cpu_baseline": cpu, "clocks": clk, "batch": batch, "scene_generation": gen, "post": post,
         }
         if method != "learned" and args.method == "auto":
             line["config"]["learned_unavailable"] = model_error[:200]

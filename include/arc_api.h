@@ -42,7 +42,8 @@ typedef enum arc_status {
     ARC_ERR_CUDA = 5,            /* CUDA runtime error (message in arc_last_error) */
     ARC_ERR_OUT_OF_MEMORY = 6,
     ARC_ERR_DEVICE = 7,          /* device-side error word set; see ARC_DEVERR_* */
-    ARC_ERR_UNSUPPORTED = 8
+    ARC_ERR_UNSUPPORTED = 8,
+    ARC_ERR_IO = 9               /* a file could not be written */
 } arc_status;
 
 /* Bits of the device error word returned by arc_context_synchronize. */
@@ -494,6 +495,46 @@ arc_status arc_context_set_tile_config(arc_context* ctx, int32_t tile_config);
 arc_status arc_autotune_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avpls, const ArcGBufferView* gbuffer,
                                    ArcFloat3 camera_position, const ArcGatherParams* params, const ArcOutputView* out,
                                    int32_t* best, float* times_ms, int32_t num_shapes);
+
+/* ---------------------------------------------------------------------------------------- */
+/* After the gather: accumulation, normalisation, image error, export                        */
+/* ---------------------------------------------------------------------------------------- */
+
+/* FP64 running sums of the three output planes over frames (Renderer::Add, Render.cpp:298-301):
+ * sum holds 9 doubles per pixel (result, radiance, antiradiance; r, g, b each), row pitch in
+ * pixels.  Caller-owned device memory. */
+typedef struct ArcAccumView {
+    double* sum;
+    int32_t width;
+    int32_t height;
+    int64_t pitch;
+} ArcAccumView;
+
+/* acc += the frame's planes (planes that are NULL in `frame` are skipped). */
+arc_status arc_accumulate(arc_context* ctx, const ArcOutputView* frame, const ArcAccumView* acc);
+/* acc = 0. */
+arc_status arc_accum_clear(arc_context* ctx, const ArcAccumView* acc);
+/* out = acc / num_paths (Renderer::Normalize, Render.cpp:639-664: 0 when num_paths is 0), rounded
+ * to float once; w = 1; out->result_fp64, when set, receives the FP64 quotient of the result. */
+arc_status arc_accum_normalize(arc_context* ctx, const ArcAccumView* acc, int64_t num_paths,
+                               const ArcOutputView* out);
+
+typedef enum arc_error_metric {
+    ARC_ERROR_REFERENCE = 0, /* CReferenceImage::GetError as written: (e_r * e_g + e_b) / 3 */
+    ARC_ERROR_RMSE = 1       /* the mean it was meant to be: (e_r + e_g + e_b) / 3 */
+} arc_error_metric;
+
+/* Error of device RGBA plane `image` against `reference` (CReferenceImage.cpp:28-51): per channel
+ * e_c = sqrt(mean over pixels of min(100, d_c^2)), d = reference - image in FP32, summed in FP64;
+ * *error per `metric`; channel_rmse (3 doubles, may be NULL) receives e. */
+arc_status arc_image_error(arc_context* ctx, const float* reference, const float* image, int32_t width,
+                           int32_t height, int64_t pitch, int32_t metric, double* error, double* channel_rmse);
+
+/* Host RGBA float plane (row 0 = top, pitch in pixels) to a file: PFM as CExport::ExportPFM
+ * (Utils/CExport.cpp:22-58: "PF", little-endian scale -1.0, RGB rows bottom to top), or Radiance
+ * RGBE .hdr as CExport::ExportHDR (top to bottom, run-length scanlines for widths 8..32767). */
+arc_status arc_export_pfm(const char* path, const float* rgba, int32_t width, int32_t height, int64_t pitch);
+arc_status arc_export_hdr(const char* path, const float* rgba, int32_t width, int32_t height, int64_t pitch);
 
 /* ---------------------------------------------------------------------------------------- */
 /* Synthetic scenes (CPU): inputs for tests and benchmarks                                   */
