@@ -71,6 +71,16 @@ class ArcOutputView(C.Structure):
                 ("result_fp64", C.c_void_p), ("pitch", C.c_int64)]
 
 
+class ArcClusterParams(C.Structure):
+    _fields_ = [("z_near", C.c_float), ("theta", C.c_float)]
+
+
+class ArcClusterInfo(C.Structure):
+    _fields_ = [("pixel_cluster", C.c_void_p), ("box", C.c_void_p), ("tile_count", C.c_void_p),
+                ("counts", C.c_void_p), ("lists", C.c_void_p), ("num_tiles", C.c_int32),
+                ("slots_per_tile", C.c_int32), ("list_entries", C.c_int64)]
+
+
 class ArcAccumView(C.Structure):
     _fields_ = [("sum", C.c_void_p), ("width", C.c_int32), ("height", C.c_int32), ("pitch", C.c_int64)]
 
@@ -212,6 +222,8 @@ SIGNATURES = {
     "arc_scene_gbuffer": (_st, [P(ArcSceneDesc), C.c_int32, C.c_int32, _vp, _vp]),
     "arc_scene_gbuffer_device": (_st, [_vp, P(ArcSceneDesc), P(ArcGBufferView)]),
     "arc_accumulate": (_st, [_vp, P(ArcOutputView), P(ArcAccumView)]),
+    "arc_antiradiance_clustered": (_st, [_vp, P(ArcAvplsGpuParam), P(ArcGBufferView), ArcFloat3, P(ArcClusterParams),
+                                         P(ArcGatherParams), P(ArcOutputView), P(ArcClusterInfo)]),
     "arc_accum_clear": (_st, [_vp, P(ArcAccumView)]),
     "arc_accum_normalize": (_st, [_vp, P(ArcAccumView), C.c_int64, P(ArcOutputView)]),
     "arc_image_error": (_st, [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int64, C.c_int32, P(C.c_double),

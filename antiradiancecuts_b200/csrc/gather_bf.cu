@@ -820,6 +820,21 @@ arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g) {
     return s;
 }
 
+arc_status launch_pack_records(arc_context* ctx, const ArcAvplsGpuParam* avpls, const float4** records) {
+    const int n = avpls->numAvpls;
+    float4* rec = nullptr;
+    ARC_TRY(ctx->arena.get("bf_records", (size_t)(n + 1) * 64, reinterpret_cast<void**>(&rec)));
+    if (n > 0) {
+        stage_begin(ctx, "bf_pack");
+        pack_bf_records<<<(n + 255) / 256, 256, 0, ctx->stream>>>(*avpls, ctx->d_materials, ctx->num_materials, rec,
+                                                                   ctx->d_error);
+        stage_end(ctx, 1);
+        ARC_TRY_CUDA(cudaGetLastError());
+    }
+    *records = rec;
+    return ARC_OK;
+}
+
 arc_status launch_antiradiance_only(arc_context* ctx, const GatherLaunch& g, double* ar64) {
     const ArcGatherParams& p = *g.params;
     BfArgs a = make_args(ctx, g);

@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "arc_internal.h"
+#include "scan.cuh"
 #include "scene_math.h"
 
 namespace arc {
@@ -68,82 +69,7 @@ __global__ void __launch_bounds__(kSceneThreads) scene_trace_kernel(const SceneD
     counts[i] = min(c, max_bounces);
 }
 
-// Exclusive scan of counts in blocks of kScanItems (kSceneThreads threads x 4 items): block-local
-// offsets and one total per block.
-constexpr int kScanItems = 4 * kSceneThreads;
-
-__global__ void __launch_bounds__(kSceneThreads) scan_blocks(const int* counts, int n, int* offsets, int* block_sums) {
-    __shared__ int warp_sums[kSceneThreads / 32];
-    const int base = blockIdx.x * kScanItems + 4 * threadIdx.x;
-    int v[4], s = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        v[k] = base + k < n ? counts[base + k] : 0;
-        s += v[k];
-    }
-    // inclusive scan of the thread sums over the block
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = s;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_sums[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        int ws = lane < kSceneThreads / 32 ? warp_sums[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, ws, o);
-            if (lane >= o) ws += y;
-        }
-        if (lane < kSceneThreads / 32) warp_sums[lane] = ws;
-    }
-    __syncthreads();
-    int run = x - s + (w > 0 ? warp_sums[w - 1] : 0);  // exclusive prefix of this thread
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (base + k < n) offsets[base + k] = run;
-        run += v[k];
-    }
-    if (threadIdx.x == kSceneThreads - 1) block_sums[blockIdx.x] = run;
-}
-
-// Exclusive scan of the block totals in place (one block, any count); *total gets their sum.
-__global__ void __launch_bounds__(1024) scan_totals(int* block_sums, int nblocks, int* total) {
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int b0 = 0; b0 < nblocks; b0 += 1024) {
-        const int i = b0 + threadIdx.x;
-        const int v = i < nblocks ? block_sums[i] : 0;
-        __shared__ int warp_sums[32];
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        int x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) warp_sums[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            int ws = warp_sums[lane];
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, ws, o);
-                if (lane >= o) ws += y;
-            }
-            warp_sums[lane] = ws;
-        }
-        __syncthreads();
-        const int incl = x + (w > 0 ? warp_sums[w - 1] : 0);
-        if (i < nblocks) block_sums[i] = carry + incl - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry += incl;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *total = carry;
-}
+constexpr int kScanItems = scan::kScanItems;
 
 struct ScatterArgs {
     const ArcAvplHost* slots;
@@ -246,7 +172,7 @@ extern "C" arc_status arc_scene_trace_avpls_device(arc_context* ctx, const ArcSc
     // the per-path slots stay within 4 GB (which also keeps every count sum within an int)
     const int64_t slot_cap = ((int64_t)4 << 30) / ((int64_t)max_bounces * (int64_t)sizeof(ArcAvplHost));
     const int batch = (int)std::min<int64_t>(std::max(4096, need), slot_cap);
-    const int nblocks = (batch + kScanItems - 1) / kScanItems;
+    const int nblocks = scan::num_blocks(batch);
     ArcAvplHost* slots = nullptr;
     int *counts = nullptr, *offsets = nullptr, *block_sums = nullptr, *state = nullptr;
     int64_t* paths = nullptr;
@@ -271,8 +197,7 @@ extern "C" arc_status arc_scene_trace_avpls_device(arc_context* ctx, const ArcSc
         const unsigned grid = (unsigned)((batch + kSceneThreads - 1) / kSceneThreads);
         scene_trace_kernel<<<grid, kSceneThreads, 0, st>>>(sd, seed, path0, batch, max_bounces, explicit_direct_illum,
                                                           slots, counts);
-        scan_blocks<<<nblocks, kSceneThreads, 0, st>>>(counts, batch, offsets, block_sums);
-        scan_totals<<<1, 1024, 0, st>>>(block_sums, nblocks, state + 1);
+        scan::exclusive_scan(counts, batch, offsets, block_sums, state + 1, st);
         ScatterArgs sa{slots, counts, offsets, block_sums, batch, max_bounces, path0, state, paths, *out};
         scatter_avpls<<<grid, kSceneThreads, 0, st>>>(sa);
         advance_produced<<<1, 1, 0, st>>>(state, state + 1, need);

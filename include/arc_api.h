@@ -497,6 +497,44 @@ arc_status arc_autotune_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avp
                                    int32_t* best, float* times_ms, int32_t num_shapes);
 
 /* ---------------------------------------------------------------------------------------- */
+/* Clustered deferred antiradiance (the reference's accelerator for the disk antiradiance)   */
+/* ---------------------------------------------------------------------------------------- */
+
+/* Screen clusters (VisiblePointsBvh, bvh.cu:986-1179): 16 x 16 pixel tiles split by depth slice
+ * k = floor(log(d / z_near) / log(1 + 2 tan(theta) / 16)), d the distance to the camera. */
+typedef struct ArcClusterParams {
+    float z_near; /* the camera's near plane distance */
+    float theta;  /* cameraTheta: half the vertical field of view, radians */
+} ArcClusterParams;
+
+/* Device arrays of the last arc_antiradiance_clustered call on the context (valid until the
+ * next call): pixel_cluster[height * width] (cluster slot or -1: no surface); box[slot][8]
+ * ({min, 0}, {max, 0}); tile_count[tile] (clusters of the tile, in slots tile * slots_per_tile
+ * ...); counts[slot] (AVPLs in the cluster's list) and lists (every list in slot order, each in
+ * AVPL order: the list of slot s starts at the sum of counts[0 .. s-1]). */
+typedef struct ArcClusterInfo {
+    const int32_t* pixel_cluster;
+    const float* box;
+    const int32_t* tile_count;
+    const int32_t* counts;
+    const int32_t* lists;
+    int32_t num_tiles;
+    int32_t slots_per_tile;
+    int64_t list_entries;
+} ArcClusterInfo;
+
+/* Disk antiradiance through screen clusters and their light lists (kernel_gather_cluster_lights +
+ * kernel_antiradiance_clusterred, cudaGather.cu:605-748): the AVPLs of a pixel's cluster are
+ * those whose ray (position, incDirection) meets the cluster box grown by twice the disk radius,
+ * which holds every AVPL whose disk antiradiance reaches the cluster's pixels, so the result is
+ * the brute-force disk antiradiance up to summation order.  Writes out->antiradiance (float4,
+ * w = 1) and, when set, out->result_fp64 (3 doubles per pixel: the antiradiance in FP64); other
+ * planes are untouched.  params: ar_kind ARC_AR_DISK with disk_radius > 0.  info may be NULL. */
+arc_status arc_antiradiance_clustered(arc_context* ctx, const ArcAvplsGpuParam* avpls, const ArcGBufferView* gbuffer,
+                                      ArcFloat3 camera_position, const ArcClusterParams* cparams,
+                                      const ArcGatherParams* params, const ArcOutputView* out, ArcClusterInfo* info);
+
+/* ---------------------------------------------------------------------------------------- */
 /* After the gather: accumulation, normalisation, image error, export                        */
 /* ---------------------------------------------------------------------------------------- */
 
