@@ -242,6 +242,49 @@ def post_leg(ctx, api, L, out, stream, hbm_gbs: float) -> dict:
                                     "frac": gbs / hbm_gbs}, "frames_averaged_error": err}
 
 
+def clustered_leg(ctx, api, scene, L, desc, mats, dv, gb, cam, stream) -> dict:
+    """Disk antiradiance of the benchmark frame (radius 2% of the scene extent, the reference's
+    photonRadiusScale 2) through screen clusters and light lists (arc_antiradiance_clustered)
+    against the brute-force disk antiradiance (antiradiance plane of arc_gather_bruteforce):
+    device times, list entries and the relative RMSE between the two."""
+    import torch
+
+    ctx.upload_materials(mats)  # the frame's materials (the batch leg uploads its own scene's)
+    r = 2.0 * scene.scene_extent(desc) / 100.0
+    prm = api.gather_params(L.ARC_AR_DISK, 30.0, 0.0, disk_radius=r)
+    cp = L.ArcClusterParams(0.1, math.radians(0.5 * desc.camera_fov_deg))
+    W, H = gb.width, gb.height
+    out = api.Outputs(W, H, fp64=False, parts=True)
+    ref = api.Outputs(W, H, fp64=False, parts=True)
+    info = L.ArcClusterInfo()
+
+    def clustered():
+        L.check(ctx.lib.arc_antiradiance_clustered(ctx.handle, C.byref(dv), C.byref(gb.view()), L.f3(cam), C.byref(cp),
+                                                   C.byref(prm), C.byref(out.view()), C.byref(info)),
+                "arc_antiradiance_clustered")
+
+    clustered()  # warm-up
+    word = ctx.synchronize()
+    assert word == 0, f"device error word 0x{word:x} in the clustered antiradiance"
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    clustered()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cl_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    api.gather_bruteforce(ctx, dv, gb, cam, prm, ref)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    bf_ms = e0.elapsed_time(e1)
+    assert ctx.synchronize() == 0
+    a = out.antiradiance.cpu().numpy()[..., :3].reshape(-1, 3).astype(np.float64)
+    b = ref.antiradiance.cpu().numpy()[..., :3].reshape(-1, 3).astype(np.float64)
+    rel = float(np.max(np.sqrt(np.mean((a - b) ** 2, 0)) / (np.sqrt(np.mean(b ** 2, 0)) + 1e-300)))
+    return {"disk_radius": r, "clustered_ms_incl_list_readback": cl_ms, "bruteforce_disk_ms": bf_ms,
+            "list_entries": int(info.list_entries), "rel_rmse_vs_bruteforce": rel}
+
+
 def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
     """Multi-view batch: views of the room + 2 boxes scene drawn with seed 4 (resolutions from
     {256^2, 512^2, 1280x720, 1920x1080}, 8,192 - 262,144 AVPLs each, log-uniform, camera inside the
@@ -563,11 +606,12 @@ def main():
                            ref64=ref64)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
-    batch = gen = post = None
+    batch = gen = post = clus = None
     if not args.no_extras:
         batch = batch_leg(ctx, api, scene, L, stream, args.batch_views)
         gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
         post = post_leg(ctx, api, L, out, stream, lbvh_roof["peak"])
+        clus = clustered_leg(ctx, api, scene, L, desc, mats, dv, gb, cam, stream)
 
     if rank == 0:
         line = {
@@ -587,6 +631,7 @@ def main():
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
             "cpu_baseline": cpu, "clocks": clk, "batch": batch, "scene_generation": gen, "post": post,
+            "clustered_antiradiance": clus,
         }
         if method != "learned" and args.method == "auto":
             line["config"]["learned_unavailable"] = model_error[:200]
