@@ -137,7 +137,8 @@ class ArcRunConfig(C.Structure):
                 ("cone_half_angle", C.c_float), ("dist_clamp", C.c_float), ("precision", C.c_int32),
                 ("considerNormals", C.c_int32), ("model", C.c_void_p), ("profile", C.c_int32),
                 ("ar_uncertain_factor", C.c_float), ("mlp_threshold", C.c_float), ("mlp_band", C.c_float),
-                ("cut_pool_entries", C.c_int64)]
+                ("cut_pool_entries", C.c_int64), ("useClusteredDeferred", C.c_int32), ("cluster_z_near", C.c_float),
+                ("cluster_theta", C.c_float)]
 
 
 class ArcBox(C.Structure):

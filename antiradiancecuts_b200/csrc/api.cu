@@ -167,6 +167,9 @@ void arc_run_config_default(ArcRunConfig* c) {
     c->mlp_threshold = cp.mlp_threshold;
     c->mlp_band = cp.mlp_band;
     c->cut_pool_entries = cp.cut_pool_entries;
+    c->useClusteredDeferred = 0;
+    c->cluster_z_near = 0.1f;
+    c->cluster_theta = 20.0f * 3.14159265358979f / 180.0f;  // half of a 40 degree field of view
 }
 
 arc_status arc_context_create(int32_t device, void* cuda_stream, arc_context** out) {
@@ -459,6 +462,10 @@ arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcF
     gp.cone_half_angle = config->cone_half_angle;
     gp.dist_clamp = config->dist_clamp;
     gp.precision = config->precision;
+    // clustered deferred antiradiance: the radiance pass gathers no antiradiance, the clustered
+    // pass adds it
+    const bool clustered = config->useClusteredDeferred != 0 && config->ar_kind == ARC_AR_DISK;
+    if (clustered) gp.ar_kind = ARC_AR_NONE;
 
     arc_status s = ARC_OK;
     if (config->useLightCuts) {
@@ -488,6 +495,13 @@ arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcF
         s = arc_gather_bruteforce(ctx, &d, gbuffer, camera_position, &gp, out);
     }
     if (s != ARC_OK) return s;
+    if (clustered) {
+        ArcGatherParams ga = gp;
+        ga.ar_kind = ARC_AR_DISK;
+        ArcClusterParams cl{config->cluster_z_near, config->cluster_theta};
+        s = launch_run_clustered_antiradiance(ctx, &d, gbuffer, camera_position, &cl, &ga, out);
+        if (s != ARC_OK) return s;
+    }
     if (prof) {
         ARC_TRY_CUDA(cudaEventRecord(ev[3], ctx->stream));
         ARC_TRY_CUDA(cudaEventSynchronize(ev[3]));

@@ -146,6 +146,12 @@ arc_status launch_gather_bruteforce(arc_context* ctx, const GatherLaunch& g);
 // 64-byte brute-force records of the AVPLs (p, n, w, L', A, 1/|w|) in the context's "bf_records"
 // buffer (valid until the next gather on this context)
 arc_status launch_pack_records(arc_context* ctx, const ArcAvplsGpuParam* avpls, const float4** records);
+// arc_run's clustered deferred antiradiance: `out` holds the radiance-only result; writes the
+// clustered disk antiradiance into out->antiradiance and result = radiance - antiradiance
+arc_status launch_run_clustered_antiradiance(arc_context* ctx, const ArcAvplsGpuParam* avpls,
+                                             const ArcGBufferView* gbuffer, ArcFloat3 camera_position,
+                                             const ArcClusterParams* cl, const ArcGatherParams* gp,
+                                             const ArcOutputView* out);
 arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const ArcLbvhParams* p);
 arc_status launch_lbvh_reference_nodes(arc_lbvh* bvh);
 arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsGpuParam* avpls,

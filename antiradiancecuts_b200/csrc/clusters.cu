@@ -292,7 +292,42 @@ __global__ void __launch_bounds__(kCThreads) clustered_ar(ArArgsC a) {
         for (int c = 0; c < 3; ++c) a.out_ar64[3 * o + c] = ar[c];
 }
 
+// result = radiance - antiradiance after the clustered pass: in FP64 when the caller keeps the
+// FP64 result (it then holds the radiance), else in FP32 from the float result plane
+__global__ void subtract_antiradiance(float4* result, double* result64, const double* ar64, int width, int height,
+                                      int64_t pitch) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)width * height) return;
+    const int64_t o = (int64_t)(i / width) * pitch + i % width;
+    double r[3];
+    for (int c = 0; c < 3; ++c) {
+        const double rad = result64 ? result64[3 * o + c] : (double)(&result[o].x)[c];
+        r[c] = rad - ar64[3 * o + c];
+        if (result64) result64[3 * o + c] = r[c];
+    }
+    if (result) result[o] = make_float4((float)r[0], (float)r[1], (float)r[2], 1.0f);
+}
+
 }  // namespace
+
+arc_status launch_run_clustered_antiradiance(arc_context* ctx, const ArcAvplsGpuParam* avpls,
+                                             const ArcGBufferView* gbuffer, ArcFloat3 camera_position,
+                                             const ArcClusterParams* cl, const ArcGatherParams* gp,
+                                             const ArcOutputView* out) {
+    const int W = gbuffer->width, H = gbuffer->height;
+    double* ar64 = nullptr;
+    ARC_TRY(ctx->arena.get("run_ar64", (size_t)H * out->pitch * 3 * sizeof(double), reinterpret_cast<void**>(&ar64)));
+    ArcOutputView ao{nullptr, nullptr, out->antiradiance, ar64, out->pitch};
+    ARC_TRY(arc_antiradiance_clustered(ctx, avpls, gbuffer, camera_position, cl, gp, &ao, nullptr));
+    const int64_t px = (int64_t)W * H;
+    stage_begin(ctx, "combine");
+    subtract_antiradiance<<<(unsigned)((px + 255) / 256), 256, 0, ctx->stream>>>(
+        reinterpret_cast<float4*>(out->result), out->result_fp64, ar64, W, H, out->pitch);
+    stage_end(ctx, 1);
+    ARC_TRY_CUDA(cudaGetLastError());
+    return ARC_OK;
+}
+
 }  // namespace arc
 
 using namespace arc;

@@ -441,6 +441,11 @@ typedef struct ArcRunConfig {
     float mlp_threshold;
     float mlp_band;
     int64_t cut_pool_entries;
+    /* useClusteredDeferred (cudaGather.cu:948-1031): the disk antiradiance through screen clusters
+     * (arc_antiradiance_clustered) instead of brute force; with ar_kind ARC_AR_DISK only */
+    int32_t useClusteredDeferred;
+    float cluster_z_near; /* ArcClusterParams.z_near */
+    float cluster_theta;  /* ArcClusterParams.theta */
 } ArcRunConfig;
 
 void arc_run_config_default(ArcRunConfig* c);

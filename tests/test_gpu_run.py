@@ -62,3 +62,23 @@ def test_back_to_back_runs_keep_their_uploads(ctx):
     assert ctx.synchronize() == 0
     assert torch.equal(got[0], ref["a"]) and torch.equal(got[1], ref["b"]) and torch.equal(got[2], ref["a"])
     assert not torch.equal(ref["a"], ref["b"])
+
+
+@pytest.mark.parametrize("use_cuts", [0, 1])
+def test_run_clustered_deferred_antiradiance(ctx, use_cuts):
+    """useClusteredDeferred (cudaGather.cu:948-1031): the disk antiradiance through screen
+    clusters gives the brute-force antiradiance's image up to summation order."""
+    d = H.workload("boxes2_720p_64k", 96, 64, 8192)
+    gb = api.GBuffer(d["pos"], d["nrm"])
+    g = api.CudaGather(ctx, gb, d["mats"])
+    ext = scene.scene_extent(d["desc"])
+    imgs = []
+    for clustered in (0, 1):
+        cfg = api.run_config(useLightCuts=use_cuts, ar_kind=L.ARC_AR_DISK, useClusteredDeferred=clustered,
+                             cluster_theta=math.radians(0.5 * d["desc"].camera_fov_deg))
+        out = g.run(d["avpls"], d["cam"], ext, cfg)
+        assert ctx.synchronize() == 0
+        imgs.append((out.result64.cpu().numpy().reshape(-1, 3).copy(), out.antiradiance.cpu().numpy().copy()))
+    assert np.abs(imgs[0][1]).max() > 0
+    assert H.rel_rmse(imgs[1][0], imgs[0][0]) < 1e-6
+    assert H.rel_rmse(imgs[1][1][..., :3].reshape(-1, 3), imgs[0][1][..., :3].reshape(-1, 3)) < 1e-5
