@@ -102,7 +102,9 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend: str | None = None):
+    """One process per GPU under torchrun: (world size, rank, local rank).  The process group is
+    NCCL on GPUs; gloo (CPU) when asked for, as the multi-process tests do."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -111,8 +113,14 @@ def dist_init():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=None)
+        dist.init_process_group(backend or "nccl", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def _on_gpu() -> bool:
+    import torch.distributed as dist
+
+    return dist.get_backend() == "nccl"
 
 
 def barrier(world):
@@ -120,16 +128,20 @@ def barrier(world):
         import torch
         import torch.distributed as dist
 
-        dist.barrier(device_ids=[torch.cuda.current_device()])
+        if _on_gpu():
+            dist.barrier(device_ids=[torch.cuda.current_device()])
+        else:
+            dist.barrier()
 
 
 def max_over_ranks(world, x: float) -> float:
+    """The maximum of x over the ranks (step times: the job takes as long as its slowest rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if _on_gpu() else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
