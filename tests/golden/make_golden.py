@@ -11,6 +11,10 @@ gather_kat.json
     Known-answer gather cases whose expected radiance / antiradiance follow in closed form from
     the reference's formulas (cudaGather.cu:45-144, Shaders/Gather.frag:149-208): one pixel, one
     AVPL, geometry chosen so every cosine, distance and reflection is exact.
+scene_gen.json
+    SHA-256 digests of the synthetic-scene generator's outputs (G-buffer planes and traced AVPLs
+    of the preset scenes at small sizes), so that a change to the generator's arithmetic, which
+    would move every benchmark and training input, shows in the CPU tests.
 """
 from __future__ import annotations
 
@@ -114,7 +118,35 @@ def make_kat():
         json.dump(cases, f, indent=1)
 
 
+SCENE_CASES = [(0, 0, 0), (1, 2, 2), (2, 3, 16), (3, 500, 0)]  # (preset, seed, boxes)
+
+
+def scene_digests() -> dict:
+    """Digests of scene.gbuffer (40 x 24) and scene.trace_avpls (4096 AVPLs, seed 7, 3 bounces)
+    for each preset case."""
+    import hashlib
+
+    from antiradiancecuts_b200 import scene
+
+    out = {}
+    for preset, seed, boxes in SCENE_CASES:
+        desc = scene.scene_desc(preset, seed, boxes)
+        pos, nrm = scene.gbuffer(desc, 40, 24)
+        av, paths = scene.trace_avpls(desc, 7, 4096, 3)
+        key = f"{preset}/{seed}/{boxes}"
+        out[key] = {"gbuffer": hashlib.sha256(pos.tobytes() + nrm.tobytes()).hexdigest(),
+                    "avpls": hashlib.sha256(av.tobytes()).hexdigest(), "paths": int(paths)}
+    return out
+
+
+def make_scene():
+    with open(os.path.join(HERE, "scene_gen.json"), "w") as f:
+        json.dump(scene_digests(), f, indent=1)
+
+
 if __name__ == "__main__":
-    make_morton()
-    make_kat()
+    if "--scene-only" not in sys.argv:
+        make_morton()
+        make_kat()
+    make_scene()
     print("wrote", os.listdir(HERE))

@@ -133,3 +133,19 @@ def test_bottom_up_invariants(room_small):
     np.testing.assert_allclose(tree["incRadiance"][n], d["avpls"]["incRadiance"].astype(np.float64).sum(0), rtol=1e-4)
     # representative of every inner node is one of its leaves
     assert math.isfinite(float(tree["records"][n][0]))
+
+
+def test_scene_generator_is_frozen():
+    """The synthetic-scene generator (shared by the CPU and GPU versions) still produces the inputs
+    the benchmark and the shipped network were made with (tests/golden/scene_gen.json)."""
+    import json
+    import os
+    import sys
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    import make_golden
+
+    with open(os.path.join(here, "scene_gen.json")) as f:
+        want = json.load(f)
+    assert make_golden.scene_digests() == want
