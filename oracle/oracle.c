@@ -199,6 +199,103 @@ OR_EXPORT void oracle_gather_fp64(const float* gb_pos, const float* gb_nrm, int3
     }
 }
 
+/*
+ * Clustered deferred disk antiradiance, restated from the reference (VisiblePointsBvh,
+ * bvh.cu:986-1179; kernel_gather_cluster_lights + intersectBB, cudaGather.cu:663-748;
+ * kernel_antiradiance_clusterred, cudaGather.cu:605-659) with the build's two decisions: a cluster
+ * is a (16 x 16 tile, depth slice k) of surface pixels, k = floor(log(d / z_near) /
+ * log(1 + 2 tan(theta) / 16)), and its list holds the AVPLs whose ray (position, incDirection) meets
+ * its box grown by twice the disk radius, in AVPL order.  Every surface pixel's antiradiance is the
+ * FP64 disk term summed over its cluster's list.  out_ar: [W * H][3]; returns the number of list
+ * entries over all clusters (*out_clusters: the number of clusters).
+ */
+static int ray_box_f(const float lo[3], const float hi[3], const float* o, const float* d) {
+    float t1[3], t2[3];
+    for (int k = 0; k < 3; ++k) {
+        const float f = 1.0f / d[k];
+        t1[k] = (lo[k] - o[k]) * f;
+        t2[k] = (hi[k] - o[k]) * f;
+    }
+    const float tmin = fmaxf(fmaxf(fminf(t1[0], t2[0]), fminf(t1[1], t2[1])), fminf(t1[2], t2[2]));
+    const float tmax = fminf(fminf(fmaxf(t1[0], t2[0]), fmaxf(t1[1], t2[1])), fmaxf(t1[2], t2[2]));
+    return !(tmax < 0.0f || tmin > tmax);
+}
+
+OR_EXPORT int64_t oracle_clustered_disk_ar(const float* gb_pos, const float* gb_nrm, int32_t W, int32_t H,
+                                           const float* a_pos, const float* a_nrm, const float* a_w, const float* a_A,
+                                           int32_t num_avpls, const float* diffuse, const float* specular,
+                                           const float* exponent, int32_t num_materials, const float* cam, float z_near,
+                                           float theta, const oracle_params* P, double* out_ar, int32_t* out_clusters) {
+    oracle_materials M = {diffuse, specular, exponent, num_materials};
+    const d3 c = d3load(cam);
+    const double step = log(1.0 + 2.0 * tan((double)theta) / 16.0);
+    const int tiles_x = (W + 15) / 16, tiles_y = (H + 15) / 16;
+    const float grow = 2.0f * P->disk_radius;
+    int64_t entries = 0;
+    int32_t clusters = 0;
+    for (int64_t i = 0; i < (int64_t)W * H * 3; ++i) out_ar[i] = 0.0;
+    int* list = (int*)malloc(sizeof(int) * (size_t)(num_avpls > 0 ? num_avpls : 1));
+    for (int ty = 0; ty < tiles_y; ++ty)
+        for (int tx = 0; tx < tiles_x; ++tx) {
+            // depth slice of every surface pixel of the tile
+            int kk[256], px[256], np = 0;
+            for (int y = ty * 16; y < ty * 16 + 16 && y < H; ++y)
+                for (int x = tx * 16; x < tx * 16 + 16 && x < W; ++x) {
+                    const float* gn = gb_nrm + 4 * ((int64_t)y * W + x);
+                    if (!(gn[3] > 0.0f)) continue;
+                    const d3 p = d3load(gb_pos + 4 * ((int64_t)y * W + x));
+                    const double d = d3len(d3sub(c, p));
+                    kk[np] = (int)floor(log(d / (double)z_near) / step);
+                    px[np++] = y * W + x;
+                }
+            // one cluster per distinct slice
+            for (int a = 0; a < np; ++a) {
+                int seen = 0;
+                for (int b = 0; b < a; ++b) seen |= kk[b] == kk[a];
+                if (seen) continue;
+                ++clusters;
+                float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+                for (int b = a; b < np; ++b) {
+                    if (kk[b] != kk[a]) continue;
+                    const float* p = gb_pos + 4 * (int64_t)px[b];
+                    for (int k = 0; k < 3; ++k) {
+                        lo[k] = fminf(lo[k], p[k]);
+                        hi[k] = fmaxf(hi[k], p[k]);
+                    }
+                }
+                for (int k = 0; k < 3; ++k) {
+                    lo[k] = lo[k] - grow;
+                    hi[k] = hi[k] + grow;
+                }
+                int nl = 0;
+                for (int32_t i = 0; i < num_avpls; ++i)
+                    if (ray_box_f(lo, hi, a_pos + 3 * i, a_w + 3 * i)) list[nl++] = i;
+                entries += nl;
+                for (int b = a; b < np; ++b) {
+                    if (kk[b] != kk[a]) continue;
+                    const float* gp = gb_pos + 4 * (int64_t)px[b];
+                    const float* gn = gb_nrm + 4 * (int64_t)px[b];
+                    const int mat = (int)gn[3];
+                    if (mat <= 0 || mat >= num_materials) continue;
+                    d3 ar = d3m(0, 0, 0);
+                    for (int q = 0; q < nl; ++q) {
+                        const int i = list[q];
+                        ar = d3add(ar, antiradiance_disk(d3load(gp), d3load(gn), mat, d3load(a_pos + 3 * i),
+                                                         d3load(a_nrm + 3 * i), d3load(a_w + 3 * i),
+                                                         d3load(a_A + 3 * i), c, &M, P));
+                    }
+                    double* o = out_ar + 3 * (int64_t)px[b];
+                    o[0] = ar.x;
+                    o[1] = ar.y;
+                    o[2] = ar.z;
+                }
+            }
+        }
+    free(list);
+    if (out_clusters) *out_clusters = clusters;
+    return entries;
+}
+
 /* ---------------------------------------------------------------------------------------- */
 /* Scalar FP32 gather: the reference's arithmetic (plain float sums, float combine), used as */
 /* the timed CPU baseline.  Lambertian fast form is not assumed: every term evaluates the     */

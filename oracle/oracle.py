@@ -87,6 +87,23 @@ def gather_fp64(pos4, nrm4, pixels, avpls, diffuse, specular, exponent, cam, prm
     return rad, ar, res
 
 
+def clustered_disk_ar(pos4, nrm4, avpls, diffuse, specular, exponent, cam, z_near, theta, prm: OracleParams):
+    """Clustered deferred disk antiradiance (oracle_clustered_disk_ar) over a whole [H, W] G-buffer
+    -> (antiradiance [H*W, 3] FP64, number of clusters, list entries)."""
+    pos4, nrm4 = _f32(pos4), _f32(nrm4)
+    h, w = pos4.shape[:2]
+    a = _avpl_arrays(avpls)
+    out = np.zeros((h * w, 3), np.float64)
+    dif, spe, ex = _f32(diffuse), _f32(specular), _f32(exponent)
+    nc = C.c_int32(0)
+    f = lib().oracle_clustered_disk_ar
+    f.restype = C.c_int64
+    entries = f(_p(pos4), _p(nrm4), C.c_int32(w), C.c_int32(h), _p(a[0]), _p(a[1]), _p(a[2]), _p(a[4]),
+                C.c_int32(len(avpls)), _p(dif), _p(spe), _p(ex), C.c_int32(len(dif)), _p(_f32(cam)),
+                C.c_float(z_near), C.c_float(theta), C.byref(prm), _p(out), C.byref(nc))
+    return out, nc.value, int(entries)
+
+
 def gather_fp32(pos4, nrm4, pixels, avpls, diffuse, specular, exponent, cam, prm: OracleParams, threads=1):
     """Scalar FP32 gather (the reference's arithmetic) -> result [k,3] float32."""
     pos4, nrm4 = _f32(pos4), _f32(nrm4)

@@ -149,3 +149,27 @@ def test_scene_generator_is_frozen():
     with open(os.path.join(here, "scene_gen.json")) as f:
         want = json.load(f)
     assert make_golden.scene_digests() == want
+
+
+def test_clustered_disk_antiradiance_equals_bruteforce_in_the_oracle():
+    """The cluster light lists keep every AVPL whose disk antiradiance reaches a pixel of the
+    cluster: in the FP64 oracle the clustered sum equals the full sum bit for bit (the AVPLs left
+    out contribute exact zeros, and the order is the AVPLs' order)."""
+    import math
+
+    import numpy as np
+
+    import helpers as H
+    from antiradiancecuts_b200 import scene
+    from oracle import oracle as O
+
+    d = H.workload("boxes2_720p_64k", 48, 32, 2048)
+    r = 2.0 * scene.scene_extent(d["desc"]) / 100.0
+    prm = O.params(1, 30.0, 0.0, r)
+    ar, nclusters, entries = O.clustered_disk_ar(d["pos"], d["nrm"], d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"],
+                                                 0.1, math.radians(0.5 * d["desc"].camera_fov_deg), prm)
+    px = np.arange(48 * 32)
+    _, full, _ = O.gather_fp64(d["pos"], d["nrm"], px, d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"], prm)
+    assert np.abs(full).max() > 0 and nclusters > 6
+    assert 0 < entries < nclusters * len(d["avpls"])  # the lists do cull
+    assert np.array_equal(ar, full)
