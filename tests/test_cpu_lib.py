@@ -96,3 +96,35 @@ def test_gbuffer_centre_pixel_hits_back_wall():
     assert abs(pos[c][2] - 1.0) < 1e-6 and nrm[c][3] == 1.0
     assert np.allclose(nrm[c][:3], [0, 0, -1])
     assert (nrm[..., 3] == 0).any()  # the corners see past the open front
+
+
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """Every ctypes structure of _lib.py has the size and field offsets that the C compiler gives
+    the header's struct of the same name (include/arc_api.h), so no call passes a skewed struct."""
+    import inspect
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "arc_api.h")).read()
+    structs = [(n, c) for n, c in inspect.getmembers(L, inspect.isclass)
+               if issubclass(c, C.Structure) and f"typedef struct {n} " in header]
+    assert len(structs) >= 15
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "arc_api.h"', "int main(void) {"]
+    for n, c in structs:
+        lines.append(f'    printf("{n} #sizeof %zu\\n", sizeof({n}));')
+        for f in c._fields_:
+            lines.append(f'    printf("{n} {f[0]} %zu\\n", offsetof({n}, {f[0]}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layouts.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layouts"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        n, field, v = line.split()
+        got[(n, field)] = int(v)
+    for n, c in structs:
+        assert got[(n, "#sizeof")] == C.sizeof(c), n
+        for f in c._fields_:
+            assert got[(n, f[0])] == getattr(c, f[0]).offset, (n, f[0])
