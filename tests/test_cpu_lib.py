@@ -128,3 +128,37 @@ def test_ctypes_layouts_match_the_header(tmp_path):
         assert got[(n, "#sizeof")] == C.sizeof(c), n
         for f in c._fields_:
             assert got[(n, f[0])] == getattr(c, f[0]).offset, (n, f[0])
+
+
+def test_plain_c_host_links_and_calls_the_library(tmp_path):
+    """A C host (the reference's side of the boundary) compiles against include/arc_api.h, links
+    libarc.so and calls it: host-only entry points, and an export written from C and read back."""
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "antiradiancecuts_b200")
+    out_file = tmp_path / "c.pfm"
+    src = tmp_path / "host.c"
+    src.write_text(r"""
+#include <stdio.h>
+#include <string.h>
+#include "arc_api.h"
+int main(int argc, char** argv) {
+    ArcRunConfig cfg;
+    arc_run_config_default(&cfg);
+    float px[2 * 2 * 4];
+    for (int i = 0; i < 16; ++i) px[i] = (float)i;
+    int s = arc_export_pfm(argv[1], px, 2, 2, 2);
+    printf("%s %d %d %s\n", arc_status_string(s), cfg.useLightCuts, cfg.useClusteredDeferred,
+           arc_status_string(ARC_ERR_INVALID_ARG));
+    return s == ARC_OK ? 0 : 1;
+}
+""")
+    exe = tmp_path / "host"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(root, "include"), str(src), "-L", libdir, "-larc",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe), str(out_file)], check=True, capture_output=True, text=True)
+    words = r.stdout.split()
+    assert words[1:3] == ["1", "0"]
+    assert out_file.read_bytes().startswith(b"PF\n2 2\n-1.0\n")
