@@ -109,3 +109,28 @@ def test_clustered_needs_the_disk_variant(ctx, case):
     st = ctx.lib.arc_antiradiance_clustered(ctx.handle, C.byref(dv.param), C.byref(gb.view()), L.f3(d["cam"]),
                                             C.byref(cp), C.byref(cone), C.byref(out.view()), None)
     assert st == L.ARC_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("w,h,z_near,theta", [(37, 21, 0.1, 0.35), (64, 48, 1e-6, 0.01)])
+def test_clustered_edge_cases(ctx, w, h, z_near, theta):
+    """Partial tiles (an image that is not a multiple of 16), and slices so thin that nearly every
+    pixel of a tile is its own cluster (up to 256 per tile): still the brute-force antiradiance."""
+    d = H.workload("boxes2_720p_64k", w, h, 4096)
+    ctx.upload_materials(d["mats"])
+    dv = api.DeviceAvpls(d["avpls"])
+    gb = api.GBuffer(d["pos"], d["nrm"])
+    r = 2.0 * scene.scene_extent(d["desc"]) / 100.0
+    prm = api.gather_params(L.ARC_AR_DISK, 30.0, 0.0, disk_radius=r)
+    out, ref = api.Outputs(w, h), api.Outputs(w, h)
+    info = L.ArcClusterInfo()
+    L.check(ctx.lib.arc_antiradiance_clustered(ctx.handle, C.byref(dv.param), C.byref(gb.view()), L.f3(d["cam"]),
+                                               C.byref(L.ArcClusterParams(z_near, theta)), C.byref(prm),
+                                               C.byref(out.view()), C.byref(info)), "arc_antiradiance_clustered")
+    api.gather_bruteforce(ctx, dv.param, gb, d["cam"], prm, ref)
+    assert ctx.synchronize() == 0
+    tc = ctx.d2h(info.tile_count, np.int32, info.num_tiles)
+    a = out.antiradiance.cpu().numpy()[..., :3].reshape(-1, 3)
+    b = ref.antiradiance.cpu().numpy()[..., :3].reshape(-1, 3)
+    assert H.rel_rmse(a, b) < 1e-5
+    if z_near < 1e-3:
+        assert tc.max() > 64  # many clusters in a tile
