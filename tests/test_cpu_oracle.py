@@ -151,25 +151,26 @@ def test_scene_generator_is_frozen():
     assert make_golden.scene_digests() == want
 
 
-def test_clustered_disk_antiradiance_equals_bruteforce_in_the_oracle():
+@pytest.mark.parametrize("w,h,z_near,theta_deg", [(48, 32, 0.1, None), (37, 21, 0.1, 20.0), (32, 32, 1e-6, 0.5)])
+def test_clustered_disk_antiradiance_equals_bruteforce_in_the_oracle(w, h, z_near, theta_deg):
     """The cluster light lists keep every AVPL whose disk antiradiance reaches a pixel of the
     cluster: in the FP64 oracle the clustered sum equals the full sum bit for bit (the AVPLs left
-    out contribute exact zeros, and the order is the AVPLs' order)."""
-    import math
-
-    import numpy as np
-
+    out contribute exact zeros, and the order is the AVPLs' order).  Also on partial tiles and with
+    slices so thin that most pixels of a tile are clusters of their own."""
     import helpers as H
     from antiradiancecuts_b200 import scene
     from oracle import oracle as O
 
-    d = H.workload("boxes2_720p_64k", 48, 32, 2048)
+    d = H.workload("boxes2_720p_64k", w, h, 2048)
     r = 2.0 * scene.scene_extent(d["desc"]) / 100.0
     prm = O.params(1, 30.0, 0.0, r)
+    theta = math.radians(0.5 * d["desc"].camera_fov_deg if theta_deg is None else theta_deg)
     ar, nclusters, entries = O.clustered_disk_ar(d["pos"], d["nrm"], d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"],
-                                                 0.1, math.radians(0.5 * d["desc"].camera_fov_deg), prm)
-    px = np.arange(48 * 32)
+                                                 z_near, theta, prm)
+    px = np.arange(w * h)
     _, full, _ = O.gather_fp64(d["pos"], d["nrm"], px, d["avpls"], d["dif"], d["spe"], d["ex"], d["cam"], prm)
     assert np.abs(full).max() > 0 and nclusters > 6
+    if z_near < 1e-3:
+        assert nclusters > 4 * 64  # four 16x16 tiles, most of their pixels in clusters of their own
     assert 0 < entries < nclusters * len(d["avpls"])  # the lists do cull
     assert np.array_equal(ar, full)
