@@ -25,3 +25,23 @@ def test_gradient_matches_finite_differences(loss):
         pm[i] -= h
         fd = (M.loss_and_grad(pp, x, lab, w, loss=loss)[0] - M.loss_and_grad(pm, x, lab, w, loss=loss)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
+
+
+def test_shipped_model_archive():
+    """The shipped cut network: the archive fields a C / C++ host reads, the parameter count the
+    library expects, finite weights, and finite logits through the FP64 network."""
+    from antiradiancecuts_b200 import _lib as L
+    from antiradiancecuts_b200 import learned
+
+    z = np.load(learned.DEFAULT_MODEL)
+    assert set(z.files) >= {"params", "loss", "threshold", "band"}
+    p = z["params"]
+    assert p.dtype == np.float32 and p.shape == (M.NUM_PARAMS,)
+    assert L.load().arc_mlp_num_params() == M.NUM_PARAMS == learned.NUM_PARAMS
+    assert np.all(np.isfinite(p)) and np.abs(p).max() > 0
+    assert int(z["loss"]) == L.ARC_MLP_LOSS_BCE
+    assert float(z["threshold"]) == pytest.approx(0.05)
+    assert float(z["band"]) == learned.PREACCEPT_BAND
+    x = np.random.default_rng(0).normal(0, 1, (256, 16))
+    logits, _ = M.forward(p.astype(np.float64), x)
+    assert np.all(np.isfinite(logits)) and np.std(logits) > 0
