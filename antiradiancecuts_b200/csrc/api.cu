@@ -446,10 +446,9 @@ arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcF
                    const ArcOutputView* out) {
     ARC_CHECK_ARG(ctx && config && gbuffer && out, "NULL argument");
     ARC_TRY_CUDA(cudaSetDevice(ctx->device));
-    cudaEvent_t ev[4];
+    ScopedEvents<4> ev;
     const bool prof = config->profile != 0;
-    if (prof)
-        for (auto& e : ev) ARC_TRY_CUDA(cudaEventCreate(&e));
+    if (prof) ARC_TRY_CUDA(ev.create());
     if (prof) ARC_TRY_CUDA(cudaEventRecord(ev[0], ctx->stream));
     ArcAvplsGpuParam d;
     ARC_TRY(arc_avpls_upload(ctx, avpls, num, &d));
@@ -512,7 +511,6 @@ arc_status arc_run(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcF
         printf("transfer avpl data to gpu took: %.3fms\n", t01);
         if (config->useLightCuts) printf("gather build bvh took: %.3fms\n", t12);
         printf("gather radiance and antiradiance took: %.3fms\n", t23);
-        for (auto& e : ev) cudaEventDestroy(e);
     }
     return check_device_errors(ctx);
 }

@@ -39,6 +39,24 @@ void set_last_error(const std::string& msg);
         if (_s != ARC_OK) return _s;       \
     } while (0)
 
+// N CUDA events that a host function creates (create()) and that are destroyed on every return.
+template <int N>
+struct ScopedEvents {
+    cudaEvent_t e[N] = {};
+    cudaError_t create() {
+        for (cudaEvent_t& x : e) {
+            const cudaError_t r = cudaEventCreate(&x);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    }
+    ~ScopedEvents() {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+    cudaEvent_t operator[](int i) const { return e[i]; }
+};
+
 // Per-material data the kernels read: {diffuse.xyz, exponent}, {specular.xyz, has_specular}.
 struct MaterialRecord {
     float4 diffuse_exp;

@@ -1099,13 +1099,10 @@ extern "C" arc_status arc_autotune_bruteforce(arc_context* ctx, const ArcAvplsGp
     ARC_CHECK_ARG(ctx && avpls && gbuffer && params && out && best, "NULL argument");
     ARC_CHECK_ARG(!times_ms || num_shapes >= kNumTileShapes, "times_ms holds fewer entries than there are shapes");
     ARC_TRY_CUDA(cudaSetDevice(ctx->device));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    ARC_TRY_CUDA(cudaEventCreate(&e0));
-    cudaError_t ce = cudaEventCreate(&e1);
-    if (ce != cudaSuccess) {
-        cudaEventDestroy(e0);
-        ARC_TRY_CUDA(ce);
-    }
+    ScopedEvents<2> ev;
+    ARC_TRY_CUDA(ev.create());
+    const cudaEvent_t e0 = ev[0], e1 = ev[1];
+    cudaError_t ce = cudaSuccess;
     arc_status s = ARC_OK;
     float best_ms = 0.0f;
     int best_i = -1;
@@ -1129,8 +1126,6 @@ extern "C" arc_status arc_autotune_bruteforce(arc_context* ctx, const ArcAvplsGp
             best_i = i;
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     ARC_TRY(s);
     ctx->bf_tile_config = best_i;
     *best = best_i;

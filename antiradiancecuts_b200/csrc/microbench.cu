@@ -59,9 +59,9 @@ extern "C" arc_status arc_measure_fp32_peak(arc_context* ctx, double* scalar_tfl
     ARC_TRY(ctx->arena.get("fma_sink", 1024 * sizeof(float), reinterpret_cast<void**>(&out)));
     const int blocks = ctx->sm_count * 8;
     const double flops = 2.0 * kChains * (double)kIters * blocks * 256;
-    cudaEvent_t e0, e1;
-    ARC_TRY_CUDA(cudaEventCreate(&e0));
-    ARC_TRY_CUDA(cudaEventCreate(&e1));
+    ScopedEvents<2> ev;
+    ARC_TRY_CUDA(ev.create());
+    const cudaEvent_t e0 = ev[0], e1 = ev[1];
     float best[2] = {1e30f, 1e30f};
     for (int rep = 0; rep < 6; ++rep) {
         for (int v = 0; v < 2; ++v) {
@@ -77,8 +77,6 @@ extern "C" arc_status arc_measure_fp32_peak(arc_context* ctx, double* scalar_tfl
             if (rep > 0 && ms < best[v]) best[v] = ms;  // rep 0 warms up
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     *scalar_tflops = flops / (best[0] * 1e-3) / 1e12;
     *packed_tflops = flops / (best[1] * 1e-3) / 1e12;
     return ARC_OK;

@@ -82,3 +82,40 @@ def test_run_clustered_deferred_antiradiance(ctx, use_cuts):
     assert np.abs(imgs[0][1]).max() > 0
     assert H.rel_rmse(imgs[1][0], imgs[0][0]) < 1e-6
     assert H.rel_rmse(imgs[1][1][..., :3].reshape(-1, 3), imgs[0][1][..., :3].reshape(-1, 3)) < 1e-5
+
+
+def test_run_profile_prints_stage_times_and_keeps_the_image(ctx, capfd):
+    """ArcRunConfig.profile: the three stage lines of the reference's run() timers
+    (cudaGather.cu:845-1049) are printed, the image is unchanged, and a profiled call that fails
+    midway (one AVPL: too few for the tree) returns its status and leaves the context usable."""
+    import ctypes as C
+
+    d = H.workload("room_256_4k", 64, 64, 4096)
+    gb = api.GBuffer(d["pos"], d["nrm"])
+    g = api.CudaGather(ctx, gb, d["mats"])
+    ext = scene.scene_extent(d["desc"])
+    ref = g.run(d["avpls"], d["cam"], ext, api.run_config(useLightCuts=1, ar_kind=L.ARC_AR_DISK)).result64.clone()
+    assert ctx.synchronize() == 0
+    got = g.run(d["avpls"], d["cam"], ext, api.run_config(useLightCuts=1, ar_kind=L.ARC_AR_DISK, profile=1))
+    assert ctx.synchronize() == 0
+    C.CDLL(None).fflush(None)
+    text = capfd.readouterr().out
+    for line in ("transfer avpl data to gpu took:", "gather build bvh took:", "gather radiance and antiradiance took:"):
+        assert line in text
+    assert np.array_equal(got.result64.cpu().numpy(), ref.cpu().numpy())
+    with pytest.raises(L.ArcError) as e:
+        g.run(d["avpls"][:1], d["cam"], ext, api.run_config(useLightCuts=1, ar_kind=L.ARC_AR_DISK, profile=1))
+    assert e.value.status == L.ARC_ERR_TOO_FEW_AVPLS
+    again = g.run(d["avpls"], d["cam"], ext, api.run_config(useLightCuts=1, ar_kind=L.ARC_AR_DISK, profile=1))
+    assert ctx.synchronize() == 0
+    assert np.array_equal(again.result64.cpu().numpy(), ref.cpu().numpy())
+
+
+def test_measure_fp32_peak_is_plausible(ctx):
+    """arc_measure_fp32_peak: the FFMA microbenchmark that is the gather kernels' roofline
+    denominator (B200: 148 SMs x 128 FP32 lanes x 2 FLOP x ~1.9 GHz = ~72 TFLOP/s)."""
+    import ctypes as C
+
+    sc, pk = C.c_double(), C.c_double()
+    L.check(ctx.lib.arc_measure_fp32_peak(ctx.handle, C.byref(sc), C.byref(pk)), "arc_measure_fp32_peak")
+    assert 20.0 < sc.value < 120.0 and 20.0 < pk.value < 120.0
