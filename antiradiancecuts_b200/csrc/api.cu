@@ -111,6 +111,7 @@ const char* arc_status_string(int32_t s) {
         case ARC_ERR_OUT_OF_MEMORY: return "ARC_ERR_OUT_OF_MEMORY";
         case ARC_ERR_DEVICE: return "ARC_ERR_DEVICE";
         case ARC_ERR_UNSUPPORTED: return "ARC_ERR_UNSUPPORTED";
+        case ARC_ERR_IO: return "ARC_ERR_IO";
         default: return "ARC_ERR_UNKNOWN";
     }
 }

@@ -42,6 +42,14 @@ def test_status_strings_and_version():
     lib = L.load()
     assert lib.arc_api_version() == 1
     assert L.status_string(L.ARC_ERR_TOO_FEW_AVPLS) == "ARC_ERR_TOO_FEW_AVPLS"
+    # every status the header declares has its own name
+    hdr = open(os.path.join(ROOT, "include", "arc_api.h")).read()
+    enum = re.search(r"typedef enum arc_status \{(.*?)\} arc_status;", hdr, re.S).group(1)
+    declared = dict((n, int(v)) for n, v in re.findall(r"(ARC_\w+)\s*=\s*(\d+)", enum))
+    assert len(declared) >= 10
+    for name, value in declared.items():
+        assert L.status_string(value) == name
+    assert L.status_string(max(declared.values()) + 1) == "ARC_ERR_UNKNOWN"
 
 
 def test_defaults():
