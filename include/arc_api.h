@@ -30,7 +30,8 @@ extern "C" {
 
 #define ARC_API_VERSION 1
 /* The reference caches at most 20 materials in shared memory (cudaGather.cu:18); this
- * library keeps up to 64 in constant memory and rejects more with ARC_ERR_INVALID_ARG. */
+ * library keeps a device table of up to 64 (staged into shared memory by the kernels that read
+ * it per pixel) and rejects more with ARC_ERR_INVALID_ARG. */
 #define ARC_MAX_MATERIALS 64
 
 typedef enum arc_status {
