@@ -57,9 +57,21 @@ def test_defaults():
     p = L.ArcCutParams()
     lib.arc_cut_params_default(C.byref(p))
     assert abs(p.solid_angle_threshold - np.pi / 10) < 1e-6 and p.error_bound == np.float32(0.01)
+    assert p.kind == L.ARC_CUT_ERROR_BOUND and p.ar_uncertain_factor == 16.0 and p.mlp_threshold == 0.5
     r = L.ArcRunConfig()
     lib.arc_run_config_default(C.byref(r))
     assert r.useLightCuts == 1 and abs(r.photonRadiusScale - 2.0) < 1e-7
+    # CConfigManager's defaults: solid-angle cut at pi / 10, disk antiradiance, no clustered pass
+    assert r.cut_kind == L.ARC_CUT_SOLID_ANGLE and abs(r.clusterRefinementThreshold - np.pi / 10) < 1e-6
+    assert r.ar_kind == L.ARC_AR_DISK and r.useClusteredDeferred == 0 and r.precision == L.ARC_PREC_KAHAN
+    assert abs(r.cluster_z_near - 0.1) < 1e-7 and abs(r.cluster_theta - np.radians(20.0)) < 1e-6
+    g = L.ArcGatherParams()
+    lib.arc_gather_params_default(C.byref(g))
+    assert g.ar_kind == L.ARC_AR_CONE and abs(g.cone_half_angle - np.radians(30.0)) < 1e-6
+    assert g.dist_clamp == 0.0 and g.precision == L.ARC_PREC_KAHAN and g.tile_config == -1
+    b = L.ArcLbvhParams()
+    lib.arc_lbvh_params_default(C.byref(b))
+    assert b.bbox_mode == L.ARC_BBOX_SCENE and b.repr_seed == 5489 and b.consider_normals == 0
 
 
 def test_null_arguments_are_rejected():
