@@ -67,3 +67,28 @@ def test_reference_arm_runs_on_rank_zero_only():
             "rc = bench.run_reference(a) if r == 1 else 0; print('rc', rc)")
     outs = _launch(code, 2)
     assert outs[1].strip().splitlines()[-1] == "rc 0"  # rank 1 returns at once, without work
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` needs no GPU: on a small workload it prints one JSON line with
+    the benchmark's metric, a cpu_baseline describing the run and an e2e with no copies."""
+    import json
+
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                        "room_256_4k", "--steps", "2", "--warmup", "1"], env=env, capture_output=True, text=True,
+                       timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [s for s in r.stdout.splitlines() if s.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    import bench
+
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["value"] > 0 and line["ms_per_step"] == line["value"] and line["higher_is_better"] is False
+    assert line["steps"] == 2 and line["warmup"] == 1 and line["n_gpus"] == 1
+    b = line["cpu_baseline"]
+    assert b["value"] == line["value"] and b["kind"] in ("port", "reference") and b["cores"] >= 1 and b["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["config"]["workload"] == "room_256_4k"
