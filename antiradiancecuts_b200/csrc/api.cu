@@ -222,6 +222,7 @@ arc_status arc_context_destroy(arc_context* ctx) {
 
 arc_status arc_context_synchronize(arc_context* ctx, uint32_t* device_error_word) {
     ARC_CHECK_ARG(ctx != nullptr, "ctx is NULL");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     uint32_t word = 0;
     ARC_TRY_CUDA(cudaMemcpyAsync(&word, ctx->d_error, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
     ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -243,6 +244,7 @@ arc_status arc_context_profile(arc_context* ctx, int32_t enable) {
 arc_status arc_context_stage_times(arc_context* ctx, char* names, size_t names_len, float* ms, int32_t max_stages,
                                    int32_t* num_stages) {
     ARC_CHECK_ARG(ctx && names && ms && num_stages && names_len > 0, "NULL argument");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     StageTimer& t = ctx->timer;
     ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
     std::string joined;
@@ -274,12 +276,14 @@ arc_status arc_device_alloc(arc_context* ctx, size_t bytes, void** out) {
 
 arc_status arc_device_free(arc_context* ctx, void* ptr) {
     ARC_CHECK_ARG(ctx != nullptr, "ctx is NULL");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     if (ptr) ARC_TRY_CUDA(cudaFree(ptr));
     return ARC_OK;
 }
 
 arc_status arc_copy_h2d(arc_context* ctx, void* dst, const void* src, size_t bytes) {
     ARC_CHECK_ARG(ctx && dst && src, "NULL argument");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     ARC_TRY_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
     ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
     return ARC_OK;
@@ -287,6 +291,7 @@ arc_status arc_copy_h2d(arc_context* ctx, void* dst, const void* src, size_t byt
 
 arc_status arc_copy_d2h(arc_context* ctx, void* dst, const void* src, size_t bytes) {
     ARC_CHECK_ARG(ctx && dst && src, "NULL argument");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     ARC_TRY_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     ARC_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
     return ARC_OK;
@@ -295,6 +300,7 @@ arc_status arc_copy_d2h(arc_context* ctx, void* dst, const void* src, size_t byt
 arc_status arc_materials_upload(arc_context* ctx, const ArcMaterial* materials, int32_t num) {
     ARC_CHECK_ARG(ctx && materials, "NULL argument");
     ARC_CHECK_ARG(num > 0 && num <= ARC_MAX_MATERIALS, "material count must be in [1, ARC_MAX_MATERIALS]");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     MaterialRecord recs[ARC_MAX_MATERIALS];
     std::memset(recs, 0, sizeof(recs));
     bool spec = false;
@@ -318,6 +324,7 @@ arc_status arc_materials_upload(arc_context* ctx, const ArcMaterial* materials, 
 arc_status arc_avpls_upload(arc_context* ctx, const ArcAvplHost* avpls, int32_t num, ArcAvplsGpuParam* out) {
     ARC_CHECK_ARG(ctx && out && (avpls || num == 0), "NULL argument");
     ARC_CHECK_ARG(num >= 0, "negative AVPL count");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     // AoS -> SoA on the host (all cores) into pinned staging, one copy, then device views
     // (data_gpu.cu:5-52).  The staging buffers alternate: this one was last read by the copy two
     // uploads ago, which is all the host waits for.
@@ -410,6 +417,7 @@ arc_status arc_lbvh_get_view(const arc_lbvh* bvh, ArcLbvhView* out) {
 arc_status arc_lbvh_reference_views(arc_lbvh* bvh, ArcBvhParam* bvh_param, ArcAvplBvhNodeDataParam* node_data) {
     ARC_CHECK_ARG(bvh && bvh_param && node_data, "NULL argument");
     ARC_CHECK_ARG(bvh->n >= 2, "LBVH not built");
+    ARC_TRY_CUDA(cudaSetDevice(bvh->ctx->device));
     if (!bvh->has_reference_nodes) ARC_TRY(launch_lbvh_reference_nodes(bvh));
     *bvh_param = bvh->ref_param;
     *node_data = bvh->ref_data;
@@ -426,6 +434,7 @@ arc_status arc_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvplsG
 
 arc_status arc_last_cut(arc_context* ctx, ArcCutLists* out) {
     ARC_CHECK_ARG(ctx && out, "NULL argument");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     const CutPool& p = ctx->last_cut.pool;
     int32_t used = 0;
     if (p.next) {

@@ -64,6 +64,7 @@ extern "C" arc_status arc_batch_create(arc_context* ctx, arc_batch** out) {
 
 extern "C" arc_status arc_batch_destroy(arc_batch* b) {
     if (!b) return ARC_OK;
+    if (b->ctx) cudaSetDevice(b->ctx->device);
     if (b->ctx && b->ctx->stream) cudaStreamSynchronize(b->ctx->stream);
     release_graph(b);
     if (b->bvh) arc_lbvh_destroy(b->bvh);

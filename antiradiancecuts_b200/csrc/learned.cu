@@ -920,6 +920,7 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     ARC_CHECK_ARG(ctx && bvh && gb && gp && cp && features_bf16 && labels && errors && count, "NULL argument");
     ARC_CHECK_ARG(bvh->n >= 2, "LBVH not built");
     ARC_CHECK_ARG(gp->ar_kind >= 0 && gp->ar_kind <= 2, "ar_kind out of range");
+    ARC_TRY_CUDA(cudaSetDevice(ctx->device));
     (void)camera_position;
     cudaStream_t st = ctx->stream;
     const int W = gb->width, H = gb->height;

@@ -446,24 +446,18 @@ arc_status mlp_launch(arc_mlp* m, bool train, const void* x, int64_t rows, float
     a.err = ctx->d_error;
     const int64_t tiles = (rows + mlp::kRows - 1) / mlp::kRows;
     if (tiles == 0) return ARC_OK;
+    // the shared-memory limit is a per-device attribute of the kernel: set it on every call (a
+    // host-side call), not once per process, so contexts on other devices get it too
     if (train) {
-        static bool attr = false;
-        if (!attr) {
-            ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)mlp::kSmemTrain));
-            attr = true;
-        }
+        ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)mlp::kSmemTrain));
         const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
         stage_begin(ctx, "mlp_train");
         mlp::mlp_train_kernel<<<grid, 128, mlp::kSmemTrain, ctx->stream>>>(a);
         stage_end(ctx, 1);
     } else {
-        static bool attr = false;
-        if (!attr) {
-            ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)mlp::kSmemInfer));
-            attr = true;
-        }
+        ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)mlp::kSmemInfer));
         const int grid = (int)std::min<int64_t>(tiles, (int64_t)ctx->sm_count * 4);
         stage_begin(ctx, "mlp_forward");
         mlp::mlp_infer_kernel<<<grid, 128, mlp::kSmemInfer, ctx->stream>>>(a);
@@ -519,17 +513,25 @@ arc_status arc_mlp_create(arc_context* ctx, uint64_t seed, arc_mlp** out) {
     fill(mlp::oB3, 64, 64);
     fill(mlp::oW4, 64, 64);
     fill(mlp::oB4, 1, 64);
-    ARC_TRY_CUDA(cudaMemcpy(m->params, p.data(), bytes, cudaMemcpyHostToDevice));
-    ARC_TRY_CUDA(cudaMemset(m->grads, 0, bytes));
-    ARC_TRY_CUDA(cudaMemset(m->adam_m, 0, bytes));
-    ARC_TRY_CUDA(cudaMemset(m->adam_v, 0, bytes));
+    e = cudaMemcpy(m->params, p.data(), bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(m->grads, 0, bytes);
+    if (e == cudaSuccess) e = cudaMemset(m->adam_m, 0, bytes);
+    if (e == cudaSuccess) e = cudaMemset(m->adam_v, 0, bytes);
+    if (e != cudaSuccess) {
+        set_last_error(std::string("arc_mlp_create: ") + cudaGetErrorString(e));
+        arc_mlp_destroy(m);
+        return ARC_ERR_CUDA;
+    }
     *out = m;
     return ARC_OK;
 }
 
 arc_status arc_mlp_destroy(arc_mlp* m) {
     if (!m) return ARC_OK;
-    if (m->ctx) cudaStreamSynchronize(m->ctx->stream);
+    if (m->ctx) {
+        cudaSetDevice(m->ctx->device);
+        cudaStreamSynchronize(m->ctx->stream);
+    }
     cudaFree(m->params);
     cudaFree(m->grads);
     cudaFree(m->adam_m);
@@ -541,6 +543,7 @@ arc_status arc_mlp_destroy(arc_mlp* m) {
 
 arc_status arc_mlp_set_params(arc_mlp* m, const float* host, int32_t n) {
     ARC_CHECK_ARG(m && host && n == mlp::kParams, "parameter count mismatch");
+    ARC_TRY_CUDA(cudaSetDevice(m->ctx->device));
     ARC_TRY_CUDA(cudaMemcpyAsync(m->params, host, sizeof(float) * n, cudaMemcpyHostToDevice, m->ctx->stream));
     ARC_TRY_CUDA(cudaStreamSynchronize(m->ctx->stream));
     return ARC_OK;
@@ -548,6 +551,7 @@ arc_status arc_mlp_set_params(arc_mlp* m, const float* host, int32_t n) {
 
 arc_status arc_mlp_get_params(arc_mlp* m, float* host, int32_t n) {
     ARC_CHECK_ARG(m && host && n == mlp::kParams, "parameter count mismatch");
+    ARC_TRY_CUDA(cudaSetDevice(m->ctx->device));
     ARC_TRY_CUDA(cudaMemcpyAsync(host, m->params, sizeof(float) * n, cudaMemcpyDeviceToHost, m->ctx->stream));
     ARC_TRY_CUDA(cudaStreamSynchronize(m->ctx->stream));
     return ARC_OK;
@@ -556,12 +560,14 @@ arc_status arc_mlp_get_params(arc_mlp* m, float* host, int32_t n) {
 arc_status arc_mlp_forward(arc_mlp* m, const void* features_bf16, int64_t rows, float* logits) {
     ARC_CHECK_ARG(m && (rows == 0 || (features_bf16 && logits)), "NULL argument");
     ARC_CHECK_ARG(reinterpret_cast<uintptr_t>(features_bf16) % 16 == 0, "features must be 16-byte aligned");
+    ARC_TRY_CUDA(cudaSetDevice(m->ctx->device));
     return mlp_launch(m, false, features_bf16, rows, logits, nullptr, nullptr, 0.0f);
 }
 
 arc_status arc_mlp_gradients(arc_mlp* m, const void* features_bf16, const float* labels, const float* weights,
                              int64_t rows, float weight_sum, float* host_grads, float* host_loss) {
     ARC_CHECK_ARG(m && features_bf16 && labels && rows > 0 && weight_sum > 0.0f, "bad argument");
+    ARC_TRY_CUDA(cudaSetDevice(m->ctx->device));
     ARC_TRY_CUDA(cudaMemsetAsync(m->grads, 0, sizeof(float) * mlp::kParams, m->ctx->stream));
     ARC_TRY_CUDA(cudaMemsetAsync(m->loss, 0, sizeof(float), m->ctx->stream));
     ARC_TRY(mlp_launch(m, true, features_bf16, rows, nullptr, labels, weights, 1.0f / weight_sum));
@@ -586,6 +592,7 @@ int32_t arc_mlp_get_loss(const arc_mlp* m) { return m ? m->loss_kind : -1; }
 arc_status arc_mlp_train_step(arc_mlp* m, const void* features_bf16, const float* labels, const float* weights,
                               int64_t rows, float weight_sum, float lr, float* device_loss_accum) {
     ARC_CHECK_ARG(m && features_bf16 && labels && rows > 0 && weight_sum > 0.0f, "bad argument");
+    ARC_TRY_CUDA(cudaSetDevice(m->ctx->device));
     float* saved = m->loss;
     if (device_loss_accum) m->loss = device_loss_accum;
     arc_status s = mlp_launch(m, true, features_bf16, rows, nullptr, labels, weights, 1.0f / weight_sum);
