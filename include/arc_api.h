@@ -153,7 +153,15 @@ const char* arc_status_string(int32_t status);
 /* Message of the last failing call on this host thread ("" if none). */
 const char* arc_last_error(void);
 
-/* cuda_stream: a cudaStream_t to run on, or NULL to let the context create its own. */
+/* Threading and ownership.  A context owns one stream, one device arena and its device error
+ * word; the trees (arc_lbvh), networks (arc_mlp) and batches (arc_batch) created from it share
+ * them.  A context and its objects are not thread-safe: use them from one host thread at a time.
+ * Distinct contexts share no mutable state and may be used from different threads at once, on
+ * the same or different devices.  Every call on a context selects the context's device first.
+ * Inputs and outputs (device arrays, G-buffer and output planes) belong to the caller; the
+ * library allocates only its own scratch, from the context's grow-only arena.
+ *
+ * cuda_stream: a cudaStream_t to run on, or NULL to let the context create its own. */
 arc_status arc_context_create(int32_t device, void* cuda_stream, arc_context** out);
 arc_status arc_context_destroy(arc_context* ctx);
 /* Waits for the context's stream; returns and clears the device error word. */
