@@ -402,6 +402,11 @@ def main():
     from antiradiancecuts_b200 import api, scene
 
     world, rank, local = dist_init()
+    if world > 1:
+        # replicas: the extra legs (exact and FP64 gathers, analytic cut, batch, scene, post,
+        # clustered) repeat one GPU's measurements on every rank, and the CPU baseline belongs to
+        # the single-GPU run, where no other rank loads the host cores
+        args.no_extras = True
     torch.cuda.set_device(local)
     ctx = api.Context(local)
     lib = ctx.lib
