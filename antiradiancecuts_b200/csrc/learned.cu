@@ -305,6 +305,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     __syncthreads();
     tc::fence_after_sync();
     bool ok = __syncthreads_and(mbar_wait_bounded(&wbar, 0, a.err)) != 0;
+    bool mma_gave_up = false;  // a tensor-core wait gave up: its commit may still be in flight
     mlp::InferCta c{smem_u32(sm), fW, fH, sm, vec, tmem_base, &bar, 0u, a.err};
     unsigned long long scored = 0;
     // The next chunk's index and entries are fetched one chunk ahead, so that neither the work
@@ -392,6 +393,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
             float y = 0.0f;
             if (!mlp::infer_tiles<kLevelTiles>(c, fX, t, &y)) {
                 ok = false;
+                mma_gave_up = true;
                 break;
             }
             scored += n_rows;
@@ -416,6 +418,13 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
         if (!ok || done) break;
     }
     if (t == 0 && scored) atomicAdd(a.rows_scored, scored);
+    if (!ok && t == 0) {
+        // a bounded wait gave up (the error word says so): before this CTA's shared memory and
+        // TMEM are released, give its weight copy and its last tensor-core commit a second
+        // bounded wait (the failed wait has already flipped the phase)
+        mbar_wait_bounded(&wbar, 0, a.err);
+        if (mma_gave_up) mbar_wait_bounded(&bar, c.phase ^ 1u, a.err);
+    }
     tc::fence_before_sync();
     __syncthreads();
     if (w == 0) tc::dealloc(tmem_base, kLevelTmemCols);

@@ -135,7 +135,12 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(Args a) {
         *reinterpret_cast<uint4*>(sm + sInX + tc::kmajor_offset(t, 0, kIn)) = x0;
         *reinterpret_cast<uint4*>(sm + sInX + tc::kmajor_offset(t, 8, kIn)) = x1;
         float y;
-        if (!infer_tile(c, sInX, t, &y)) break;
+        if (!infer_tile(c, sInX, t, &y)) {
+            // the wait gave up (the error word says so): its commit gets a second bounded wait
+            // before the TMEM and shared memory are released (the failed wait flipped the phase)
+            if (t == 0) mbar_wait_bounded(&bar, c.phase ^ 1u, a.err);
+            break;
+        }
         if (valid) a.logits[row] = y;
     }
     tc::fence_before_sync();
@@ -193,6 +198,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
     const uint32_t base = smem_u32(sm);
     uint32_t phase = 0;
     bool any_tile = false;
+    bool gave_up = false;  // a tensor-core wait gave up: its commit may still be in flight
 
     constexpr uint32_t idKK64 = tc::idesc_bf16(128, 64, false, false);
     constexpr uint32_t idKM64 = tc::idesc_bf16(128, 64, false, true);
@@ -204,7 +210,9 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         const bool ok = mbar_wait_bounded(&bar, phase, a.err);
         phase ^= 1u;
         tc::fence_after_sync();
-        return __syncthreads_and(ok) != 0;
+        const bool all = __syncthreads_and(ok) != 0;
+        if (!all) gave_up = true;
+        return all;
     };
     // make this thread's generic-proxy smem writes visible to the tensor cores, then barrier
     auto publish_smem = [&]() {
@@ -367,7 +375,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         any_tile = true;
     }
 
-    if (any_tile) {
+    if (any_tile && !gave_up) {
         // weight gradients: D rows 0..63 (= output features) live in TMEM lanes 0..63
         if (w < 2) {
             float v[64];
@@ -390,6 +398,9 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         }
         if (t == 0) atomicAdd(&a.grads[oB4], gb4[0]);
     }
+    // after a wait that gave up (the error word says so), the last commit gets a second bounded
+    // wait before the TMEM and shared memory are released (the failed wait flipped the phase)
+    if (gave_up && t == 0) mbar_wait_bounded(&bar, phase ^ 1u, a.err);
     tc::fence_before_sync();
     __syncthreads();
     if (w == 0) tc::dealloc(tmem, kCols);
