@@ -182,3 +182,33 @@ int main(int argc, char** argv) {
     words = r.stdout.split()
     assert words[1:3] == ["1", "0"]
     assert out_file.read_bytes().startswith(b"PF\n2 2\n-1.0\n")
+
+
+def test_cpp_host_compiles_warning_free_and_links(tmp_path):
+    """The reference's host is C++: the header compiles as C++17 with every warning an error, its
+    declarations have C linkage (the link resolves them in libarc.so), and a null context is
+    rejected with ARC_ERR_INVALID_ARG before any CUDA call."""
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "antiradiancecuts_b200")
+    src = tmp_path / "host.cpp"
+    src.write_text(r"""
+#include <cstdio>
+#include <vector>
+#include "arc_api.h"
+int main() {
+    ArcGatherParams gp;
+    arc_gather_params_default(&gp);
+    std::vector<ArcMaterial> mats(2);
+    const arc_status s = arc_materials_upload(nullptr, mats.data(), (int32_t)mats.size());
+    std::printf("%s %d %d\n", arc_status_string(s), gp.ar_kind, arc_mlp_num_params());
+    return s == ARC_ERR_INVALID_ARG ? 0 : 1;
+}
+""")
+    exe = tmp_path / "host"
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(root, "include"), str(src),
+                    "-L", libdir, "-larc", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], check=True, capture_output=True, text=True)
+    assert r.stdout.split() == ["ARC_ERR_INVALID_ARG", str(L.ARC_AR_CONE), "9473"]
