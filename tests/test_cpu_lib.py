@@ -81,6 +81,31 @@ def test_null_arguments_are_rejected():
     assert b"NULL" in lib.arc_last_error() or b"out" in lib.arc_last_error()
 
 
+def test_every_entry_point_rejects_null_handles_before_any_cuda_call():
+    """Every arc_status entry point of the header, called with NULL pointers and zero sizes, returns
+    ARC_ERR_INVALID_ARG (the destroy functions accept NULL as a no-op) without touching CUDA: this
+    machine has no GPU, so a CUDA call would have answered ARC_ERR_CUDA."""
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "arc_api.h")).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\barc_status\s+(arc_[a-z0-9_]+)\s*\(", hdr)))
+    assert len(names) >= 45
+    lib = L.load()
+    for name in names:
+        _, argtypes = L.SIGNATURES[name]
+        vals = []
+        for a in argtypes:
+            if isinstance(a, type) and issubclass(a, C.Structure):
+                vals.append(a())
+            elif a in (C.c_float, C.c_double):
+                vals.append(0.0)
+            elif a in (C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_size_t):
+                vals.append(0)
+            else:
+                vals.append(None)
+        got = getattr(lib, name)(*vals)
+        want = L.ARC_OK if name.endswith("_destroy") else L.ARC_ERR_INVALID_ARG
+        assert got == want, (name, L.status_string(got), lib.arc_last_error())
+
+
 def test_scene_generator_is_deterministic():
     d = scene.scene_desc(L.ARC_SCENE_ROOM_2BOXES, 2)
     a1, p1 = scene.trace_avpls(d, 2, 5000, 3)
