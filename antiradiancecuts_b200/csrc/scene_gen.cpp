@@ -9,11 +9,21 @@
 
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
+
+namespace arc {
+void set_last_error(const std::string& msg);  // api.cu: the thread's arc_last_error() message
+}
 
 using namespace arc::scene;
 
 namespace {
+
+arc_status invalid(const char* msg) {
+    arc::set_last_error(msg);
+    return ARC_ERR_INVALID_ARG;
+}
 
 ArcMaterial lambert(float r, float g, float b) {
     ArcMaterial m;
@@ -26,9 +36,10 @@ ArcMaterial lambert(float r, float g, float b) {
 }  // namespace
 
 extern "C" arc_status arc_scene_preset_desc(int32_t preset, uint64_t seed, int32_t num_boxes, ArcSceneDesc* out) {
-    if (!out || preset < 0 || preset > ARC_SCENE_TRAIN_VARIANT || num_boxes < 0 ||
-        num_boxes > ARC_SCENE_MAX_BOXES - 2)
-        return ARC_ERR_INVALID_ARG;
+    if (!out) return invalid("arc_scene_preset_desc: out is NULL");
+    if (preset < 0 || preset > ARC_SCENE_TRAIN_VARIANT) return invalid("arc_scene_preset_desc: unknown preset");
+    if (num_boxes < 0 || num_boxes > ARC_SCENE_MAX_BOXES - 2)
+        return invalid("arc_scene_preset_desc: num_boxes must be in [0, ARC_SCENE_MAX_BOXES - 2]");
     ArcSceneDesc& s = *out;
     std::memset(&s, 0, sizeof(s));
     // material 0: no surface; 1 gray; 2 red; 3 green; 4 light (black, emissive)
@@ -87,7 +98,8 @@ extern "C" arc_status arc_scene_preset_desc(int32_t preset, uint64_t seed, int32
 extern "C" arc_status arc_scene_trace_avpls(const ArcSceneDesc* scene, uint64_t seed, int32_t max_bounces,
                                             int32_t explicit_direct_illum, int32_t num_avpls, ArcAvplHost* out,
                                             int64_t* num_paths) {
-    if (!scene || !out || num_avpls < 0 || max_bounces < 1) return ARC_ERR_INVALID_ARG;
+    if (!scene || !out) return invalid("arc_scene_trace_avpls: NULL argument");
+    if (num_avpls < 0 || max_bounces < 1) return invalid("arc_scene_trace_avpls: num_avpls < 0 or max_bounces < 1");
     Rect rects[kMaxRects];
     const int nrects = build_rects(*scene, rects);
     // Paths are independent (one PCG32 stream each), so batches of paths are traced in
@@ -111,7 +123,8 @@ extern "C" arc_status arc_scene_trace_avpls(const ArcSceneDesc* scene, uint64_t 
             if (produced >= num_avpls && num_paths) *num_paths = path0 + i + 1;
         }
         path0 += batch;
-        if (path0 > (int64_t)num_avpls * 1000 + 100000) return ARC_ERR_INVALID_ARG;  // light sees nothing
+        if (path0 > (int64_t)num_avpls * 1000 + 100000)
+            return invalid("arc_scene_trace_avpls: the light paths make no indirect AVPLs (light sees nothing)");
     }
     if (num_avpls == 0 && num_paths) *num_paths = 0;
     return ARC_OK;
@@ -119,7 +132,8 @@ extern "C" arc_status arc_scene_trace_avpls(const ArcSceneDesc* scene, uint64_t 
 
 extern "C" arc_status arc_scene_gbuffer(const ArcSceneDesc* scene, int32_t width, int32_t height, float* position,
                                         float* normal) {
-    if (!scene || !position || !normal || width <= 0 || height <= 0) return ARC_ERR_INVALID_ARG;
+    if (!scene || !position || !normal) return invalid("arc_scene_gbuffer: NULL argument");
+    if (width <= 0 || height <= 0) return invalid("arc_scene_gbuffer: width and height must be positive");
     Rect rects[kMaxRects];
     const int nrects = build_rects(*scene, rects);
     const Camera cam = make_camera(*scene, width, height);
@@ -133,7 +147,8 @@ extern "C" arc_status arc_scene_gbuffer(const ArcSceneDesc* scene, int32_t width
 
 extern "C" arc_status arc_scene_batch_views(const ArcSceneDesc* scene, uint64_t seed, int32_t count,
                                             ArcBatchViewDesc* out) {
-    if (!scene || !out || count < 0) return ARC_ERR_INVALID_ARG;
+    if (!scene || !out) return invalid("arc_scene_batch_views: NULL argument");
+    if (count < 0) return invalid("arc_scene_batch_views: negative count");
     static const int32_t kRes[4][2] = {{256, 256}, {512, 512}, {1280, 720}, {1920, 1080}};
     arc_pcg32 rng;
     arc_pcg32_seed(&rng, seed, 0);

@@ -83,8 +83,9 @@ def test_null_arguments_are_rejected():
 
 def test_every_entry_point_rejects_null_handles_before_any_cuda_call():
     """Every arc_status entry point of the header, called with NULL pointers and zero sizes, returns
-    ARC_ERR_INVALID_ARG (the destroy functions accept NULL as a no-op) without touching CUDA: this
-    machine has no GPU, so a CUDA call would have answered ARC_ERR_CUDA."""
+    ARC_ERR_INVALID_ARG (the destroy functions accept NULL as a no-op) without touching CUDA (this
+    machine has no GPU, so a CUDA call would have answered ARC_ERR_CUDA), and sets its own
+    arc_last_error() message."""
     hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "arc_api.h")).read(), flags=re.S)
     names = sorted(set(re.findall(r"\barc_status\s+(arc_[a-z0-9_]+)\s*\(", hdr)))
     assert len(names) >= 45
@@ -101,9 +102,13 @@ def test_every_entry_point_rejects_null_handles_before_any_cuda_call():
                 vals.append(0)
             else:
                 vals.append(None)
+        lib.arc_context_create(0, None, None)  # leaves the message "out is NULL"
+        marker = lib.arc_last_error()
         got = getattr(lib, name)(*vals)
         want = L.ARC_OK if name.endswith("_destroy") else L.ARC_ERR_INVALID_ARG
         assert got == want, (name, L.status_string(got), lib.arc_last_error())
+        if got != L.ARC_OK and name != "arc_context_create":
+            assert lib.arc_last_error() != marker, f"{name} failed without setting its own message"
 
 
 def test_scene_generator_is_deterministic():
