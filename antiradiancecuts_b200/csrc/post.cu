@@ -9,8 +9,11 @@
 // normalised planes are rounded to float once.  The error sums the clamped squared differences in
 // FP64 in a fixed order (the reference sums in FP32 in pixel order).
 #include <algorithm>
+#include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <string>
 #include <vector>
 
 #include "arc_internal.h"
@@ -210,11 +213,21 @@ extern "C" arc_status arc_image_error(arc_context* ctx, const float* reference, 
     return ARC_OK;
 }
 
+namespace {
+
+// ARC_ERR_IO with the failing step, the path and the C library's reason as the thread's message
+arc_status io_error(const char* what, const char* path) {
+    arc::set_last_error(std::string(what) + " " + path + ": " + std::strerror(errno));
+    return ARC_ERR_IO;
+}
+
+}  // namespace
+
 extern "C" arc_status arc_export_pfm(const char* path, const float* rgba, int32_t width, int32_t height,
                                      int64_t pitch) {
     ARC_CHECK_ARG(path && rgba && width > 0 && height > 0 && pitch >= width, "bad argument");
     FILE* f = std::fopen(path, "wb");
-    if (!f) return ARC_ERR_IO;
+    if (!f) return io_error("arc_export_pfm: cannot open", path);
     // little-endian (scale -1), rows bottom to top; this plane's row 0 is the top of the image
     std::fprintf(f, "PF\n%d %d\n-1.0\n", width, height);
     std::vector<float> row(3 * (size_t)width);
@@ -226,14 +239,14 @@ extern "C" arc_status arc_export_pfm(const char* path, const float* rgba, int32_
         ok = std::fwrite(row.data(), sizeof(float), row.size(), f) == row.size();
     }
     ok = (std::fclose(f) == 0) && ok;
-    return ok ? ARC_OK : ARC_ERR_IO;
+    return ok ? ARC_OK : io_error("export: cannot write", path);
 }
 
 extern "C" arc_status arc_export_hdr(const char* path, const float* rgba, int32_t width, int32_t height,
                                      int64_t pitch) {
     ARC_CHECK_ARG(path && rgba && width > 0 && height > 0 && pitch >= width, "bad argument");
     FILE* f = std::fopen(path, "wb");
-    if (!f) return ARC_ERR_IO;
+    if (!f) return io_error("arc_export_hdr: cannot open", path);
     std::fprintf(f, "#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y %d +X %d\n", height, width);
     std::vector<unsigned char> px(4 * (size_t)width), out;
     const bool rle = width >= 8 && width <= 0x7fff;  // the run-length scanline format's range
@@ -260,5 +273,5 @@ extern "C" arc_status arc_export_hdr(const char* path, const float* rgba, int32_
         ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
     }
     ok = (std::fclose(f) == 0) && ok;
-    return ok ? ARC_OK : ARC_ERR_IO;
+    return ok ? ARC_OK : io_error("export: cannot write", path);
 }

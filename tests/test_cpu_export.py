@@ -44,8 +44,12 @@ def test_hdr_round_trip(tmp_path, shape):
 def test_export_reports_unwritable_path(tmp_path):
     a = _plane(4, 4, 0)
     lib = L.load()
-    st = lib.arc_export_pfm(str(tmp_path / "missing" / "x.pfm").encode(), a.ctypes.data, 4, 4, 4)
-    assert st == L.ARC_ERR_IO
+    for fn in (lib.arc_export_pfm, lib.arc_export_hdr):
+        bad = str(tmp_path / "missing" / "x.out")
+        st = fn(bad.encode(), a.ctypes.data, 4, 4, 4)
+        assert st == L.ARC_ERR_IO
+        msg = lib.arc_last_error().decode()
+        assert "cannot open" in msg and bad in msg and "No such file" in msg
 
 
 def test_reference_error_formula():
