@@ -155,7 +155,8 @@ const char* arc_last_error(void);
 
 /* Threading and ownership.  A context owns one stream, one device arena and its device error
  * word; the trees (arc_lbvh), networks (arc_mlp) and batches (arc_batch) created from it share
- * them.  A context and its objects are not thread-safe: use them from one host thread at a time.
+ * them, so destroy them before the context.  A context and its objects are not thread-safe: use
+ * them from one host thread at a time.
  * Distinct contexts share no mutable state and may be used from different threads at once, on
  * the same or different devices.  Every call on a context selects the context's device first.
  * Inputs and outputs (device arrays, G-buffer and output planes) belong to the caller; the
