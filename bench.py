@@ -155,19 +155,23 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
     prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
     H, W = pos.shape[:2]
     valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
-    rng = np.random.default_rng(7)
-    t0 = time.perf_counter()
-    probe = rng.choice(valid, size=min(len(valid), 4 * threads), replace=False)
-    O.gather_fp32(pos, nrm, probe, avpls, dif, spe, ex, cam, prm, threads=threads)
-    dt = max(time.perf_counter() - t0, 1e-3)
-    k = int(min(len(valid), max(4 * threads, len(probe) * target_s / dt)))
-    sample = rng.choice(valid, size=k, replace=False)
-    t0 = time.perf_counter()
-    O.gather_fp32(pos, nrm, sample, avpls, dif, spe, ex, cam, prm, threads=threads)
-    dt = time.perf_counter() - t0
+    order = np.random.default_rng(7).permutation(valid)
+    # chunks of a seeded pixel permutation until target_s of gather time is spent (or every surface
+    # pixel is done); each chunk is sized from the rate measured so far, aiming at a quarter of the
+    # remaining time
+    k, dt, chunk = 0, 0.0, 4 * threads
+    while k < len(order) and dt < target_s:
+        part = order[k:k + chunk]
+        t0 = time.perf_counter()
+        O.gather_fp32(pos, nrm, part, avpls, dif, spe, ex, cam, prm, threads=threads)
+        dt += time.perf_counter() - t0
+        k += len(part)
+        rate = k / max(dt, 1e-6)
+        chunk = int(max(4 * threads, min(4 * chunk, rate * max(target_s - dt, 0.0) / 4)))
     # every pixel costs the same (all AVPLs); background pixels cost nothing, so extrapolate over
     # the valid pixels
-    ms_frame = dt * 1e3 * len(valid) / k
+    ms_frame = dt * 1e3 * len(valid) / max(k, 1)
+    sample = order[:k]
     check = None
     if ref64 is not None:
         px = sample[:64]
