@@ -93,7 +93,7 @@ class ArcGatherParams(C.Structure):
 
 class ArcLbvhParams(C.Structure):
     _fields_ = [("consider_normals", C.c_int32), ("bbox_mode", C.c_int32), ("scene_min", ArcFloat3),
-                ("scene_max", ArcFloat3), ("repr_seed", C.c_uint32)]
+                ("scene_max", ArcFloat3), ("repr_seed", C.c_uint32), ("wait_limit", C.c_uint32)]
 
 
 class ArcBvhNode(C.Structure):
@@ -214,7 +214,7 @@ SIGNATURES = {
     "arc_mlp_set_loss": (_st, [_vp, C.c_int32]),
     "arc_mlp_get_loss": (C.c_int32, [_vp]),
     "arc_cut_training_samples": (_st, [_vp, _vp, P(ArcGBufferView), ArcFloat3, P(ArcGatherParams), P(ArcCutParams),
-                                       C.c_float, _vp, _vp, _vp, C.c_int32, P(C.c_int32)]),
+                                       C.c_float, _vp, _vp, _vp, _vp, C.c_int32, P(C.c_int32)]),
     "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),
                       P(ArcOutputView)]),
     "arc_scene_preset_desc": (_st, [C.c_int32, C.c_uint64, C.c_int32, P(ArcSceneDesc)]),
@@ -270,6 +270,22 @@ def load() -> C.CDLL:
         fn.restype = res
         fn.argtypes = args
     _lib = lib
+    return lib
+
+
+SCENE_SYMBOLS = ("arc_scene_preset_desc", "arc_scene_trace_avpls", "arc_scene_gbuffer", "arc_scene_batch_views")
+
+
+def load_scene_library(path: str) -> C.CDLL:
+    """A library that exports only the CPU scene generator's entry points (arc_scene_* and
+    arc_last_error), with their signatures declared: the generator's source compiled on its own,
+    for a process that must make the synthetic inputs without loading libarc."""
+    lib = C.CDLL(path)
+    for name in SCENE_SYMBOLS + ("arc_last_error",):
+        res, args = SIGNATURES[name]
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
     return lib
 
 

@@ -157,13 +157,14 @@ class AvplBvh:
         ctx._children.add(self)
 
     def build(self, avpls: L.ArcAvplsGpuParam, consider_normals=False, bbox_mode=L.ARC_BBOX_SCENE,
-              scene_min=(0, 0, 0), scene_max=(1, 1, 1), repr_seed=None) -> None:
+              scene_min=(0, 0, 0), scene_max=(1, 1, 1), repr_seed=None, wait_limit=0) -> None:
         p = L.ArcLbvhParams()
         self.ctx.lib.arc_lbvh_params_default(C.byref(p))
         p.consider_normals = int(consider_normals)
         p.bbox_mode = bbox_mode
         p.scene_min = L.f3(scene_min)
         p.scene_max = L.f3(scene_max)
+        p.wait_limit = int(wait_limit)
         if repr_seed is not None:
             p.repr_seed = repr_seed
         L.check(self.ctx.lib.arc_lbvh_build(self.handle, C.byref(avpls), C.byref(p)), "arc_lbvh_build")

@@ -97,6 +97,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// A CTA whose bounded wait on its ring of `stages` bulk-copy buffers gave up at chunk `fail_c`
+// may still have the copies of chunks fail_c .. fail_c + stages - 1 in flight (the issuing thread
+// refills a buffer only after its own wait succeeded).  The issuing thread calls this before the
+// CTA exits, so that no copy still writes shared memory that the next CTA on the SM may own: one
+// more bounded wait per such copy (the phase a copy completes is the one its chunk waits for).
+__device__ __forceinline__ void drain_ring_bounded(uint64_t* bars, int stages, int fail_c, int nchunks,
+                                                   uint32_t* err) {
+    for (int c = fail_c; c < fail_c + stages && c < nchunks; ++c)
+        mbar_wait_bounded(&bars[c % stages], (uint32_t)((c / stages) & 1), err);
+}
+
 // Packed FP32 pairs (sm_100 f32x2 instructions: two IEEE round-to-nearest operations each, the
 // same results as the scalar forms).
 __device__ __forceinline__ uint64_t f2(float lo, float hi) {

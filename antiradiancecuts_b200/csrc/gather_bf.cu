@@ -188,10 +188,14 @@ __global__ void __launch_bounds__(kThreads) gather_bf_kernel(BfArgs k) {
     }
 
     bool ok = true;
+    int fail_c = -1;  // first chunk whose wait gave up
     for (int c = 0; c < nchunks; ++c) {
         const int s = c % kStages;
         const uint32_t parity = (uint32_t)((c / kStages) & 1);
-        if (ok) ok = mbar_wait_bounded(&bars[s], parity, k.err);
+        if (ok) {
+            ok = mbar_wait_bounded(&bars[s], parity, k.err);
+            if (!ok) fail_c = c;
+        }
         if (ok) {
             const int cnt = min(k.chunk, k.n - c * k.chunk);
             const float4* rec = stage + (size_t)s * k.chunk * 4;
@@ -250,6 +254,8 @@ __global__ void __launch_bounds__(kThreads) gather_bf_kernel(BfArgs k) {
                      &bars[s]);
         }
     }
+    // the copies the ring still has in flight after a wait gave up (only thread 0 issues them)
+    if (tid == 0 && fail_c >= 0) drain_ring_bounded(bars, kStages, fail_c, nchunks, k.err);
 
     // epilogue: receiver BRDF, signed combine, stores
 #pragma unroll
@@ -436,10 +442,14 @@ __global__ void __launch_bounds__(kThreads) gather_bf_packed_kernel(BfArgs k) {
     const uint64_t kTiny2 = f2(1e-30f, 1e-30f);
 
     bool ok = true;
+    int fail_c = -1;  // first chunk whose wait gave up
     for (int c = 0; c < nchunks; ++c) {
         const int s = c % kStages;
         const uint32_t parity = (uint32_t)((c / kStages) & 1);
-        if (ok) ok = mbar_wait_bounded(&bars[s], parity, k.err);
+        if (ok) {
+            ok = mbar_wait_bounded(&bars[s], parity, k.err);
+            if (!ok) fail_c = c;
+        }
         if (ok) {
             const int pairs = min(k.chunk, npad - c * k.chunk) >> 1;
             const float* st = stage + (size_t)s * k.chunk * 16;
@@ -504,6 +514,8 @@ __global__ void __launch_bounds__(kThreads) gather_bf_packed_kernel(BfArgs k) {
                      &bars[s]);
         }
     }
+    // the copies the ring still has in flight after a wait gave up (only thread 0 issues them)
+    if (tid == 0 && fail_c >= 0) drain_ring_bounded(bars, kStages, fail_c, nchunks, k.err);
 
     // epilogue: receiver BRDF, FP64 signed combine, stores
 #pragma unroll
@@ -941,23 +953,59 @@ namespace {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
+// per device: the context the address was looked up in, and the address
+void* g_noalloc_ctx[kNoAllocMaxDevices] = {};
 unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device with that
-// device current.  The host-side name g_noalloc_scratch is only a stand-in for the symbol and
-// must never be handed to a kernel.
+using CtxGetCurrentFn = int (*)(void**);  // cuCtxGetCurrent(CUcontext*) -> CUresult
+
+// The driver context current on this thread (NULL if the driver entry point is unavailable).
+void* current_driver_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    void* c = nullptr;
+    if (fn && fn(&c) != 0) c = nullptr;
+    return c;
+}
+
+// Device address of g_noalloc_scratch in the current device's context, looked up with that
+// device current the first time a call runs in that context (again after a device reset or in
+// another driver context, where the module is loaded anew at another address).  The host-side
+// name g_noalloc_scratch is only a stand-in for the symbol and must never be handed to a kernel.
 arc_status noalloc_scratch(unsigned char** out) {
     int dev = 0;
     ARC_TRY_CUDA(cudaGetDevice(&dev));
     ARC_CHECK_ARG(dev >= 0 && dev < kNoAllocMaxDevices, "device index beyond the allocation-free path's table");
+    // (NULL before the runtime has made the device's primary context current: looked up then)
+    const void* c = current_driver_context();
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || !c || c != g_noalloc_ctx[dev]) {
         void* p = nullptr;
         ARC_TRY_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+        g_noalloc_ctx[dev] = current_driver_context();  // current now, after the lookup
     }
     *out = g_noalloc_addr[dev];
     return ARC_OK;
+}
+
+// The material table travels as a kernel argument (no host buffer is read after the call
+// returns); the same launch clears the call's error word.
+struct NoAllocMaterials {
+    MaterialRecord rec[ARC_MAX_MATERIALS];
+    int count;
+};
+
+__global__ void noalloc_write_materials(NoAllocMaterials t, MaterialRecord* mats, uint32_t* err) {
+    const int i = threadIdx.x;
+    if (i < t.count) mats[i] = t.rec[i];
+    if (i == 0) *err = 0u;
 }
 
 }  // namespace
@@ -1001,17 +1049,22 @@ extern "C" arc_status arc_gather_bruteforce_noalloc(void* cuda_stream, const Arc
 
     // material table and error word: the scratch keeps the previous call's contents, so both are
     // rewritten here (the records are rewritten by the pack kernel for every AVPL used)
-    MaterialRecord recs[ARC_MAX_MATERIALS];
+    NoAllocMaterials tab;
+    tab.count = num_materials;
     bool spec = false;
     for (int i = 0; i < num_materials; ++i) {
         const ArcMaterial& m = materials[i];
         const float sl = sqrtf(m.specular.x * m.specular.x + m.specular.y * m.specular.y + m.specular.z * m.specular.z);
-        recs[i].diffuse_exp = make_float4(m.diffuse.x, m.diffuse.y, m.diffuse.z, m.exponent);
-        recs[i].specular_flag = make_float4(m.specular.x, m.specular.y, m.specular.z, sl > 0.0f ? 1.0f : 0.0f);
+        tab.rec[i].diffuse_exp = make_float4(m.diffuse.x, m.diffuse.y, m.diffuse.z, m.exponent);
+        tab.rec[i].specular_flag = make_float4(m.specular.x, m.specular.y, m.specular.z, sl > 0.0f ? 1.0f : 0.0f);
         spec = spec || sl > 0.0f;
     }
-    ARC_TRY_CUDA(cudaMemcpyAsync(mats, recs, sizeof(MaterialRecord) * num_materials, cudaMemcpyHostToDevice, st));
-    ARC_TRY_CUDA(cudaMemsetAsync(err, 0, sizeof(uint32_t), st));
+    for (int i = num_materials; i < ARC_MAX_MATERIALS; ++i) {
+        tab.rec[i].diffuse_exp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        tab.rec[i].specular_flag = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    noalloc_write_materials<<<1, ARC_MAX_MATERIALS, 0, st>>>(tab, mats, err);
+    ARC_TRY_CUDA(cudaGetLastError());
 
     BfArgs a{};
     a.n = avpls->numAvpls;

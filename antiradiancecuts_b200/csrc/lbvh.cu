@@ -199,6 +199,9 @@ struct SortPassArgs {
     uint32_t* tile_counter;
     int32_t n;
     int shift;
+    int pass;
+    uint32_t spin_limit;  // polls of the look-back before it gives up
+    uint32_t* abort;      // the build's abort word: 1 + the pass whose look-back gave up, or 0
     uint32_t* err;
 };
 
@@ -207,6 +210,11 @@ __global__ void __launch_bounds__(kSortThreads) lbvh_sort_pass(SortPassArgs s) {
     __shared__ uint32_t tile_off[256];
     __shared__ int tile_sh;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // An earlier pass gave up (its output is not a permutation, so this pass's digit offsets,
+    // counted from the unsorted keys, no longer bound its writes): the build stops here.  CTAs of
+    // the pass that gave up keep going, so that none of its tiles waits on a tile that left.
+    const uint32_t ab = *reinterpret_cast<volatile uint32_t*>(s.abort);
+    if (ab != 0u && ab <= (uint32_t)s.pass) return;
     if (tid == 0) tile_sh = (int)atomicAdd(s.tile_counter, 1u);
     for (int i = tid; i < kSortWarps * 256; i += kSortThreads) (&warp_cnt[0][0])[i] = 0;
     __syncthreads();
@@ -261,8 +269,11 @@ __global__ void __launch_bounds__(kSortThreads) lbvh_sort_pass(SortPassArgs s) {
             while (t >= 0) {
                 const uint32_t v = st[(size_t)t * 256 + d];
                 if ((v & ~kValueMask) == 0) {
-                    if (++spins > (1u << 26)) {
+                    if (++spins > s.spin_limit) {
+                        // publish what was summed: later tiles' offsets stay within the digit's
+                        // range, and the passes after this one do not run
                         set_error(s.err, ARC_DEVERR_TIMEOUT);
+                        atomicMax(s.abort, (uint32_t)s.pass + 1u);
                         break;
                     }
                     continue;
@@ -314,13 +325,14 @@ struct KarrasArgs {
     ArcAvplBvhNodeDataParam nd;
     ArcFloat3* sorted_pos;
     ArcFloat3* sorted_nrm;
+    const uint32_t* abort;  // set when the sort gave up: its order is not a permutation
     uint32_t* err;
 };
 
 __global__ void __launch_bounds__(256) lbvh_karras(KarrasArgs k) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = k.n, num_nodes = n - 1;
-    if (i >= n) return;
+    if (i >= n || *k.abort != 0u) return;
     // ---- inner node i ----
     if (i < num_nodes) {
         const uint32_t* m = k.morton;
@@ -428,6 +440,7 @@ __device__ __forceinline__ float4 cone_union(float4 c1, float4 c2) {
 }
 
 struct BottomUpArgs {
+    const uint32_t* abort;  // set when the sort gave up
     uint32_t* err;
     int32_t n;
     uint32_t seed;
@@ -539,6 +552,7 @@ __global__ void __launch_bounds__(kBottomUpThreads) lbvh_bottom_up(BottomUpArgs 
     const int base = blockIdx.x * kBottomUpThreads;
     const int i = base + threadIdx.x;
     const int n = b.n;
+    if (*b.abort != 0u) return;  // uniform over the CTA: before any barrier below
     if (i >= n) return;
     int parent = b.parents[i];
     // a valid tree reaches the root within n - 1 steps; the bound guards against a corrupt one
@@ -609,8 +623,8 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     ARC_TRY(get(bvh, "keys1", n, &keys1));
     ARC_TRY(get(bvh, "vals0", n, &vals0));
     ARC_TRY(get(bvh, "vals1", n, &vals1));
-    // hist[4*256] | tile counters[4] | bbox[12] share one zeroed block
-    ARC_TRY(get(bvh, "hist", 1024 + 4 + 12, &hist));
+    // hist[4*256] | tile counters[4] | bbox[12] | abort word share one zeroed block
+    ARC_TRY(get(bvh, "hist", 1024 + 4 + 12 + 1, &hist));
     ARC_TRY(get(bvh, "status", (size_t)4 * tiles * 256, &status));
     ARC_TRY(get(bvh, "left", n - 1, &left));
     ARC_TRY(get(bvh, "right", n - 1, &right));
@@ -634,8 +648,10 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     ARC_TRY(get(bvh, "sorted_nrm", n, &bvh->sorted_normals));
     bb = hist + 1024 + 4;
     uint32_t* tile_counters = hist + 1024;
+    uint32_t* abort = hist + 1024 + 4 + 12;
 
     ARC_TRY_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 1028, st));
+    ARC_TRY_CUDA(cudaMemsetAsync(abort, 0, sizeof(uint32_t), st));
     ARC_TRY_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t) * 4 * (size_t)tiles * 256, st));
     ARC_TRY_CUDA(cudaMemsetAsync(visit, 0, sizeof(int32_t) * (size_t)(n - 1), st));
 
@@ -678,6 +694,9 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
         s.tile_counter = tile_counters + pass;
         s.n = n;
         s.shift = 8 * pass;
+        s.pass = pass;
+        s.spin_limit = p->wait_limit ? p->wait_limit : (1u << 26);
+        s.abort = abort;
         s.err = ctx->d_error;
         lbvh_sort_pass<<<tiles, kSortThreads, 0, st>>>(s);
         ARC_TRY_CUDA(cudaGetLastError());
@@ -707,6 +726,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     k.nd = nd;
     k.sorted_pos = bvh->sorted_positions;
     k.sorted_nrm = bvh->sorted_normals;
+    k.abort = abort;
     k.err = ctx->d_error;
     lbvh_karras<<<(n + 255) / 256, 256, 0, st>>>(k);
     stage_end(ctx, 1);
@@ -726,6 +746,7 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     bu.bbox = bbox;
     bu.bounds = bounds;
     bu.nd = nd;
+    bu.abort = abort;
     bu.err = ctx->d_error;
     stage_begin(ctx, "lbvh_bottom_up");
     lbvh_bottom_up<<<(n + kBottomUpThreads - 1) / kBottomUpThreads, kBottomUpThreads, 0, st>>>(bu);
@@ -747,6 +768,19 @@ arc_status launch_lbvh_build(arc_lbvh* bvh, const ArcAvplsGpuParam* avpls, const
     v.node_data = nd;
     v.dirstat = reinterpret_cast<const float*>(dirstat);
     bvh->has_reference_nodes = false;
+    if (p->wait_limit != 0) {
+        // a caller-chosen wait limit: learn now whether the sort gave up, and if it did leave the
+        // object unbuilt (its arrays hold no tree) and report the timeout
+        uint32_t aborted = 0;
+        ARC_TRY_CUDA(cudaMemcpyAsync(&aborted, abort, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        ARC_TRY_CUDA(cudaStreamSynchronize(st));
+        if (aborted) {
+            bvh->n = 0;
+            set_last_error("LBVH build: the radix sort's look-back gave up after " + std::to_string(p->wait_limit) +
+                           " polls (pass " + std::to_string(aborted - 1) + ")");
+            return ARC_ERR_TIMEOUT;
+        }
+    }
     return ARC_OK;
 }
 

@@ -583,6 +583,7 @@ struct LabelArgs {
     __nv_bfloat16* feats;
     float* labels;
     float* errs;
+    int* keys;  // optional: (tile, node) of each sample
     int* count;
     int capacity;
     uint32_t* err;
@@ -759,6 +760,10 @@ __global__ void __launch_bounds__(32) label_traverse(LabelArgs a, const int* ran
                 store_features(a.feats + (size_t)r * kFeat, f);
                 a.labels[r] = refine ? 1.0f : 0.0f;
                 a.errs[r] = Eexact > 0.0f ? erms / Eexact : 0.0f;
+                if (a.keys) {
+                    a.keys[2 * (size_t)r] = tile;
+                    a.keys[2 * (size_t)r + 1] = node;
+                }
             }
         }
         if (extra) continue;
@@ -925,7 +930,8 @@ using namespace arc;
 extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gb,
                                                ArcFloat3 camera_position, const ArcGatherParams* gp,
                                                const ArcCutParams* cp, float delta, void* features_bf16,
-                                               float* labels, float* errors, int32_t capacity, int32_t* count) {
+                                               float* labels, float* errors, int32_t* keys, int32_t capacity,
+                                               int32_t* count) {
     ARC_CHECK_ARG(ctx && bvh && gb && gp && cp && features_bf16 && labels && errors && count, "NULL argument");
     ARC_CHECK_ARG(bvh->n >= 2, "LBVH not built");
     ARC_CHECK_ARG(gp->ar_kind >= 0 && gp->ar_kind <= 2, "ar_kind out of range");
@@ -978,6 +984,7 @@ extern "C" arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh*
     a.feats = static_cast<__nv_bfloat16*>(features_bf16);
     a.labels = labels;
     a.errs = errors;
+    a.keys = keys;
     a.count = dcount;
     a.capacity = capacity;
     a.err = ctx->d_error;

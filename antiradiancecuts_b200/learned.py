@@ -147,7 +147,7 @@ def scene_samples(ctx: api.Context, seed: int, capacity: int, width=TRAIN_W, hei
         L.check(ctx.lib.arc_cut_training_samples(ctx.handle, bvh.handle, C.byref(gv), L.f3(cam), C.byref(prm),
                                                  C.byref(cut), delta, C.c_void_p(feats[o:].data_ptr()),
                                                  C.c_void_p(labels[o:].data_ptr()), C.c_void_p(errs[o:].data_ptr()),
-                                                 capacity - o, C.byref(count)), "arc_cut_training_samples")
+                                                 None, capacity - o, C.byref(count)), "arc_cut_training_samples")
         word = ctx.synchronize()
         if word:
             raise RuntimeError(f"device error word 0x{word:x} while labelling scene {seed}")

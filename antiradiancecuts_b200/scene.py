@@ -1,6 +1,8 @@
 """Seeded synthetic inputs: scene descriptions, AVPL sets and G-buffers as numpy arrays, produced
 by libarc's CPU scene generator (arc_scene_*), plus the named workloads the tests and the
-benchmark run.  These are inputs of the gather, not part of it."""
+benchmark run.  These are inputs of the gather, not part of it.  Every CPU generator function takes
+an optional `lib`: another library that exports the arc_scene_* entry points (the generator's
+source built without the GPU library, see _lib.load_scene_library); libarc by default."""
 from __future__ import annotations
 
 import ctypes as C
@@ -18,27 +20,35 @@ AVPL_DTYPE = np.dtype([("position", "<f4", 3), ("normal", "<f4", 3), ("incRadian
 assert AVPL_DTYPE.itemsize == C.sizeof(L.ArcAvplHost)
 
 
-def scene_desc(preset: int, seed: int = 0, num_boxes: int = 0) -> L.ArcSceneDesc:
+def _check(lib, status: int, where: str) -> None:
+    if status != L.ARC_OK:
+        raise L.ArcError(status, where, lib.arc_last_error().decode())
+
+
+def scene_desc(preset: int, seed: int = 0, num_boxes: int = 0, lib=None) -> L.ArcSceneDesc:
+    lib = lib or L.load()
     d = L.ArcSceneDesc()
-    L.check(L.load().arc_scene_preset_desc(int(preset), int(seed), int(num_boxes), C.byref(d)), "arc_scene_preset_desc")
+    _check(lib, lib.arc_scene_preset_desc(int(preset), int(seed), int(num_boxes), C.byref(d)), "arc_scene_preset_desc")
     return d
 
 
 def trace_avpls(desc: L.ArcSceneDesc, seed: int, num: int, max_bounces: int = 3,
-                explicit_direct: bool = True) -> tuple[np.ndarray, int]:
+                explicit_direct: bool = True, lib=None) -> tuple[np.ndarray, int]:
+    lib = lib or L.load()
     out = np.zeros(num, dtype=AVPL_DTYPE)
     paths = C.c_int64(0)
-    L.check(L.load().arc_scene_trace_avpls(C.byref(desc), int(seed), int(max_bounces), int(explicit_direct), int(num),
-                                           out.ctypes.data_as(C.POINTER(L.ArcAvplHost)), C.byref(paths)),
-            "arc_scene_trace_avpls")
+    _check(lib, lib.arc_scene_trace_avpls(C.byref(desc), int(seed), int(max_bounces), int(explicit_direct), int(num),
+                                          out.ctypes.data_as(C.POINTER(L.ArcAvplHost)), C.byref(paths)),
+           "arc_scene_trace_avpls")
     return out, int(paths.value)
 
 
-def gbuffer(desc: L.ArcSceneDesc, width: int, height: int) -> tuple[np.ndarray, np.ndarray]:
+def gbuffer(desc: L.ArcSceneDesc, width: int, height: int, lib=None) -> tuple[np.ndarray, np.ndarray]:
+    lib = lib or L.load()
     pos = np.zeros((height, width, 4), dtype=np.float32)
     nrm = np.zeros((height, width, 4), dtype=np.float32)
-    L.check(L.load().arc_scene_gbuffer(C.byref(desc), int(width), int(height), pos.ctypes.data, nrm.ctypes.data),
-            "arc_scene_gbuffer")
+    _check(lib, lib.arc_scene_gbuffer(C.byref(desc), int(width), int(height), pos.ctypes.data, nrm.ctypes.data),
+           "arc_scene_gbuffer")
     return pos, nrm
 
 
@@ -101,11 +111,11 @@ class Workload:
     error_bound: float = 0.01
     extra: dict = field(default_factory=dict)
 
-    def build(self, width: int | None = None, height: int | None = None, num_avpls: int | None = None):
+    def build(self, width: int | None = None, height: int | None = None, num_avpls: int | None = None, lib=None):
         """Scene description, AVPLs, G-buffer (optionally at a reduced size for tests)."""
-        desc = scene_desc(self.preset, self.scene_seed, self.num_boxes)
-        avpls, paths = trace_avpls(desc, self.avpl_seed, num_avpls or self.num_avpls, self.max_bounces)
-        pos, nrm = gbuffer(desc, width or self.width, height or self.height)
+        desc = scene_desc(self.preset, self.scene_seed, self.num_boxes, lib=lib)
+        avpls, paths = trace_avpls(desc, self.avpl_seed, num_avpls or self.num_avpls, self.max_bounces, lib=lib)
+        pos, nrm = gbuffer(desc, width or self.width, height or self.height, lib=lib)
         return desc, avpls, paths, pos, nrm
 
 

@@ -146,31 +146,44 @@ def max_over_ranks(world, x: float) -> float:
     return float(t.item())
 
 
-def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, threads: int, ref64=None) -> dict:
-    """The scalar FP32 CPU gather (oracle restatement of the reference's formulas) on a seeded
-    pixel sample over all AVPLs, extrapolated to the full frame.  With ref64 (the all-FP64 GPU
-    image, [pixels, 3]) it also checks that image against the CPU FP64 oracle on 64 sampled pixels."""
-    from oracle import oracle as O
-
-    prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
-    H, W = pos.shape[:2]
-    valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
-    order = np.random.default_rng(7).permutation(valid)
-    # chunks of a seeded pixel permutation until target_s of gather time is spent (or every surface
-    # pixel is done); each chunk is sized from the rate measured so far, aiming at a quarter of the
-    # remaining time
-    k, dt, chunk = 0, 0.0, 4 * threads
+def _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s: float, threads: int):
+    """Runs the scalar FP32 CPU gather over chunks of the pixel list `order` until target_s seconds
+    of gather time are spent (or the list is done) -> (pixels gathered, seconds).  Every chunk is a
+    multiple of `threads` pixels and the gather hands out one pixel at a time, so no thread idles
+    while another still has pixels; after the first chunk each is sized to about a quarter of the
+    remaining time at the rate measured so far."""
+    k, dt, chunk = 0, 0.0, threads
     while k < len(order) and dt < target_s:
         part = order[k:k + chunk]
         t0 = time.perf_counter()
         O.gather_fp32(pos, nrm, part, avpls, dif, spe, ex, cam, prm, threads=threads)
         dt += time.perf_counter() - t0
         k += len(part)
-        rate = k / max(dt, 1e-6)
-        chunk = int(max(4 * threads, min(4 * chunk, rate * max(target_s - dt, 0.0) / 4)))
+        want = (k / max(dt, 1e-6)) * max(target_s - dt, 0.0) / 4
+        chunk = max(threads, int(want // threads) * threads)
+    return k, dt
+
+
+def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, threads: int, ref64=None,
+                 single_s: float = 0.0) -> dict:
+    """The scalar FP32 CPU gather (oracle restatement of the reference's formulas, -O3) on a seeded
+    pixel sample over all AVPLs, with `threads` host threads, extrapolated to the full frame; with
+    single_s > 0 also one thread for single_s seconds.  With ref64 (the all-FP64 GPU image,
+    [pixels, 3]) it also checks that image against the CPU FP64 oracle on 64 sampled pixels."""
+    from oracle import oracle as O
+
+    prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
+    valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
+    order = np.random.default_rng(7).permutation(valid)
+    k, dt = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s, threads)
     # every pixel costs the same (all AVPLs); background pixels cost nothing, so extrapolate over
     # the valid pixels
     ms_frame = dt * 1e3 * len(valid) / max(k, 1)
+    single = None
+    if single_s > 0:
+        k1, dt1 = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, single_s, 1)
+        single = {"value": dt1 * 1e3 * len(valid) / max(k1, 1), "unit": UNIT, "cores": 1,
+                  "sample": f"{k1} random surface pixels x {len(avpls)} AVPLs, {dt1:.1f} s"}
     sample = order[:k]
     check = None
     if ref64 is not None:
@@ -178,9 +191,14 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
         _, _, o64 = O.gather_fp64(pos, nrm, px, avpls, dif, spe, ex, cam, prm, threads=threads)
         d = ref64[px] - o64
         check = float(np.max(np.sqrt(np.mean(d ** 2, 0)) / (np.sqrt(np.mean(o64 ** 2, 0)) + 1e-300)))
-    return {"value": ms_frame, "unit": UNIT, "cores": threads, "kind": "port", "fp64_image_vs_oracle_rel_rmse": check,
-            "sample": f"{k} random surface pixels x {len(avpls)} AVPLs (scalar FP32 C, -O2, {threads} threads), "
-                      f"{dt:.1f} s, extrapolated to {len(valid)} surface pixels"}
+    out = {"value": ms_frame, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"{k} random surface pixels x {len(avpls)} AVPLs (scalar FP32 C, -O3, {threads} threads, "
+                     f"one pixel per work item), {dt:.1f} s, extrapolated to {len(valid)} surface pixels"}
+    if single is not None:
+        out["single_thread"] = single
+    if ref64 is not None:
+        out["fp64_image_vs_oracle_rel_rmse"] = check
+    return out
 
 
 def scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream) -> dict:
@@ -357,10 +375,16 @@ def run_reference(args):
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return 0
+    # the inputs come from the scene generator's source built without the GPU library
+    # (oracle/libinputs.so): this process loads no GPU code
+    from antiradiancecuts_b200 import _lib as L
     from antiradiancecuts_b200 import scene
+    from oracle import oracle as O
 
+    if not os.path.exists(O.INPUTS_LIB):
+        O.build()
     wl = scene.WORKLOADS[args.workload]
-    desc, avpls, paths, pos, nrm = wl.build()
+    desc, avpls, paths, pos, nrm = wl.build(lib=L.load_scene_library(O.INPUTS_LIB))
     _, dif, spe, ex = scene.materials(desc)
     cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
     threads = os.cpu_count() or 1
@@ -394,7 +418,8 @@ def main():
     ap.add_argument("--error-bound", type=float, default=0.002, help="analytic cut (error_bound method)")
     ap.add_argument("--small", action="store_true", help="640x360 / 262,144 AVPLs, no extras (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip exact / FP64 / CPU legs")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="all-core CPU baseline sample")
+    ap.add_argument("--cpu-single-seconds", type=float, default=5.0, help="single-thread CPU baseline sample")
     ap.add_argument("--batch-views", type=int, default=32, help="views of the multi-view batch leg")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -624,7 +649,7 @@ def main():
     cpu = None
     if rank == 0 and not args.no_extras:
         cpu = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, args.cpu_seconds, os.cpu_count() or 1,
-                           ref64=ref64)
+                           ref64=ref64, single_s=args.cpu_single_seconds)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
     batch = gen = post = clus = None

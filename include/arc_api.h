@@ -220,9 +220,12 @@ arc_status arc_gather_bruteforce(arc_context* ctx, const ArcAvplsGpuParam* avpls
  * passes the AVPL arrays, the G-buffer and the outputs.  Its scratch (packed AVPL records, the
  * material table, the device error word) is one fixed file-scope device array that every GPU
  * loading libarc holds until process exit; it is sized for at most 65,536 AVPLs, and larger
- * inputs are rejected with ARC_ERR_INVALID_ARG.  The first call on a device looks up that
- * array's device address; make it before any stream capture.  All calls share the array:
- * calls whose GPU work overlaps (on different streams or devices sharing a process) race on it.
+ * inputs are rejected with ARC_ERR_INVALID_ARG.  The first call on a device (and the first after
+ * a device reset, or in another driver context) looks up that array's device address; make it
+ * before any stream capture.  Every device holds its own copy of the array, which keeps the last
+ * call's contents: calls whose GPU work overlaps on the same device (different streams) race on
+ * that device's copy; calls on different devices do not share it.  The material table is passed
+ * to the GPU as a kernel argument, so `materials` may be released when the call returns.
  * If device_error_word is non-NULL the call waits for the stream and returns the error word
  * (ARC_DEVERR_*) of this call. */
 arc_status arc_gather_bruteforce_noalloc(void* cuda_stream, const ArcMaterial* materials, int32_t num_materials,
@@ -245,6 +248,13 @@ typedef struct ArcLbvhParams {
     ArcFloat3 scene_min;
     ArcFloat3 scene_max;
     uint32_t repr_seed; /* seed of the counter-based hash that replaces the host mt19937 of bvh.cu:694-697 */
+    /* Polls after which the radix sort's look-back (a bounded wait on another tile's published
+     * offsets) gives up.  0 (default): 2^26, after which the wait sets ARC_DEVERR_TIMEOUT and the
+     * rest of the build is skipped on the device (the object then holds no valid tree until the
+     * next build).  Non-zero: that limit, and arc_lbvh_build waits for the build and returns
+     * ARC_ERR_TIMEOUT (the object left unbuilt) if the wait gave up -- a knob for tests of the
+     * timeout path. */
+    uint32_t wait_limit;
 } ArcLbvhParams;
 
 void arc_lbvh_params_default(ArcLbvhParams* p);
@@ -421,12 +431,14 @@ arc_status arc_mlp_train_step(arc_mlp* mlp, const void* features_bf16, const flo
  * prefix sums over the sorted leaves) and writes, for each visited node that the learned selection
  * with `cut` would score (its bound above cut->error_bound times the estimate and not above
  * cut->mlp_band times that), its 16 BF16 features, its 0/1 label and its error relative to the
- * tile value.  Device output arrays of `capacity` rows; *count receives the rows written.  Waits
- * for the stream. */
+ * tile value.  Device output arrays of `capacity` rows; keys (optional, 2 ints per row) receives
+ * each row's (tile, node): the tile index in row-major 8x8 tiles of `gbuffer`, the node in record
+ * index space (inner k at num_leaves + k).  Rows come in no particular order across tiles.
+ * *count receives the rows written.  Waits for the stream. */
 arc_status arc_cut_training_samples(arc_context* ctx, const arc_lbvh* bvh, const ArcGBufferView* gbuffer,
                                     ArcFloat3 camera_position, const ArcGatherParams* params, const ArcCutParams* cut,
-                                    float delta, void* features_bf16, float* labels, float* errors, int32_t capacity,
-                                    int32_t* count);
+                                    float delta, void* features_bf16, float* labels, float* errors, int32_t* keys,
+                                    int32_t capacity, int32_t* count);
 
 /* ---------------------------------------------------------------------------------------- */
 /* CudaGather::run                                                                           */

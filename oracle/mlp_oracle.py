@@ -79,3 +79,24 @@ def loss_and_grad(p, x, labels, weights=None, loss="bce"):
     dz1 = (dz2 @ P["W2"]) * gelu_grad(z1)
     g["W1"], g["b1"] = dz1.T @ x, dz1.sum(0)
     return loss, pack(g)
+
+
+def bf16(x):
+    """Round to the nearest BF16 (ties to even), returned as float64."""
+    u = np.ascontiguousarray(np.asarray(x, np.float32)).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward_bf16(p, x):
+    """The network with the tensor-core kernels' rounding points: BF16 inputs, weights W1..W3 and
+    hidden activations h1, h2; FP64 otherwise (accumulation, biases, GELU, the 64 -> 1 layer)."""
+    P = unpack(p)
+    h = bf16(x)
+    z1 = h @ bf16(P["W1"]).T + P["b1"]
+    h1 = bf16(gelu(z1))
+    z2 = h1 @ bf16(P["W2"]).T + P["b2"]
+    h2 = bf16(gelu(z2))
+    z3 = h2 @ bf16(P["W3"]).T + P["b3"]
+    h3 = gelu(z3)
+    return h3 @ P["w4"] + P["b4"][0]

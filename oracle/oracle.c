@@ -175,7 +175,7 @@ OR_EXPORT void oracle_gather_fp64(const float* gb_pos, const float* gb_nrm, int3
     oracle_materials M = {diffuse, specular, exponent, num_materials};
     d3 c = d3load(cam);
     (void)width;
-#pragma omp parallel for schedule(dynamic, 16) num_threads(num_threads > 0 ? num_threads : 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads > 0 ? num_threads : 1)
     for (int32_t k = 0; k < num_pixels; ++k) {
         const int64_t px = pixels[k];
         const float* gp = gb_pos + 4 * px;
@@ -343,7 +343,7 @@ OR_EXPORT void oracle_gather_fp32(const float* gb_pos, const float* gb_nrm, int3
     const float cos_half = cosf(P->cone_half_angle);
     const float clamp2 = P->dist_clamp * P->dist_clamp;
     (void)width;
-#pragma omp parallel for schedule(dynamic, 16) num_threads(num_threads > 0 ? num_threads : 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads > 0 ? num_threads : 1)
     for (int32_t k = 0; k < num_pixels; ++k) {
         const int64_t px = pixels[k];
         const int mat = (int)gb_nrm[4 * px + 3];
@@ -818,7 +818,7 @@ OR_EXPORT void oracle_cut_solid_angle(const float* gb_pos, const float* gb_nrm, 
     P.dist_clamp = dist_clamp;
     d3 c = d3load(cam);
     const float two_pi = 2.0f * kPiF;
-#pragma omp parallel for schedule(dynamic, 16) num_threads(num_threads > 0 ? num_threads : 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads > 0 ? num_threads : 1)
     for (int32_t q = 0; q < num_pixels; ++q) {
         const int64_t px = pixels[q];
         const float* gp = gb_pos + 4 * px;
@@ -1226,4 +1226,371 @@ OR_EXPORT void oracle_eval_cut(const float* gb_pos, const float* gb_nrm, int32_t
             out_res[3 * px + k] = r[k] - a[k];
         }
     }
+}
+
+/* ---------------------------------------------------------------------------------------- */
+/* Learned cut: tile records, the 16 features of a (tile, inner node) pair, training labels  */
+/* (no counterpart in the reference; restates antiradiancecuts_b200/csrc/learned.cu with     */
+/* correctly rounded operations where the GPU uses approximate log2 / rsqrt / division)      */
+/* ---------------------------------------------------------------------------------------- */
+
+/* tile record: [tmin3, tmax3, ncone4, kdl, tau, mean, valid, rt, sn] */
+enum { OR_TREC = 16 };
+
+static void tile_record(const tile_info* t, float* r) {
+    for (int k = 0; k < 3; ++k) {
+        r[k] = t->tmin[k];
+        r[3 + k] = t->tmax[k];
+    }
+    for (int k = 0; k < 4; ++k) r[6 + k] = t->ncone[k];
+    r[10] = t->kdl;
+    r[11] = t->tau;
+    r[12] = t->mean;
+    r[13] = (float)t->valid;
+    float et[3] = {t->tmax[0] - t->tmin[0], t->tmax[1] - t->tmin[1], t->tmax[2] - t->tmin[2]};
+    r[14] = t->valid > 0 ? 0.5f * sqrtf(dot3(et, et)) : 0.0f;
+    r[15] = sqrtf(fmaxf(0.0f, 1.0f - t->ncone[3] * t->ncone[3]));
+}
+
+static void tile_from_record(const float* r, tile_info* t) {
+    for (int k = 0; k < 3; ++k) {
+        t->tmin[k] = r[k];
+        t->tmax[k] = r[3 + k];
+    }
+    for (int k = 0; k < 4; ++k) t->ncone[k] = r[6 + k];
+    t->kdl = r[10];
+    t->tau = r[11];
+    t->mean = r[12];
+    t->valid = (int)r[13];
+}
+
+/* Tile records of every 8x8 tile (cut_tile_setup's quantities): out [tiles][16]. */
+OR_EXPORT void oracle_tile_records(const float* gb_pos, const float* gb_nrm, int32_t W, int32_t H, int32_t n,
+                                   const float* bounds, const float* records, const float* diffuse,
+                                   int32_t num_materials, float eps_bound, float dist_clamp, float* out,
+                                   int32_t num_threads) {
+    const int tx_n = (W + 7) / 8, ty_n = (H + 7) / 8;
+    const float clamp2 = dist_clamp > 0.0f ? dist_clamp * dist_clamp : 0.0f;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(num_threads > 0 ? num_threads : 1)
+    for (int tile = 0; tile < tx_n * ty_n; ++tile) {
+        tile_info t;
+        tile_setup(gb_pos, gb_nrm, W, H, tile % tx_n, tile / tx_n, n, bounds, records, diffuse, num_materials,
+                   eps_bound, clamp2, &t);
+        tile_record(&t, out + (size_t)OR_TREC * tile);
+    }
+}
+
+/* Radiance and antiradiance luminance of a record {p, n, w} with luminances L, A at the point c
+ * with unit normal nn (record_at of learned.cu). */
+static void record_at(const float* q, float L, float A, const float* c, const float* nn, float clamp2, float cos_thr,
+                      float* rad, float* ar) {
+    const float dx = q[0] - c[0], dy = q[1] - c[1], dz = q[2] - c[2];
+    const float l2 = fmaxf((dx * dx + dy * dy) + dz * dz, 1e-12f);
+    const float r = 1.0f / sqrtf(l2);
+    const float c1 = ((nn[0] * dx + nn[1] * dy) + nn[2] * dz) * r;
+    const float c2 = -((q[3] * dx + q[4] * dy) + q[5] * dz) * r;
+    const float inv = 1.0f / fmaxf(l2, clamp2);
+    *rad = ((L * fmaxf(c1, 0.0f)) * fmaxf(c2, 0.0f)) * inv;
+    const float cw = -((q[6] * dx + q[7] * dy) + q[8] * dz) * r;
+    *ar = (cw > cos_thr && c1 > 0.001f) ? (A * c1) * inv : 0.0f;
+}
+
+static float clampf2(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+static float safe_log2f(float v) { return log2f(fmaxf(v, 1e-30f)); }
+
+/* The 16 features of (tile, inner node) (node_features of learned.cu).  geom: node_bound's
+ * d2c, cos1, cos2, ar_ok, dc, rs, rn; b: the node's 16-float bounds record (cones at 8 and 12);
+ * rec, rl, rr: records of the node and its children; ds: the node's direction statistics.
+ * aux (may be NULL): |rad - rad_l - rad_r| s, (|rad| + |rad_l| + |rad_r|) s and the same for
+ * antiradiance, the conditioning of features 12 and 13. */
+static void node_features(const tile_info* t, const float* geom, float M, const float* b, const float* rec,
+                          const float* rl, const float* rr, const float* ds, int depth, float clamp2, float cos_thr,
+                          float* f, float* aux) {
+    const float E = fmaxf(t->mean, 1e-30f);
+    const float dc = geom[4], rs = geom[5], rn = geom[6];
+    const float inv_dc = 1.0f / fmaxf(dc, 1e-6f);
+    const float rt = rs - rn;
+    const float c[3] = {0.5f * (t->tmin[0] + t->tmax[0]), 0.5f * (t->tmin[1] + t->tmax[1]),
+                        0.5f * (t->tmin[2] + t->tmax[2])};
+    float nn[3] = {t->ncone[0], t->ncone[1], t->ncone[2]};
+    const float nl = dot3(nn, nn);
+    if (nl > 0.0f) {
+        const float s = 1.0f / sqrtf(nl);
+        nn[0] *= s;
+        nn[1] *= s;
+        nn[2] *= s;
+    }
+    const float Ls = lum3f(rec[9], rec[10], rec[11]), As = lum3f(rec[12], rec[13], rec[14]);
+    float rad, ar, radl, arl, radr, arr;
+    record_at(rec, Ls, As, c, nn, clamp2, cos_thr, &rad, &ar);
+    record_at(rl, lum3f(rl[9], rl[10], rl[11]), lum3f(rl[12], rl[13], rl[14]), c, nn, clamp2, cos_thr, &radl, &arl);
+    record_at(rr, lum3f(rr[9], rr[10], rr[11]), lum3f(rr[12], rr[13], rr[14]), c, nn, clamp2, cos_thr, &radr, &arr);
+    const float s = t->kdl / E;
+    f[0] = clampf2((M > 0.0f ? safe_log2f(M / fmaxf(t->tau, 1e-30f)) : -32.0f) * 0.125f, -4.0f, 4.0f);
+    f[1] = clampf2(safe_log2f(Ls * s) * 0.125f, -4.0f, 4.0f);
+    f[2] = clampf2(safe_log2f(As * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[3] = clampf2(rn * inv_dc, 0.0f, 4.0f);
+    f[4] = clampf2(rt * inv_dc, 0.0f, 4.0f);
+    f[5] = clampf2(sqrtf(geom[0]) * inv_dc, 0.0f, 4.0f);
+    f[6] = geom[1];
+    f[7] = geom[2];
+    f[8] = geom[3] == 1.0f ? 1.0f : 0.0f;
+    f[9] = geom[3] > 0.0f ? 1.0f : 0.0f;
+    f[10] = b[11];
+    f[11] = b[15];
+    const float dr = fabsf((rad - radl) - radr), da = fabsf((ar - arl) - arr);
+    f[12] = clampf2(safe_log2f(dr * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[13] = clampf2(safe_log2f(da * s + 1e-20f) * 0.125f, -4.0f, 4.0f);
+    f[14] = (float)depth * (1.0f / 32.0f);
+    const float sl = sqrtf((ds[0] * ds[0] + ds[1] * ds[1]) + ds[2] * ds[2]);
+    f[15] = ds[3] > 0.0f ? clampf2(2.0f * (sl / ds[3]) - 1.0f, -1.0f, 1.0f) : -1.0f;
+    if (aux) {
+        aux[0] = dr * s;
+        aux[1] = ((fabsf(rad) + fabsf(radl)) + fabsf(radr)) * s;
+        aux[2] = da * s;
+        aux[3] = ((fabsf(ar) + fabsf(arl)) + fabsf(arr)) * s;
+    }
+}
+
+static void fill_bound_params(bound_params* bp, float dist_clamp, int32_t ar_kind, float cone_half_angle,
+                              float disk_radius, float ar_uncertain) {
+    bp->clamp2 = dist_clamp > 0.0f ? dist_clamp * dist_clamp : 0.0f;
+    bp->ar_kind = ar_kind;
+    bp->eps_cone = 0.001f;
+    bp->cos_thr = fmaxf(cosf(cone_half_angle), 0.001f);
+    bp->disk_scale = disk_radius > 0.0f ? 1.0f / (kPiF * disk_radius * disk_radius) : 0.0f;
+    bp->ar_uncertain = ar_uncertain;
+}
+
+static int child_of(const float* b, int which, int32_t n) {
+    int32_t c;
+    memcpy(&c, &b[which ? 7 : 3], 4);
+    return c >= 0 ? c : n - (c + 1);
+}
+
+/* Analytic bound and features of listed (tile, inner node) pairs: tile records from
+ * oracle_tile_records; nodes in record index space (inner k at n + k); out_M [k], out_feat
+ * [k][16], out_aux [k][4] (may be NULL). */
+OR_EXPORT void oracle_pair_features(const float* tile_records, int32_t num_pairs, const int32_t* tiles,
+                                    const int32_t* nodes, const int32_t* depths, int32_t n, const float* bounds,
+                                    const float* records, const float* dirstat, float dist_clamp, int32_t ar_kind,
+                                    float cone_half_angle, float disk_radius, float ar_uncertain, float* out_M,
+                                    float* out_feat, float* out_aux, int32_t num_threads) {
+    bound_params bp;
+    fill_bound_params(&bp, dist_clamp, ar_kind, cone_half_angle, disk_radius, ar_uncertain);
+#pragma omp parallel for schedule(static) num_threads(num_threads > 0 ? num_threads : 1)
+    for (int32_t i = 0; i < num_pairs; ++i) {
+        tile_info t;
+        tile_from_record(tile_records + (size_t)OR_TREC * tiles[i], &t);
+        const int node = nodes[i];
+        const float* b = bounds + 16 * (size_t)(node - n);
+        const float* rec = records + 16 * (size_t)node;
+        float geom[7];
+        const float M = node_bound(&t, b, rec, &bp, geom);
+        out_M[i] = M;
+        node_features(&t, geom, M, b, rec, records + 16 * (size_t)child_of(b, 0, n),
+                      records + 16 * (size_t)child_of(b, 1, n), dirstat + 4 * (size_t)node, depths[i], bp.clamp2,
+                      bp.cos_thr, out_feat + 16 * (size_t)i, out_aux ? out_aux + 4 * (size_t)i : NULL);
+    }
+}
+
+/* FP64 luminance of one record's signed contribution at a pixel (p, unit normal nn) with the
+ * receiver's diffuse/pi kd (record_lum of learned.cu over the pair terms of pair_math.cuh). */
+static double record_lum64(const float* q, const double* p, const double* nn, const double* kd, int ar_kind,
+                           double cos_thr, double inv_clamp2, double disk_r2, double disk_scale) {
+    const double dx = (double)q[0] - p[0], dy = (double)q[1] - p[1], dz = (double)q[2] - p[2];
+    double l2 = dx * dx + dy * dy + dz * dz;
+    if (!(l2 > 1e-30)) l2 = 1e-30;
+    const double r = 1.0 / sqrt(l2);
+    const double nd = nn[0] * dx + nn[1] * dy + nn[2] * dz;
+    const double nad = q[3] * dx + q[4] * dy + q[5] * dz;
+    const double c1 = nd * r, c2 = -nad * r;
+    const double rr = r * r;
+    const double inv = rr < inv_clamp2 ? rr : inv_clamp2;
+    const double g = (c1 > 0 ? c1 : 0) * (c2 > 0 ? c2 : 0) * inv;
+    double ga = 0.0, as = 1.0;
+    if (ar_kind == 2) {
+        const double cw = -(q[6] * dx + q[7] * dy + q[8] * dz) * r;
+        ga = (cw > cos_thr && c1 > 0.001) ? c1 * inv : 0.0;
+    } else if (ar_kind == 1) {
+        const double ww = (double)q[6] * q[6] + (double)q[7] * q[7] + (double)q[8] * q[8];
+        const double wn = q[6] * nn[0] + q[7] * nn[1] + q[8] * nn[2];
+        if (ww > 0 && wn < 0) {
+            const double t = -nd / wn, ts = t / sqrt(ww);
+            const double hx = dx + ts * q[6], hy = dy + ts * q[7], hz = dz + ts * q[8];
+            if (t > 0 && hx * hx + hy * hy + hz * hz < disk_r2 && nad > 0) ga = 1.0;
+        }
+        as = disk_scale;
+    }
+    const double c0 = kd[0] * (q[9] * g - as * q[12] * ga), cc1 = kd[1] * (q[10] * g - as * q[13] * ga),
+                 cc2 = kd[2] * (q[11] * g - as * q[14] * ga);
+    return 0.2126 * c0 + 0.7152 * cc1 + 0.0722 * cc2;
+}
+
+/*
+ * Training samples of the learned cut (arc_cut_training_samples): for every 8x8 tile with a
+ * surface, the exact per-pixel contribution of each node (FP64 over its leaves), and the
+ * labelling walk of label_traverse: depth-first from the root, nodes the analytic bound
+ * accepts are skipped, nodes above band times tau are refined without a sample, every other
+ * node gets a sample (features, label = RMS over the tile's pixels of |exact - node estimate| >
+ * delta * mean |exact tile value|, error = that RMS / the mean) and its children are walked; the
+ * children of an accepted node are sampled one level only.  Samples are written tile after tile,
+ * each tile's in walk order.  keys [cap][2] = (tile, node).  Returns the number of samples (may
+ * exceed capacity: only the first `capacity` are written).
+ */
+OR_EXPORT int32_t oracle_training_samples(const float* gb_pos, const float* gb_nrm, int32_t W, int32_t H, int32_t n,
+                                          const float* bounds, const float* records, const float* dirstat,
+                                          const float* diffuse, int32_t num_materials, float eps_bound,
+                                          float dist_clamp, int32_t ar_kind, float cone_half_angle,
+                                          float disk_radius, float ar_uncertain, float band, float delta,
+                                          int32_t capacity, int32_t* out_keys, float* out_feat, float* out_labels,
+                                          float* out_errs, int32_t num_threads) {
+    const int tx_n = (W + 7) / 8, ty_n = (H + 7) / 8, tiles = tx_n * ty_n;
+    bound_params bp;
+    fill_bound_params(&bp, dist_clamp, ar_kind, cone_half_angle, disk_radius, ar_uncertain);
+    const double cos_thr = (double)bp.cos_thr;
+    const double inv_clamp2 = dist_clamp > 0.0f ? 1.0 / (double)bp.clamp2 : INFINITY;
+    const double disk_r2 = (double)disk_radius * disk_radius;
+    const double disk_scale = (double)bp.disk_scale;
+    /* leaf range [first, last] of every inner node: the leftmost and rightmost leaf below it */
+    int32_t* range = (int32_t*)malloc(sizeof(int32_t) * 2 * (size_t)(n > 1 ? n - 1 : 1));
+    for (int32_t k = 0; k + 1 < n; ++k) {
+        int node = n + k;
+        while (node >= n) node = child_of(bounds + 16 * (size_t)(node - n), 0, n);
+        range[2 * k] = node;
+        node = n + k;
+        while (node >= n) node = child_of(bounds + 16 * (size_t)(node - n), 1, n);
+        range[2 * k + 1] = node;
+    }
+    int32_t* tcount = (int32_t*)calloc((size_t)tiles, sizeof(int32_t));
+    int32_t** tkeys = (int32_t**)calloc((size_t)tiles, sizeof(int32_t*));
+    float** tfeat = (float**)calloc((size_t)tiles, sizeof(float*));
+    float** tlab = (float**)calloc((size_t)tiles, sizeof(float*));
+#pragma omp parallel num_threads(num_threads > 0 ? num_threads : 1)
+    {
+        double* P = (double*)malloc(sizeof(double) * 64 * (size_t)(n + 1));
+        int32_t* stack = (int32_t*)malloc(sizeof(int32_t) * 3 * 256);
+#pragma omp for schedule(dynamic, 1)
+        for (int tile = 0; tile < tiles; ++tile) {
+            tile_info t;
+            tile_setup(gb_pos, gb_nrm, W, H, tile % tx_n, tile / tx_n, n, bounds, records, diffuse, num_materials,
+                       eps_bound, bp.clamp2, &t);
+            if (t.valid == 0) continue;
+            double px[64][3], nn[64][3], kd[64][3];
+            int valid[64], nv = 0;
+            for (int p = 0; p < 64; ++p) {
+                const int x = (tile % tx_n) * 8 + p % 8, y = (tile / tx_n) * 8 + p / 8;
+                valid[p] = 0;
+                if (x >= W || y >= H) continue;
+                const float* gp = gb_pos + 4 * ((size_t)y * W + x);
+                const float* gn = gb_nrm + 4 * ((size_t)y * W + x);
+                const int m = (int)gn[3];
+                if (m <= 0 || m >= num_materials) continue;
+                const double l = sqrt((double)gn[0] * gn[0] + (double)gn[1] * gn[1] + (double)gn[2] * gn[2]);
+                for (int k = 0; k < 3; ++k) {
+                    px[p][k] = gp[k];
+                    nn[p][k] = gn[k] / l;
+                    kd[p][k] = (double)(kOneOverPiF * diffuse[3 * m + k]);
+                }
+                valid[p] = 1;
+                ++nv;
+            }
+            /* P[i][p]: sum of the first i leaves' contributions at pixel p */
+            for (int p = 0; p < 64; ++p) P[p] = 0.0;
+            for (int32_t i = 0; i < n; ++i) {
+                const float* q = records + 16 * (size_t)i;
+                for (int p = 0; p < 64; ++p)
+                    P[64 * (size_t)(i + 1) + p] =
+                        P[64 * (size_t)i + p] +
+                        (valid[p] ? record_lum64(q, px[p], nn[p], kd[p], ar_kind, cos_thr, inv_clamp2, disk_r2,
+                                                 disk_scale)
+                                  : 0.0);
+            }
+            double E = 0.0;
+            for (int p = 0; p < 64; ++p)
+                if (valid[p]) E += fabs(P[64 * (size_t)n + p]);
+            E /= (double)nv;
+            const double thr = (double)delta * E;
+            int cap_t = 256, cnt = 0;
+            int32_t* keys = (int32_t*)malloc(sizeof(int32_t) * 2 * cap_t);
+            float* feat = (float*)malloc(sizeof(float) * 16 * cap_t);
+            float* lab = (float*)malloc(sizeof(float) * 2 * cap_t);
+            /* stack entries: node, depth, extra */
+            int sp = 0;
+            stack[0] = n; stack[1] = 0; stack[2] = 0; sp = 1;
+            int64_t budget = 4 * (int64_t)n;
+            while (sp > 0 && --budget > 0) {
+                --sp;
+                const int node = stack[3 * sp], depth = stack[3 * sp + 1], extra = stack[3 * sp + 2];
+                if (node < n) continue;
+                const float* b = bounds + 16 * (size_t)(node - n);
+                const float* rec = records + 16 * (size_t)node;
+                float geom[7];
+                const float M = node_bound(&t, b, rec, &bp, geom);
+                if (!(M > t.tau)) continue;
+                const int c0 = child_of(b, 0, n), c1 = child_of(b, 1, n);
+                const int d1 = depth + 1 < 127 ? depth + 1 : 127;
+                if (M > band * t.tau) {
+                    if (!extra && sp + 2 <= 256) {
+                        stack[3 * sp] = c1; stack[3 * sp + 1] = d1; stack[3 * sp + 2] = 0; ++sp;
+                        stack[3 * sp] = c0; stack[3 * sp + 1] = d1; stack[3 * sp + 2] = 0; ++sp;
+                    }
+                    continue;
+                }
+                const int k = node - n, f0 = range[2 * k], l0 = range[2 * k + 1];
+                double e2 = 0.0;
+                for (int p = 0; p < 64; ++p) {
+                    if (!valid[p]) continue;
+                    const double exact = P[64 * (size_t)(l0 + 1) + p] - P[64 * (size_t)f0 + p];
+                    const double approx =
+                        record_lum64(rec, px[p], nn[p], kd[p], ar_kind, cos_thr, inv_clamp2, disk_r2, disk_scale);
+                    e2 += (exact - approx) * (exact - approx);
+                }
+                const double erms = sqrt(e2 / (double)nv);
+                const int refine = erms > thr;
+                if (cnt == cap_t) {
+                    cap_t *= 2;
+                    keys = (int32_t*)realloc(keys, sizeof(int32_t) * 2 * cap_t);
+                    feat = (float*)realloc(feat, sizeof(float) * 16 * cap_t);
+                    lab = (float*)realloc(lab, sizeof(float) * 2 * cap_t);
+                }
+                keys[2 * cnt] = tile;
+                keys[2 * cnt + 1] = node;
+                node_features(&t, geom, M, b, rec, records + 16 * (size_t)c0, records + 16 * (size_t)c1,
+                              dirstat + 4 * (size_t)node, depth, bp.clamp2, bp.cos_thr, feat + 16 * (size_t)cnt, NULL);
+                lab[2 * cnt] = refine ? 1.0f : 0.0f;
+                lab[2 * cnt + 1] = E > 0.0 ? (float)(erms / E) : 0.0f;
+                ++cnt;
+                if (extra || sp + 2 > 256) continue;
+                stack[3 * sp] = c1; stack[3 * sp + 1] = d1; stack[3 * sp + 2] = !refine; ++sp;
+                stack[3 * sp] = c0; stack[3 * sp + 1] = d1; stack[3 * sp + 2] = !refine; ++sp;
+            }
+            tcount[tile] = cnt;
+            tkeys[tile] = keys;
+            tfeat[tile] = feat;
+            tlab[tile] = lab;
+        }
+        free(stack);
+        free(P);
+    }
+    int64_t total = 0;
+    for (int tile = 0; tile < tiles; ++tile) {
+        for (int j = 0; j < tcount[tile]; ++j, ++total) {
+            if (total >= capacity) continue;
+            out_keys[2 * total] = tkeys[tile][2 * j];
+            out_keys[2 * total + 1] = tkeys[tile][2 * j + 1];
+            memcpy(out_feat + 16 * (size_t)total, tfeat[tile] + 16 * (size_t)j, 16 * sizeof(float));
+            out_labels[total] = tlab[tile][2 * j];
+            out_errs[total] = tlab[tile][2 * j + 1];
+        }
+        free(tkeys[tile]);
+        free(tfeat[tile]);
+        free(tlab[tile]);
+    }
+    free(tcount);
+    free(tkeys);
+    free(tfeat);
+    free(tlab);
+    free(range);
+    return (int32_t)(total < INT32_MAX ? total : INT32_MAX);
 }

@@ -27,9 +27,18 @@ class OracleParams(C.Structure):
                 ("dist_clamp", C.c_float), ("geo_limit_radiance", C.c_float), ("geo_limit_antiradiance", C.c_float)]
 
 
+INPUTS_LIB = os.path.join(HERE, "libinputs.so")
+
+
 def build() -> None:
-    """Compile liboracle.so (and the reference Morton wrapper when the reference tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True, capture_output=True)
+    """Compile liboracle.so, libinputs.so and, when the reference's Framework/ directory is found
+    (environment variable ARC_REFERENCE_FRAMEWORK, else the checkout this recipe was written
+    against), the reference Morton wrapper in _ref/."""
+    ref = os.environ.get("ARC_REFERENCE_FRAMEWORK") or "/root/reference/Framework"
+    cmd = ["make", "-s", "-C", HERE]
+    if os.path.exists(os.path.join(ref, "morton.h")):
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True, capture_output=True)
 
 
 def lib() -> C.CDLL:
@@ -293,3 +302,116 @@ def node_bound(pos4, nrm4, tree, diffuse, tile, inner, eps_bound, dist_clamp, ar
           C.c_float(math.radians(cone_half_angle_deg)), C.c_float(ar_uncertain), C.c_int32(inner), _p(geom),
           _p(tinfo))
     return float(m), geom, tinfo
+
+
+# --- learned cut ---------------------------------------------------------------------------------
+# tile record columns: tmin(3) tmax(3) ncone(4) kdl tau mean valid rt sn
+TREC_TAU, TREC_MEAN, TREC_VALID = 11, 12, 13
+
+
+def tile_records(pos4, nrm4, tree, diffuse, eps_bound, dist_clamp, threads=0):
+    """Per 8x8 tile: the quantities of the GPU's tile set-up -> float32 [tiles, 16]."""
+    H, W = pos4.shape[:2]
+    pos4, nrm4 = _f32(pos4), _f32(nrm4)
+    n = len(tree["morton"])
+    tiles = ((W + 7) // 8) * ((H + 7) // 8)
+    out = np.zeros((tiles, 16), np.float32)
+    b, r, dif = _f32(tree["bounds"]), _f32(tree["records"]), _f32(diffuse)
+    lib().oracle_tile_records(_p(pos4), _p(nrm4), C.c_int32(W), C.c_int32(H), C.c_int32(n), _p(b), _p(r), _p(dif),
+                              C.c_int32(len(dif)), C.c_float(eps_bound), C.c_float(dist_clamp), _p(out),
+                              C.c_int32(threads or os.cpu_count() or 1))
+    return out
+
+
+def pair_features(trec, tiles, nodes, depths, tree, dist_clamp, ar_kind, cone_half_angle_deg, disk_radius=0.0,
+                  ar_uncertain=16.0, threads=0):
+    """(bound M [k], features [k, 16], conditioning [k, 4]) of (tile, inner node) pairs; nodes in
+    record index space (inner k at n + k).  Conditioning: |rad - rad_l - rad_r| s, (|rad| + |rad_l| +
+    |rad_r|) s and the same for antiradiance (features 12 and 13 are logs of the differences)."""
+    tiles, nodes, depths = _i32(tiles), _i32(nodes), _i32(depths)
+    k = len(tiles)
+    n = len(tree["morton"])
+    M = np.zeros(k, np.float32)
+    F = np.zeros((k, 16), np.float32)
+    A = np.zeros((k, 4), np.float32)
+    b, r, ds = _f32(tree["bounds"]), _f32(tree["records"]), _f32(tree["dirstat"])
+    trec = _f32(trec)
+    lib().oracle_pair_features(_p(trec), C.c_int32(k), _p(tiles), _p(nodes), _p(depths), C.c_int32(n), _p(b), _p(r),
+                               _p(ds), C.c_float(dist_clamp), C.c_int32(ar_kind),
+                               C.c_float(math.radians(cone_half_angle_deg)), C.c_float(disk_radius),
+                               C.c_float(ar_uncertain), _p(M), _p(F), _p(A), C.c_int32(threads or os.cpu_count() or 1))
+    return M, F, A
+
+
+def training_samples(pos4, nrm4, tree, diffuse, eps_bound, dist_clamp, ar_kind, cone_half_angle_deg, band, delta,
+                     disk_radius=0.0, ar_uncertain=16.0, capacity=1 << 20, threads=0):
+    """The learned cut's labelling walk with FP64 exact node contributions -> (keys [k, 2] = (tile,
+    node), features [k, 16] float32, labels [k], errors [k]), tile after tile."""
+    H, W = pos4.shape[:2]
+    pos4, nrm4 = _f32(pos4), _f32(nrm4)
+    n = len(tree["morton"])
+    keys = np.zeros((capacity, 2), np.int32)
+    F = np.zeros((capacity, 16), np.float32)
+    lab = np.zeros(capacity, np.float32)
+    err = np.zeros(capacity, np.float32)
+    b, r, ds, dif = _f32(tree["bounds"]), _f32(tree["records"]), _f32(tree["dirstat"]), _f32(diffuse)
+    f = lib().oracle_training_samples
+    f.restype = C.c_int32
+    k = f(_p(pos4), _p(nrm4), C.c_int32(W), C.c_int32(H), C.c_int32(n), _p(b), _p(r), _p(ds), _p(dif),
+          C.c_int32(len(dif)), C.c_float(eps_bound), C.c_float(dist_clamp), C.c_int32(ar_kind),
+          C.c_float(math.radians(cone_half_angle_deg)), C.c_float(disk_radius), C.c_float(ar_uncertain),
+          C.c_float(band), C.c_float(delta), C.c_int32(capacity), _p(keys), _p(F), _p(lab), _p(err),
+          C.c_int32(threads or os.cpu_count() or 1))
+    k = min(k, capacity)
+    return keys[:k], F[:k], lab[:k], err[:k]
+
+
+def learned_cut(pos4, nrm4, tree, diffuse, params, eps_bound, ar_uncertain, band, thr_logit, dist_clamp, ar_kind,
+                cone_half_angle_deg, disk_radius=0.0, threads=0):
+    """The learned cut selection, level by level: leaves and nodes whose bound is within tau are
+    accepted, nodes above band * tau refined, the rest scored by the network (BF16 rounding points
+    of the tensor-core kernels, FP64 otherwise) and refined iff the logit reaches thr_logit.
+    -> (sorted node array per tile, scored (tile, node, logit) rows)."""
+    from . import mlp_oracle
+
+    n = len(tree["morton"])
+    trec = tile_records(pos4, nrm4, tree, diffuse, eps_bound, dist_clamp, threads)
+    tiles_n = trec.shape[0]
+    bounds = np.asarray(tree["bounds"], np.float32)
+    lc = bounds[:, 3].view(np.int32)
+    rc = bounds[:, 7].view(np.int32)
+    lc = np.where(lc >= 0, lc, n - (lc + 1))
+    rc = np.where(rc >= 0, rc, n - (rc + 1))
+    ft = np.nonzero(trec[:, TREC_VALID] > 0)[0].astype(np.int32)
+    fn = np.full(len(ft), n, np.int32)
+    depth = 0
+    acc_t, acc_n, scored = [], [], []
+    band32 = np.float32(band)
+    while len(ft):
+        leaf = fn < n
+        acc_t.append(ft[leaf])
+        acc_n.append(fn[leaf])
+        it, inn = ft[~leaf], fn[~leaf]
+        M, F, _ = pair_features(trec, it, inn, np.full(len(it), depth, np.int32), tree, dist_clamp, ar_kind,
+                                cone_half_angle_deg, disk_radius, ar_uncertain, threads)
+        tau = trec[it, TREC_TAU]
+        accept = ~(M > tau)
+        refine = (M > band32 * tau) & ~accept
+        score = ~accept & ~refine
+        if score.any():
+            y = mlp_oracle.forward_bf16(params, F[score])
+            refine[np.nonzero(score)[0][y >= thr_logit]] = True
+            scored.append(np.stack([it[score], inn[score], y], 1))
+        done = ~refine
+        acc_t.append(it[done])
+        acc_n.append(inn[done])
+        k = inn[refine] - n
+        ft = np.concatenate([it[refine], it[refine]]).astype(np.int32)
+        fn = np.concatenate([lc[k], rc[k]]).astype(np.int32)
+        depth += 1
+    at, an = np.concatenate(acc_t), np.concatenate(acc_n)
+    order = np.lexsort((an, at))
+    at, an = at[order], an[order]
+    starts = np.searchsorted(at, np.arange(tiles_n + 1))
+    cuts = [an[starts[t]:starts[t + 1]] for t in range(tiles_n)]
+    return cuts, (np.concatenate(scored) if scored else np.zeros((0, 3)))

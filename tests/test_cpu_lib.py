@@ -71,7 +71,7 @@ def test_defaults():
     assert g.dist_clamp == 0.0 and g.precision == L.ARC_PREC_KAHAN and g.tile_config == -1
     b = L.ArcLbvhParams()
     lib.arc_lbvh_params_default(C.byref(b))
-    assert b.bbox_mode == L.ARC_BBOX_SCENE and b.repr_seed == 5489 and b.consider_normals == 0
+    assert b.bbox_mode == L.ARC_BBOX_SCENE and b.repr_seed == 5489 and b.consider_normals == 0 and b.wait_limit == 0
 
 
 def test_null_arguments_are_rejected():

@@ -92,3 +92,18 @@ def test_reference_arm_prints_the_contract_line():
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == "room_256_4k"
+
+
+def test_reference_arm_loads_no_gpu_library():
+    """The reference arm makes its inputs with the scene generator built alone (oracle/libinputs.so)
+    and times the oracle's CPU gather: the process maps neither libarc.so nor any CUDA library."""
+    code = (f"import sys; sys.path.insert(0, {ROOT!r}); import bench, argparse; "
+            "a = argparse.Namespace(workload='room_256_4k', steps=1, warmup=0); bench.run_reference(a); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('LIBS', sorted({l.split()[-1] for l in maps.splitlines() if '.so' in l}))")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    libs = [s for s in r.stdout.splitlines() if s.startswith("LIBS")][0]
+    assert "liboracle.so" in libs and "libinputs.so" in libs
+    assert "libarc.so" not in libs and "libcuda" not in libs and "libcudart" not in libs and "libtorch" not in libs
