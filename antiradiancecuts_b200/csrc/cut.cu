@@ -622,18 +622,58 @@ __global__ void __launch_bounds__(64) cut_eval_kernel(EvalArgs a) {
 }
 
 // Cut evaluation with packed FP32 pairs (no or cone antiradiance): each thread (one pixel) takes
-// two cut nodes per step with f32x2 arithmetic.  The chunk's records are staged interleaved by
-// node pair: float pair * 32 + 2 f + h holds field f (0..15 of the packed record) of node
-// 2 pair + h, so one 16-byte shared load brings two fields of both nodes.  An odd chunk is padded
-// with a zero record, which contributes exactly 0.  Same terms as pair_terms; the even and odd
-// nodes' partial sums are added before the chunk's Kahan step.
+// two cut nodes per step with f32x2 arithmetic.  The records are staged 128 nodes at a time,
+// interleaved by node pair: float pair * 32 + 2 f + h holds field f (0..15 of the packed record)
+// of node 2 pair + h, so one 16-byte shared load brings two fields of both nodes.  Staging is
+// double-buffered with 4-byte cp.async copies straight into that layout: the copies of the next
+// 128 nodes (and the load of the node ids after them) are in flight while the current 128 are
+// evaluated.  An odd count is padded with a zero record, which contributes exactly 0.  Same terms
+// as pair_terms; the even and odd nodes' partial sums are added before each chunk's Kahan step.
 template <int AR>
 __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
-    constexpr int kChunk = 256;
-    __shared__ __align__(16) float srec[kChunk * 16];
+    constexpr int kSub = 128;  // nodes per stage; divides kChunkSize, so a stage never straddles two pool chunks
+    __shared__ __align__(16) float srec[2][kSub * 16];
     const int tile = a.order[blockIdx.x];
     const int i = threadIdx.x;
     const int x = (tile % a.tiles_x) * kTile + i % kTile, y = (tile / a.tiles_x) * kTile + i / kTile;
+    const int count = a.pool.counts[tile];
+    const int nsub = (count + kSub - 1) / kSub;
+    const int32_t* table = a.pool.tables + (size_t)tile * a.pool.max_chunks;
+    // this thread's two slots (i, i + 64) of stage s: node ids, or -1 past the end
+    auto ids_of = [&](int s, int& id0, int& id1) {
+        const int base = s * kSub;
+        const int cnt = min(kSub, count - base);
+        const int32_t* nodes = a.pool.entries + (size_t)table[base / kChunkSize] * kChunkSize + base % kChunkSize;
+        id0 = i < cnt ? nodes[i] : -1;
+        id1 = i + 64 < cnt ? nodes[i + 64] : -1;
+    };
+    // copies of stage s into buffer s & 1 (one cp.async group per thread); the pad slot of an odd
+    // count gets zeros
+    auto stage = [&](int s, int id0, int id1) {
+        const int cnt = min(kSub, count - s * kSub);
+        float* buf = srec[s & 1];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int nl = i + 64 * h, id = h ? id1 : id0;
+            float* d = buf + (nl >> 1) * 32 + (nl & 1);
+            if (id >= 0) {
+                const float* src = reinterpret_cast<const float*>(a.records + 4 * (size_t)id);
+#pragma unroll
+                for (int f = 0; f < 16; ++f) cp_async4(d + 2 * f, src + f);
+            } else if (nl == cnt && (cnt & 1)) {
+#pragma unroll
+                for (int f = 0; f < 16; ++f) d[2 * f] = 0.0f;
+            }
+        }
+        cp_async_commit();
+    };
+    int nid0 = -1, nid1 = -1;
+    if (nsub > 0) {
+        ids_of(0, nid0, nid1);
+        stage(0, nid0, nid1);
+    }
+    if (nsub > 1) ids_of(1, nid0, nid1);
+
     bool valid = x < a.width && y < a.height;
     float4 gp = make_float4(0, 0, 0, 0), gn = make_float4(0, 0, 0, 0);
     int mat = 0;
@@ -656,28 +696,22 @@ __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
     // distance floor folded into the FMA chain: l2 + 1e-30 equals max(l2, 1e-30) for l2 above ~1e-23
     const uint64_t kTiny2 = f2(1e-30f, 1e-30f);
     float ss[6] = {0, 0, 0, 0, 0, 0}, sc[6] = {0, 0, 0, 0, 0, 0};
-    const int count = a.pool.counts[tile];
-    for (int base = 0; base < count; base += kChunk) {
-        const int cnt = min(kChunk, count - base);
-        const int pairs = (cnt + 1) >> 1;
-        // kChunk divides kChunkSize: a sub-chunk never straddles two pool chunks
-        const int32_t* nodes = a.pool.entries + (size_t)a.pool.tables[(size_t)tile * a.pool.max_chunks + base / kChunkSize] *
-                                                    kChunkSize + base % kChunkSize;
+    for (int s = 0; s < nsub; ++s) {
+        // stage s has landed for every thread, and every thread is done with stage s - 1, whose
+        // buffer the next copies overwrite
+        cp_async_wait<0>();
         __syncthreads();
-        for (int j = i; j < pairs * 8; j += 64) {
-            const int nl = j >> 2, quad = j & 3;
-            const float4 q = nl < cnt ? a.records[4 * (size_t)nodes[nl] + quad] : make_float4(0, 0, 0, 0);
-            float* d = srec + (nl >> 1) * 32 + 8 * quad + (nl & 1);
-            d[0] = q.x;
-            d[2] = q.y;
-            d[4] = q.z;
-            d[6] = q.w;
+        if (s + 1 < nsub) {
+            stage(s + 1, nid0, nid1);
+            if (s + 2 < nsub) ids_of(s + 2, nid0, nid1);
         }
-        __syncthreads();
+        const int cnt = min(kSub, count - s * kSub);
+        const int pairs = (cnt + 1) >> 1;
+        const float* srs = srec[s & 1];
         uint64_t R0 = 0, R1 = 0, R2 = 0, A0 = 0, A1 = 0, A2 = 0;  // packed zeros
 #pragma unroll 2
         for (int pr = 0; pr < pairs; ++pr) {
-            const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(srec + pr * 32);
+            const ulonglong2* s2 = reinterpret_cast<const ulonglong2*>(srs + pr * 32);
             const ulonglong2 f01 = s2[0], f23 = s2[1], f45 = s2[2], f67 = s2[3], f89 = s2[4], f1011 = s2[5];
             const uint64_t dx = f2_add(f01.x, PX), dy = f2_add(f01.y, PY), dz = f2_add(f23.x, PZ);
             const uint64_t l2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_fma(dx, dx, kTiny2)));  // >= 1e-30

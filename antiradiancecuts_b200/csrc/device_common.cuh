@@ -97,6 +97,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// cp.async (global -> shared, 4 bytes, through L1): one thread's copies complete as a group.
+__device__ __forceinline__ void cp_async4(void* dst_smem, const void* src_gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst_smem)), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// waits until at most N of this thread's most recent groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // A CTA whose bounded wait on its ring of `stages` bulk-copy buffers gave up at chunk `fail_c`
 // may still have the copies of chunks fail_c .. fail_c + stages - 1 in flight (the issuing thread
 // refills a buffer only after its own wait succeeded).  The issuing thread calls this before the

@@ -218,6 +218,173 @@ def evaluate(ctx: api.Context, model: Model, feats, labels, delta: float = LABEL
             "refine_fraction": lab.float().mean().item(), **extra}
 
 
+# Scenes of the operating-point choice: neither the training seeds nor the evaluation seeds
+VALIDATION_SEEDS = tuple(range(164, 172))
+# Scenes the benchmark reports: the held-out evaluation scene (seed 500) and three more
+EVAL_SEEDS = (500, 501, 502, 503)
+
+
+def image_errors(img, ref, rad, ar) -> dict:
+    """Errors of an FP64 [pixels, 3] image against the all-FP64 image `ref` (whose radiance and
+    antiradiance planes are rad, ar): the max over channels of the relative RMSE, and the max over
+    surface pixels and channels of |img - ref| / (|rad| + |ar|) (the pixel's error relative to the
+    magnitude of the two sums that cancel in it)."""
+    img = np.asarray(img, np.float64).reshape(-1, 3)
+    ref = np.asarray(ref, np.float64).reshape(-1, 3)
+    scale = np.abs(np.asarray(rad, np.float64).reshape(-1, 3)) + np.abs(np.asarray(ar, np.float64).reshape(-1, 3))
+    d = np.abs(img - ref)
+    rms = float(np.max(np.sqrt(np.mean(d ** 2, 0)) / (np.sqrt(np.mean(ref ** 2, 0)) + 1e-300)))
+    live = scale > 0
+    mx = float(np.max(d[live] / scale[live])) if live.any() else 0.0
+    return {"rel_rmse": rms, "max_rel_err": mx}
+
+
+class EvalScene:
+    """One room variant (seed) at the evaluation scale on the GPU: its AVPLs in their own device
+    buffers, its LBVH, its G-buffer and its all-FP64 exact image (radiance, antiradiance and the
+    signed result), for timing cuts and scoring their images."""
+
+    def __init__(self, ctx: api.Context, seed: int, width=TRAIN_W, height=TRAIN_H, num_avpls=TRAIN_AVPLS,
+                 cone_half_angle_deg=30.0, dist_clamp=0.01):
+        import torch
+
+        self.ctx, self.seed = ctx, seed
+        self.desc = scene.scene_desc(L.ARC_SCENE_TRAIN_VARIANT, seed)
+        avpls, self.paths = scene.trace_avpls(self.desc, seed, num_avpls, 3)
+        pos, nrm = scene.gbuffer(self.desc, width, height)
+        self.width, self.height, self.num_avpls = width, height, num_avpls
+        self.surface_pixels = int((nrm[..., 3] > 0).sum())
+        self.mats, _, _, _ = scene.materials(self.desc)
+        self.cam = (self.desc.camera_position.x, self.desc.camera_position.y, self.desc.camera_position.z)
+        self.dv = api.DeviceAvpls(avpls)
+        self.gb = api.GBuffer(pos, nrm)
+        self.prm = api.gather_params(L.ARC_AR_CONE, cone_half_angle_deg, dist_clamp)
+        self.bvh = api.AvplBvh(ctx)
+        ctx.upload_materials(self.mats)
+        self.bvh.build(self.dv.param)
+        out64 = api.Outputs(width, height)
+        api.gather_bruteforce(ctx, self.dv.param, self.gb, self.cam,
+                              api.gather_params(L.ARC_AR_CONE, cone_half_angle_deg, dist_clamp,
+                                                precision=L.ARC_PREC_FP64), out64)
+        word = ctx.synchronize()
+        if word:
+            raise RuntimeError(f"device error word 0x{word:x} while rendering the FP64 image of scene {seed}")
+        self.ref = out64.result64.cpu().numpy().reshape(-1, 3)
+        self.rad = out64.radiance[..., :3].cpu().numpy().reshape(-1, 3)
+        self.ar = out64.antiradiance[..., :3].cpu().numpy().reshape(-1, 3)
+        self.out = api.Outputs(width, height)
+        self.tiles = ((width + 7) // 8) * ((height + 7) // 8)
+        del out64
+        torch.cuda.synchronize()
+
+    def _time(self, fn, reps: int) -> float:
+        import torch
+
+        self.ctx.upload_materials(self.mats)
+        fn()  # warm-up
+        word = self.ctx.synchronize()
+        if word:
+            raise RuntimeError(f"device error word 0x{word:x} on scene {self.seed}")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.ctx.stream)
+        for _ in range(reps):
+            fn()
+        e1.record(self.ctx.stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def cut(self, cut, reps: int = 2) -> dict:
+        """One frame of the cut gather (LBVH build + selection + evaluation): ms per frame, mean
+        nodes per tile and the image's errors."""
+        def frame():
+            self.bvh.build(self.dv.param)
+            api.gather_cut(self.ctx, self.bvh, None, self.gb, self.cam, self.prm, cut, self.out)
+
+        ms = self._time(frame, reps)
+        nodes = float(api.cut_counts(self.ctx).mean())
+        err = image_errors(self.out.result64.cpu().numpy(), self.ref, self.rad, self.ar)
+        return {"ms": ms, "nodes_per_tile": nodes, **err}
+
+    def exact(self, reps: int = 1) -> dict:
+        """The exact brute-force gather (default precision): ms per frame and its errors."""
+        ms = self._time(lambda: api.gather_bruteforce(self.ctx, self.dv.param, self.gb, self.cam, self.prm,
+                                                       self.out), reps)
+        return {"ms": ms, **image_errors(self.out.result64.cpu().numpy(), self.ref, self.rad, self.ar)}
+
+    def close(self):
+        self.bvh.close()
+
+
+def sweep(scenes, model: Model | None, values, pool_per_tile: int = 65536) -> list[list[dict]]:
+    """For each value, each scene's cut result: the learned cut at that threshold (model given) or
+    the analytic error-bound cut at that bound (model None)."""
+    res = []
+    for v in values:
+        row = []
+        for sc in scenes:
+            pool = sc.tiles * pool_per_tile
+            if model is not None:
+                cp = cut_params(model, threshold=v, cut_pool_entries=pool)
+            else:
+                cp = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=v, ar_uncertain_factor=PREACCEPT_K,
+                                    cut_pool_entries=pool)
+            row.append(sc.cut(cp, reps=1))
+        res.append(row)
+    return res
+
+
+def choose(values, results, target: float, larger_is_faster: bool = True):
+    """The fastest value whose worst scene stays within `target` relative RMSE (None if none)."""
+    ok = [(v, r) for v, r in zip(values, results) if max(x["rel_rmse"] for x in r) <= target]
+    if not ok:
+        return None
+    return max(ok, key=lambda vr: vr[0])[0] if larger_is_faster else min(ok, key=lambda vr: vr[0])[0]
+
+
+THRESHOLDS = (0.01, 0.02, 0.03, 0.05, 0.07, 0.1, 0.15, 0.2, 0.3)
+ANALYTIC_BOUNDS = (0.001, 0.0015, 0.002, 0.0025, 0.003, 0.004)
+CALIBRATION_TARGET = 0.0095  # the worst validation scene's relative RMSE: 1% with a margin
+
+
+def calibrate(ctx: api.Context, model_paths, seeds=VALIDATION_SEEDS, target=CALIBRATION_TARGET, log=print) -> dict:
+    """Operating points chosen on the validation scenes only: for every candidate model its
+    threshold (the largest within `target` on every validation scene) and mean frame time there;
+    the analytic cut's error bound likewise.  The candidate with the fastest calibrated frame wins."""
+    t0 = time.time()
+    scenes = []
+    for s in seeds:
+        scenes.append(EvalScene(ctx, s))
+        log(f"validation scene {s}: {scenes[-1].surface_pixels} surface pixels ({time.time() - t0:.1f} s)")
+    report = {"seeds": list(seeds), "target_rel_rmse": target, "candidates": []}
+    an = sweep(scenes, None, ANALYTIC_BOUNDS)
+    eps = choose(ANALYTIC_BOUNDS, an, target, larger_is_faster=True)
+    report["analytic"] = {"error_bounds": list(ANALYTIC_BOUNDS), "chosen": eps,
+                          "worst_rel_rmse": [max(x["rel_rmse"] for x in r) for r in an],
+                          "mean_ms": [float(np.mean([x["ms"] for x in r])) for r in an]}
+    log(f"analytic: bound {eps} ({time.time() - t0:.1f} s)")
+    best = None
+    for path in model_paths:
+        m = Model.load(ctx, path)
+        res = sweep(scenes, m, THRESHOLDS)
+        thr = choose(THRESHOLDS, res, target, larger_is_faster=True)
+        worst = [max(x["rel_rmse"] for x in r) for r in res]
+        mean_ms = [float(np.mean([x["ms"] for x in r])) for r in res]
+        cand = {"model": os.path.basename(path), "band": m.band, "threshold": thr, "worst_rel_rmse": worst,
+                "mean_ms": mean_ms, "thresholds": list(THRESHOLDS)}
+        if thr is not None:
+            cand["calibrated_mean_ms"] = mean_ms[THRESHOLDS.index(thr)]
+            if best is None or cand["calibrated_mean_ms"] < best["calibrated_mean_ms"]:
+                best = cand
+        report["candidates"].append(cand)
+        log(f"{os.path.basename(path)}: threshold {thr}, worst rel RMSE {worst}, ms {mean_ms} "
+            f"({time.time() - t0:.1f} s)")
+        m.close()
+    report["chosen"] = best
+    for sc in scenes:
+        sc.close()
+    return report
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -230,10 +397,33 @@ def main(argv=None):
     tr.add_argument("--band", type=float, default=PREACCEPT_BAND)
     tr.add_argument("--threshold", type=float, default=None, help="selection threshold stored with the model")
     tr.add_argument("--out", default=DEFAULT_MODEL)
+    ca = sub.add_parser("calibrate", help="choose the operating point on the validation scenes")
+    ca.add_argument("models", nargs="+", help="candidate model archives (band and delta differ)")
+    ca.add_argument("--target", type=float, default=CALIBRATION_TARGET)
+    ca.add_argument("--report", default=None, help="write the JSON report here")
+    ca.add_argument("--install", default=None, help="save the chosen model with its threshold here")
     a = ap.parse_args(argv)
     import torch
 
     ctx = api.Context(0)
+    if a.cmd == "calibrate":
+        import json
+
+        rep = calibrate(ctx, a.models, target=a.target, log=lambda m: print(m, flush=True))
+        if a.report:
+            with open(a.report, "w") as f:
+                json.dump(rep, f, indent=1)
+        ch = rep["chosen"]
+        if ch is None:
+            print("no candidate stays within the target on every validation scene")
+            return 1
+        if a.install:
+            src = [p for p in a.models if os.path.basename(p) == ch["model"]][0]
+            m = Model.load(ctx, src)
+            m.threshold = ch["threshold"]
+            m.save(a.install)
+            print("installed", ch["model"], "threshold", ch["threshold"], "->", a.install)
+        return 0
     regress = a.objective == "regression"
     per_scene = max(1, a.samples // a.scenes)
     fs, ls = [], []

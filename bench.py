@@ -42,6 +42,18 @@ FLOP_PER_PAIR = {0: 30, 1: 54, 2: 43}
 FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64)
 
 
+CALIBRATION = os.path.join(ROOT, "antiradiancecuts_b200", "models", "cutnet_calibration.json")
+
+
+def calibrated_error_bound(default: float = 0.002) -> float:
+    """The analytic cut's error bound chosen on the validation scenes (learned.calibrate)."""
+    try:
+        v = json.load(open(CALIBRATION))["analytic"]["chosen"]
+        return float(v) if v is not None else default
+    except (OSError, KeyError, ValueError):
+        return default
+
+
 def lbvh_bytes_per_avpl() -> dict:
     """Compulsory DRAM bytes per AVPL of each LBVH kernel (reads + writes of its inputs and
     outputs once, N leaves and N - 1 inner nodes)."""
@@ -319,6 +331,35 @@ def clustered_leg(ctx, api, scene, L, desc, mats, dv, gb, cam, stream) -> dict:
             "list_entries": int(info.list_entries), "rel_rmse_vs_bruteforce": rel}
 
 
+def seeds_leg(ctx, model, error_bound: float, seeds) -> dict:
+    """The headline comparison on more than one scene: for each room variant seed at 1920x1080 with
+    1,048,576 AVPLs, the learned cut (the model's calibrated threshold), the analytic cut (at its
+    calibrated bound) and the exact brute-force gather, each timed on the GPU and scored against
+    the scene's all-FP64 image (relative RMSE and max relative error).  The operating points were
+    chosen on other scenes (the validation seeds), so none of these is a tuning scene."""
+    from antiradiancecuts_b200 import api, learned
+
+    rows = []
+    for s in seeds:
+        sc = learned.EvalScene(ctx, s)
+        pool = sc.tiles * 65536
+        lc = sc.cut(learned.cut_params(model, cut_pool_entries=pool), reps=3) if model is not None else None
+        an = sc.cut(api.cut_params(api.L.ARC_CUT_ERROR_BOUND, error_bound=error_bound,
+                                   ar_uncertain_factor=learned.PREACCEPT_K, cut_pool_entries=pool), reps=2)
+        ex = sc.exact(reps=1)
+        row = {"seed": s, "surface_pixels": sc.surface_pixels, "exact": ex, "analytic": an}
+        if lc is not None:
+            row["learned"] = lc
+            row["speedup_learned_vs_exact"] = ex["ms"] / lc["ms"]
+        row["speedup_analytic_vs_exact"] = ex["ms"] / an["ms"]
+        rows.append(row)
+        sc.close()
+        del sc
+    return {"scenes": rows, "analytic_error_bound": error_bound,
+            "mlp_threshold": model.threshold if model is not None else None,
+            "all_learned_within_1pct": all(r["learned"]["rel_rmse"] <= 0.01 for r in rows) if model else None}
+
+
 def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
     """Multi-view batch: views of the room + 2 boxes scene drawn with seed 4 (resolutions from
     {256^2, 512^2, 1280x720, 1920x1080}, 8,192 - 262,144 AVPLs each, log-uniform, camera inside the
@@ -415,7 +456,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="variant500_1080p_1m")
     ap.add_argument("--method", default="auto", choices=["auto", "learned", "error_bound"])
-    ap.add_argument("--error-bound", type=float, default=0.002, help="analytic cut (error_bound method)")
+    ap.add_argument("--error-bound", type=float, default=None,
+                    help="analytic cut bound (default: the one calibrated on the validation scenes)")
+    ap.add_argument("--seeds", default="500,501,502,503", help="scenes of the per-scene comparison ('' = none)")
     ap.add_argument("--small", action="store_true", help="640x360 / 262,144 AVPLs, no extras (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip exact / FP64 / CPU legs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="all-core CPU baseline sample")
@@ -424,6 +467,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.error_bound is None:
+        args.error_bound = calibrated_error_bound()
 
     import torch
 
@@ -652,7 +697,10 @@ def main():
                            ref64=ref64, single_s=args.cpu_single_seconds)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
-    batch = gen = post = clus = None
+    batch = gen = post = clus = seeds = None
+    if not args.no_extras and args.seeds:
+        seeds = seeds_leg(ctx, model, args.error_bound, [int(x) for x in args.seeds.split(",")])
+        ctx.upload_materials(mats)
     if not args.no_extras:
         batch = batch_leg(ctx, api, scene, L, stream, args.batch_views)
         gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
@@ -677,7 +725,7 @@ def main():
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
             "cpu_baseline": cpu, "clocks": clk, "batch": batch, "scene_generation": gen, "post": post,
-            "clustered_antiradiance": clus,
+            "clustered_antiradiance": clus, "scenes": seeds,
         }
         if method != "learned" and args.method == "auto":
             line["config"]["learned_unavailable"] = model_error[:200]

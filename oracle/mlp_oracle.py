@@ -88,15 +88,23 @@ def bf16(x):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def forward_bf16(p, x):
+def gelu_half_tanh(x):
+    """GELU with its tanh taken in BF16: the argument and the tanh rounded to BF16 (the learned cut
+    selection's tanh.approx.bf16x2)."""
+    return 0.5 * x * (1.0 + bf16(np.tanh(bf16(_A * (x + _B * x ** 3)))))
+
+
+def forward_bf16(p, x, half_tanh=False):
     """The network with the tensor-core kernels' rounding points: BF16 inputs, weights W1..W3 and
-    hidden activations h1, h2; FP64 otherwise (accumulation, biases, GELU, the 64 -> 1 layer)."""
+    hidden activations h1, h2; FP64 otherwise (accumulation, biases, GELU, the 64 -> 1 layer).
+    half_tanh: the activations' tanh in BF16, as the learned cut's selection evaluates it."""
     P = unpack(p)
+    act = gelu_half_tanh if half_tanh else gelu
     h = bf16(x)
     z1 = h @ bf16(P["W1"]).T + P["b1"]
-    h1 = bf16(gelu(z1))
+    h1 = bf16(act(z1))
     z2 = h1 @ bf16(P["W2"]).T + P["b2"]
-    h2 = bf16(gelu(z2))
+    h2 = bf16(act(z2))
     z3 = h2 @ bf16(P["W3"]).T + P["b3"]
-    h3 = gelu(z3)
+    h3 = act(z3)
     return h3 @ P["w4"] + P["b4"][0]
