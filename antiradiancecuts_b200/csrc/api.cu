@@ -192,6 +192,8 @@ arc_status arc_context_create(int32_t device, void* cuda_stream, arc_context** o
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_error, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(ctx->d_error, 0, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_materials, sizeof(MaterialRecord) * ARC_MAX_MATERIALS);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_learned_rows, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_learned_rows, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
         set_last_error(std::string("context creation: ") + cudaGetErrorString(e));
@@ -211,6 +213,7 @@ arc_status arc_context_destroy(arc_context* ctx) {
     for (auto e : ctx->timer.end) cudaEventDestroy(e);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_materials) cudaFree(ctx->d_materials);
+    if (ctx->d_learned_rows) cudaFree(ctx->d_learned_rows);
     for (int i = 0; i < 2; ++i) {
         if (ctx->h_staging[i]) cudaFreeHost(ctx->h_staging[i]);
         if (ctx->staged[i]) cudaEventDestroy(ctx->staged[i]);
@@ -265,7 +268,15 @@ arc_status arc_context_stage_times(arc_context* ctx, char* names, size_t names_l
 
 uint64_t arc_context_launch_count(arc_context* ctx) { return ctx ? ctx->launches : 0; }
 
-uint64_t arc_context_learned_rows(arc_context* ctx) { return ctx ? ctx->learned_rows : 0; }
+uint64_t arc_context_learned_rows(arc_context* ctx) {
+    if (!ctx || !ctx->d_learned_rows) return 0;
+    unsigned long long rows = 0;
+    if (cudaSetDevice(ctx->device) != cudaSuccess ||
+        cudaMemcpyAsync(&rows, ctx->d_learned_rows, sizeof(rows), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return 0;
+    return rows;
+}
 
 arc_status arc_device_alloc(arc_context* ctx, size_t bytes, void** out) {
     ARC_CHECK_ARG(ctx && out, "NULL argument");

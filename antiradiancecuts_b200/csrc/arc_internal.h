@@ -130,7 +130,7 @@ struct arc_context {
     arc_lbvh* run_bvh = nullptr;  // tree rebuilt by arc_run every frame
     arc::StageTimer timer;
     uint64_t launches = 0;  // kernels launched by this context
-    uint64_t learned_rows = 0;  // rows scored by the cut network so far
+    unsigned long long* d_learned_rows = nullptr;  // rows scored by the cut network so far (device counter)
     int32_t bf_tile_config = -1;  // brute-force launch shape for tile_config = -1 (arc_autotune_bruteforce)
 };
 

@@ -373,7 +373,8 @@ __global__ void cut_node_extra(int n, const float4* bounds, const float4* record
     const float4 q2 = records[4 * ((size_t)n + k) + 2], q3 = records[4 * ((size_t)n + k) + 3];
     const float rn = half_diagonal(rn_sub(b1.x, b0.x), rn_sub(b1.y, b0.y), rn_sub(b1.z, b0.z));
     ext[2 * (size_t)k] = make_float4(rn, cone_sine(nc.w), cone_sine(wc.w), lum3(q2.y, q2.z, q2.w));
-    ext[2 * (size_t)k + 1] = make_float4(lum3(q3.x, q3.y, q3.z), 0.0f, 0.0f, 0.0f);
+    ext[2 * (size_t)k + 1] = make_float4(lum3(q3.x, q3.y, q3.z), rn_mul(0.5f, rn_add(b0.x, b1.x)),
+                                         rn_mul(0.5f, rn_add(b0.y, b1.y)), rn_mul(0.5f, rn_add(b0.z, b1.z)));
 }
 
 __device__ __forceinline__ TileInfo load_tile(const float4* info, int tile) {

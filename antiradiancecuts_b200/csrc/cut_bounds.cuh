@@ -27,12 +27,13 @@ struct NodeExtra {
     float swc;  // sine of the direction cone's half-angle
     float Ls;   // luminance of the summed radiance
     float As;   // luminance of the summed antiradiance
+    float cn[3];  // centre of the node's box, 0.5 (bmin + bmax)
 };
 
-// two float4 per inner node: {rn, snc, swc, Ls}, {As, 0, 0, 0}
+// two float4 per inner node: {rn, snc, swc, Ls}, {As, centre}
 __device__ __forceinline__ NodeExtra load_node_extra(const float4* ext, int k) {
     const float4 e0 = ext[2 * (size_t)k], e1 = ext[2 * (size_t)k + 1];
-    return NodeExtra{e0.x, e0.y, e0.z, e0.w, e1.x};
+    return NodeExtra{e0.x, e0.y, e0.z, e0.w, e1.x, {e1.y, e1.z, e1.w}};
 }
 
 struct BoundParams {
@@ -112,9 +113,8 @@ __device__ __forceinline__ NodeGeom node_geom(const TileInfo& t, float4 b0, floa
     float v[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const float cn = rn_mul(0.5f, rn_add(bmin[k], bmax[k]));
         const float ct = rn_mul(0.5f, rn_add(t.tmin[k], t.tmax[k]));
-        v[k] = rn_sub(ct, cn);
+        v[k] = rn_sub(ct, ne.cn[k]);
     }
     const float dc = rn_sqrt(rn_dot(v[0], v[1], v[2], v[0], v[1], v[2]));
     const float rn = ne.rn;

@@ -809,7 +809,6 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     int2 *fa, *fb;
     int2* accepted;
     int *counters, *tile_counts, *chunk_base, *fill;
-    unsigned long long* rows_scored;
     ARC_TRY(arena_get(ctx, "lc_front_a", cap, &fa));
     ARC_TRY(arena_get(ctx, "lc_front_b", cap, &fb));
     ARC_TRY(arena_get(ctx, "lc_accepted", acc_cap, &accepted));
@@ -817,12 +816,10 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     constexpr int kMaxLevels = 96;
     constexpr int kSlots = 8 + 4 * (kMaxLevels + 1);
     ARC_TRY(arena_get(ctx, "lc_counters", kSlots, &counters));
-    ARC_TRY(arena_get(ctx, "lc_rows", 1, &rows_scored));
     ARC_TRY(arena_get(ctx, "lc_tile_counts", tiles, &tile_counts));
     ARC_TRY(arena_get(ctx, "lc_chunk_base", tiles, &chunk_base));
     ARC_TRY(arena_get(ctx, "lc_fill", tiles, &fill));
     ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * kSlots, st));
-    ARC_TRY_CUDA(cudaMemsetAsync(rows_scored, 0, sizeof(unsigned long long), st));
     ARC_TRY_CUDA(cudaMemsetAsync(tile_counts, 0, sizeof(int) * tiles, st));
     ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * tiles, st));
 
@@ -837,7 +834,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.extra = extra;
     la.bp = bound_params(gp, cp);
     la.capacity = cap;
-    la.rows_scored = rows_scored;
+    la.rows_scored = ctx->d_learned_rows;
     unsigned char* img;
     ARC_TRY(arena_get(ctx, "lc_weight_image", mlp::kImageBytes, &img));
     la.weight_image = img;
@@ -870,38 +867,24 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, counters + 8, info, tiles, n);
     kernels += 2;
     int2 *cur = fa, *nxt = fb;
-    // the frontier size is read back every kCheck levels; launches past the last level return
-    // at once
-    constexpr int kCheck = 6;
-    int level = 0;
-    bool empty = false;
-    while (level < kMaxLevels && !empty) {
-        const int upto = std::min(kMaxLevels, level + kCheck);
-        for (; level < upto; ++level) {
-            la.in = cur;
-            la.in_count = counters + 8 + 4 * level;
-            la.work = counters + 8 + 4 * level + 2;
-            la.out = nxt;
-            la.out_count = counters + 8 + 4 * (level + 1);
-            learned_level<<<ctx->sm_count * per_sm, kLevelThreads, kLevelSmem, st>>>(la);
-            ++kernels;
-            std::swap(cur, nxt);
-        }
-        int host_count = 0;
-        ARC_TRY_CUDA(cudaMemcpyAsync(&host_count, counters + 8 + 4 * level, sizeof(int), cudaMemcpyDeviceToHost, st));
-        ARC_TRY_CUDA(cudaStreamSynchronize(st));
-        empty = host_count == 0;
-    }
-    if (!empty) {  // deeper than the walk goes: accept what is left
+    // Every level up to kMaxLevels is launched without reading anything back: a launch past the
+    // tree's last level finds an empty frontier and returns at once, so the selection holds no
+    // host synchronisation and can be recorded into a CUDA graph.  Pairs still in the frontier
+    // after the last launch (a tree deeper than kMaxLevels) are accepted.
+    for (int level = 0; level < kMaxLevels; ++level) {
         la.in = cur;
         la.in_count = counters + 8 + 4 * level;
-        accept_frontier<<<grid, 256, 0, st>>>(la);
+        la.work = counters + 8 + 4 * level + 2;
+        la.out = nxt;
+        la.out_count = counters + 8 + 4 * (level + 1);
+        learned_level<<<ctx->sm_count * per_sm, kLevelThreads, kLevelSmem, st>>>(la);
         ++kernels;
+        std::swap(cur, nxt);
     }
-    unsigned long long rows = 0;
-    ARC_TRY_CUDA(cudaMemcpyAsync(&rows, rows_scored, sizeof(rows), cudaMemcpyDeviceToHost, st));
-    ARC_TRY_CUDA(cudaStreamSynchronize(st));
-    ctx->learned_rows += (int64_t)rows;
+    la.in = cur;
+    la.in_count = counters + 8 + 4 * kMaxLevels;
+    accept_frontier<<<grid, 256, 0, st>>>(la);
+    ++kernels;
     ScatterArgs sa;
     sa.accepted = accepted;
     sa.acc_count = counters + 3;

@@ -331,6 +331,54 @@ def clustered_leg(ctx, api, scene, L, desc, mats, dv, gb, cam, stream) -> dict:
             "list_entries": int(info.list_entries), "rel_rmse_vs_bruteforce": rel}
 
 
+# compulsory DRAM bytes per AVPL of an LBVH build (the survey's minimum: bbox read 12, Morton 16,
+# sort 4 passes x 16 with histograms, payload permute 128, Karras writes 12, bottom-up 204)
+LBVH_MIN_BYTES_PER_AVPL = 470
+
+
+def lbvh_sweep_leg(ctx, api, scene, L, desc, sizes, hbm_gbs: float, stream) -> dict:
+    """LBVH build time per stage at several AVPL counts (AVPLs made by the GPU light tracer), with
+    the achieved bandwidth against both the survey's compulsory 470 B/AVPL and this design's
+    itemised bytes (lbvh_bytes_per_avpl)."""
+    import torch
+
+    design = sum(lbvh_bytes_per_avpl().values())
+    names = C.create_string_buffer(4096)
+    st_ms = (C.c_float * 256)()
+    nst = C.c_int32()
+    rows = []
+    for n in sizes:
+        dv, _ = scene.trace_avpls_device(ctx, desc, 7, n, 3)
+        bvh = api.AvplBvh(ctx)
+        bvh.build(dv.param)  # warm-up (sizes the arena)
+        assert ctx.synchronize() == 0
+        reps = 3
+        ctx.lib.arc_context_profile(ctx.handle, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            bvh.build(dv.param)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        ctx.lib.arc_context_stage_times(ctx.handle, names, 4096, st_ms, 256, C.byref(nst))
+        ctx.lib.arc_context_profile(ctx.handle, 0)
+        stages = {}
+        for nme, v in zip(names.value.decode().split(","), list(st_ms)[: nst.value]):
+            stages[nme] = stages.get(nme, 0.0) + v / reps
+        assert ctx.synchronize() == 0
+        gbs_min = LBVH_MIN_BYTES_PER_AVPL * n / (ms * 1e-3) / 1e9
+        gbs_design = design * n / (ms * 1e-3) / 1e9
+        rows.append({"avpls": n, "ms": ms, "stage_ms": stages,
+                     "achieved_gbs_at_470_b": gbs_min, "frac_at_470_b": gbs_min / hbm_gbs,
+                     "achieved_gbs_at_design_b": gbs_design, "frac_at_design_b": gbs_design / hbm_gbs})
+        bvh.close()
+        del dv
+        torch.cuda.empty_cache()
+    return {"sizes": rows, "bytes_per_avpl_min": LBVH_MIN_BYTES_PER_AVPL, "bytes_per_avpl_design": design,
+            "peak_gbs": hbm_gbs, "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+
+
 def seeds_leg(ctx, model, error_bound: float, seeds) -> dict:
     """The headline comparison on more than one scene: for each room variant seed at 1920x1080 with
     1,048,576 AVPLs, the learned cut (the model's calibrated threshold), the analytic cut (at its
@@ -606,7 +654,9 @@ def main():
     lb_bytes = sum(lbvh_bytes_per_avpl().values()) * N
     lbvh_roof = {"achieved": lb_bytes / (lb_ms * 1e-3) / 1e9 if lb_ms else None, "peak": peaks["hbm_gbs"],
                  "unit": "GB/s", "frac": (lb_bytes / (lb_ms * 1e-3) / 1e9) / peaks["hbm_gbs"] if lb_ms else None,
-                 "ms": lb_ms, "bytes_per_avpl": sum(lbvh_bytes_per_avpl().values())}
+                 "ms": lb_ms, "bytes_per_avpl": sum(lbvh_bytes_per_avpl().values()),
+                 "frac_at_470_b": (LBVH_MIN_BYTES_PER_AVPL * N / (lb_ms * 1e-3) / 1e9) / peaks["hbm_gbs"]
+                 if lb_ms else None}
 
     result = {}
     cut_img = out.result64.cpu().numpy().reshape(-1, 3).copy()
@@ -697,7 +747,7 @@ def main():
                            ref64=ref64, single_s=args.cpu_single_seconds)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
-    batch = gen = post = clus = seeds = None
+    batch = gen = post = clus = seeds = sweep = None
     if not args.no_extras and args.seeds:
         seeds = seeds_leg(ctx, model, args.error_bound, [int(x) for x in args.seeds.split(",")])
         ctx.upload_materials(mats)
@@ -706,6 +756,8 @@ def main():
         gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
         post = post_leg(ctx, api, L, out, stream, lbvh_roof["peak"])
         clus = clustered_leg(ctx, api, scene, L, desc, mats, dv, gb, cam, stream)
+        sweep = lbvh_sweep_leg(ctx, api, scene, L, desc, (1 << 20, 1 << 22, 1 << 24), lbvh_roof["peak"], stream)
+        ctx.upload_materials(mats)
 
     if rank == 0:
         line = {
@@ -725,7 +777,7 @@ def main():
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(68 * N),
                     "d2h_bytes_per_step": int(W * H * 16)},
             "cpu_baseline": cpu, "clocks": clk, "batch": batch, "scene_generation": gen, "post": post,
-            "clustered_antiradiance": clus, "scenes": seeds,
+            "clustered_antiradiance": clus, "scenes": seeds, "lbvh_sweep": sweep,
         }
         if method != "learned" and args.method == "auto":
             line["config"]["learned_unavailable"] = model_error[:200]

@@ -494,17 +494,22 @@ typedef struct ArcBatchView {
 
 typedef struct arc_batch arc_batch;
 
-/* A batch renderer on `ctx`: it owns one LBVH that every view's build reuses in turn. */
+/* A batch renderer on `ctx`.  It owns four lanes -- sub-contexts on the same device, each with its
+ * own stream, scratch arena, LBVH and error word -- that render their share of a batch's views
+ * concurrently, so that views of uneven sizes share the GPU.  The lanes copy `ctx`'s material
+ * table before each render. */
 arc_status arc_batch_create(arc_context* ctx, arc_batch** out);
 arc_status arc_batch_destroy(arc_batch* batch);
-/* Per view, in order, on the context's stream: the LBVH build of its AVPLs (`lbvh`) and the cut
- * gather (`cut`; SOLID_ANGLE, ERROR_BOUND or LEARNED) into its outputs.  Enqueued only. */
+/* Per view, the LBVH build of its AVPLs (`lbvh`, default wait limit) and the cut gather (`cut`;
+ * SOLID_ANGLE, ERROR_BOUND or LEARNED) into its outputs.  The views are dealt to the lanes longest
+ * first (estimated work: pixels x log2 AVPLs); the lanes fork from the context's stream and join
+ * back into it, folding their device error words into the context's.  Enqueued only. */
 arc_status arc_batch_render(arc_batch* batch, const ArcBatchView* views, int32_t num_views, const ArcLbvhParams* lbvh,
                             const ArcGatherParams* gather, const ArcCutParams* cut);
 /* Records arc_batch_render of these views into one CUDA graph: it first renders them once eagerly
- * (sizing every library buffer), then captures the same work from the context's stream.  The views'
- * buffers must stay valid and in place while the graph is used.  ERROR_BOUND cuts only (the learned
- * selection reads its frontier size on the host).  Replaces any previously recorded graph. */
+ * (sizing every library buffer), then captures the same work -- every lane, the fork and the join --
+ * from the context's stream.  The views' buffers must stay valid and in place while the graph is
+ * used.  ERROR_BOUND and LEARNED cuts.  Replaces any previously recorded graph. */
 arc_status arc_batch_capture(arc_batch* batch, const ArcBatchView* views, int32_t num_views,
                              const ArcLbvhParams* lbvh, const ArcGatherParams* gather, const ArcCutParams* cut);
 /* Replays the recorded graph on the context's stream: the whole batch in one launch.  Enqueued

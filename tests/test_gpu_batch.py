@@ -82,15 +82,57 @@ def test_batch_equals_individual_views_and_graph_replays_it(ctx, views):
     batch.close()
 
 
-def test_learned_cuts_cannot_be_recorded(ctx, views):
+def test_learned_cuts_record_and_replay(ctx, views):
+    """The learned selection reads nothing back on the host, so a batch of learned cuts records into
+    one graph; its images equal each view rendered on its own (up to the order in which a tile's
+    accepted nodes are summed, which the selection's atomics leave open)."""
+    from antiradiancecuts_b200 import learned
+
+    model = learned.load_default_model(ctx)
     lp, gp, _ = _params()
-    v = views[0]
-    out = api.Outputs(v["w"], v["h"])
-    arr = api.Batch.views([(v["avpls"], v["gb"], v["cam"], out)])
+    cp = learned.cut_params(model)
+    ref = []
+    for v in views:
+        bvh = api.AvplBvh(ctx)
+        L.check(ctx.lib.arc_lbvh_build(bvh.handle, C.byref(v["avpls"]), C.byref(lp)), "build")
+        out = api.Outputs(v["w"], v["h"])
+        api.gather_cut(ctx, bvh, v["avpls"], v["gb"], v["cam"], gp, cp, out)
+        assert ctx.synchronize() == 0
+        ref.append(out.result64.cpu().numpy().copy())
+        bvh.close()
+    outs = [api.Outputs(v["w"], v["h"]) for v in views]
+    arr = api.Batch.views([(v["avpls"], v["gb"], v["cam"], o) for v, o in zip(views, outs)])
     batch = api.Batch(ctx)
-    st = ctx.lib.arc_batch_capture(batch.handle, arr, 1, C.byref(lp), C.byref(gp),
-                                   C.byref(api.cut_params(L.ARC_CUT_LEARNED)))
-    assert st == L.ARC_ERR_INVALID_ARG
+    batch.capture(arr, lp, gp, cp)
+    assert ctx.synchronize() == 0
+    for _ in range(2):
+        for o in outs:
+            o.result64.zero_()
+        batch.launch()
+        assert ctx.synchronize() == 0
+        for o, r in zip(outs, ref):
+            assert H.rel_rmse(o.result64.cpu().numpy(), r) < 1e-6
+    batch.close()
+    model.close()
+
+
+def test_device_errors_of_a_lane_reach_the_batch(ctx, views):
+    """A view whose G-buffer names a material past the table: the lane that renders it reports
+    ARC_DEVERR_BAD_MATERIAL into the owner context's error word."""
+    lp, gp, cp = _params()
+    v = views[1]
+    nrm = v["gb"].nrm.clone()
+    nrm[0, 0, 3] = 60.0
+    gb = api.GBuffer(None, None, size=(v["w"], v["h"]))
+    gb.pos.copy_(v["gb"].pos)
+    gb.nrm.copy_(nrm)
+    out = api.Outputs(v["w"], v["h"])
+    arr = api.Batch.views([(v["avpls"], gb, v["cam"], out)])
+    batch = api.Batch(ctx)
+    batch.render(arr, lp, gp, cp)
+    assert ctx.synchronize() & L.ARC_DEVERR_BAD_MATERIAL
+    batch.render(api.Batch.views([(v["avpls"], v["gb"], v["cam"], out)]), lp, gp, cp)
+    assert ctx.synchronize() == 0  # the lane's word was cleared when it was folded in
     batch.close()
 
 
