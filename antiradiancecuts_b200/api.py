@@ -457,9 +457,58 @@ def lbvh_params(**kw) -> L.ArcLbvhParams:
     return p
 
 
+class TuningCache:
+    """Brute-force launch shapes chosen by the autotuner, keyed by the workload (width, height,
+    AVPL count, antiradiance kind, precision), kept in a JSON file (shipped beside the cut network
+    as models/autotune.json) so that a later process applies a shape without timing again."""
+
+    def __init__(self, path: str | None = None):
+        import json
+        import os
+
+        self.path = path
+        self.entries: dict[str, dict] = {}
+        if path and os.path.exists(path):
+            with open(path) as f:
+                self.entries = json.load(f).get("bruteforce", {})
+
+    @staticmethod
+    def key(width: int, height: int, num_avpls: int, ar_kind: int, precision: int) -> str:
+        return f"{width}x{height}x{num_avpls}:ar{ar_kind}:prec{precision}"
+
+    def get(self, key: str) -> int | None:
+        e = self.entries.get(key)
+        return int(e["tile_config"]) if e is not None else None
+
+    def put(self, key: str, tile_config: int, times_ms) -> None:
+        self.entries[key] = {"tile_config": int(tile_config), "times_ms": [round(float(t), 3) for t in times_ms]}
+
+    def save(self, path: str | None = None) -> None:
+        import json
+
+        with open(path or self.path, "w") as f:
+            json.dump({"bruteforce": self.entries}, f, indent=1, sort_keys=True)
+
+
 def autotune_bruteforce(ctx: Context, avpls: L.ArcAvplsGpuParam, gb: GBuffer, cam, params: L.ArcGatherParams,
-                        out: Outputs) -> tuple[int, np.ndarray]:
-    """arc_autotune_bruteforce: (chosen tile_config, time of every shape in ms)."""
+                        out: Outputs, cache: TuningCache | None = None) -> tuple[int, np.ndarray]:
+    """arc_autotune_bruteforce: (chosen tile_config, time of every shape in ms).  With a cache that
+    holds this workload's shape, the shape is applied as the context default without timing (times
+    then come from the cache)."""
+    if cache is not None:
+        key = TuningCache.key(gb.width, gb.height, avpls.numAvpls, params.ar_kind, params.precision)
+        hit = cache.get(key)
+        if hit is not None and 0 <= hit < ctx.lib.arc_bruteforce_num_tile_shapes():
+            L.check(ctx.lib.arc_context_set_tile_config(ctx.handle, hit), "arc_context_set_tile_config")
+            return hit, np.asarray(cache.entries[key]["times_ms"], np.float32)
+    best, times = _autotune(ctx, avpls, gb, cam, params, out)
+    if cache is not None:
+        cache.put(key, best, times)
+    return best, times
+
+
+def _autotune(ctx: Context, avpls: L.ArcAvplsGpuParam, gb: GBuffer, cam, params: L.ArcGatherParams,
+              out: Outputs) -> tuple[int, np.ndarray]:
     n = ctx.lib.arc_bruteforce_num_tile_shapes()
     times = np.zeros(n, np.float32)
     best = C.c_int32()

@@ -692,8 +692,8 @@ struct TileShape {
     int px;
     int chunk;
 };
-constexpr TileShape kTileShapes[] = {{1, 128}, {2, 128}, {2, 256}, {4, 128}, {4, 256}, {1, 256},
-                                     {2, 64},  {4, 64},  {1, 512}, {2, 512}};
+constexpr TileShape kTileShapes[] = {{1, 128}, {2, 128}, {2, 256}, {4, 128}, {4, 256}, {1, 256}, {2, 64},
+                                     {4, 64},  {1, 512}, {2, 512}, {4, 512}, {1, 1024}, {2, 1024}};
 constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
 constexpr int kDefaultTileShape = 2;
 

@@ -43,6 +43,7 @@ FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64)
 
 
 CALIBRATION = os.path.join(ROOT, "antiradiancecuts_b200", "models", "cutnet_calibration.json")
+TUNING = os.path.join(ROOT, "antiradiancecuts_b200", "models", "autotune.json")
 
 
 def calibrated_error_bound(default: float = 0.002) -> float:
@@ -507,6 +508,8 @@ def main():
     ap.add_argument("--error-bound", type=float, default=None,
                     help="analytic cut bound (default: the one calibrated on the validation scenes)")
     ap.add_argument("--seeds", default="500,501,502,503", help="scenes of the per-scene comparison ('' = none)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time every brute-force launch shape and store the best in models/autotune.json")
     ap.add_argument("--small", action="store_true", help="640x360 / 262,144 AVPLs, no extras (profiling)")
     ap.add_argument("--no-extras", action="store_true", help="skip exact / FP64 / CPU legs")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="all-core CPU baseline sample")
@@ -661,9 +664,18 @@ def main():
     result = {}
     cut_img = out.result64.cpu().numpy().reshape(-1, 3).copy()
     if not args.no_extras:
-        # ---- exact brute-force gather (same GPU) ----
+        # ---- exact brute-force gather (same GPU), in the launch shape the autotuner chose for this
+        # workload (models/autotune.json; --autotune times every shape and updates the file) ----
         prm_bf = api.gather_params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
         out_bf = api.Outputs(W, H)
+        tcache = api.TuningCache(TUNING)
+        tkey = api.TuningCache.key(W, H, N, prm_bf.ar_kind, prm_bf.precision)
+        tuned = tcache.get(tkey)
+        if args.autotune or tuned is not None:
+            tuned, _ = api.autotune_bruteforce(ctx, dv, gb, cam, prm_bf, out_bf, cache=None if args.autotune else tcache)
+            if args.autotune:
+                tcache.put(tkey, tuned, _)
+                tcache.save()
         api.gather_bruteforce(ctx, dv, gb, cam, prm_bf, out_bf)  # warm-up
         torch.cuda.synchronize()
         lib.arc_context_profile(ctx.handle, 1)
@@ -715,6 +727,7 @@ def main():
                              "rel_rmse_vs_fp64": rel_rmse(out_an.result64.cpu().numpy().reshape(-1, 3), ref64),
                              "nodes_per_tile": an_nodes},
             "exact_ms_per_frame": exact_ms,
+            "exact_tile_config": tuned if tuned is not None else "built-in",
             "speedup_vs_exact": exact_ms / ms,
             "rel_rmse_vs_fp64": rel_rmse(cut_img, ref64),
             "exact_rel_rmse_vs_fp64": rel_rmse(exact_img, ref64),

@@ -517,7 +517,7 @@ arc_status arc_batch_capture(arc_batch* batch, const ArcBatchView* views, int32_
 arc_status arc_batch_launch(arc_batch* batch);
 
 /* Times every brute-force launch shape (pixel tile 16 x 16 PX, PX in {1, 2, 4}, AVPL chunk 64 ...
- * 512, ArcGatherParams.tile_config index) on this workload and makes the fastest the context's
+ * 1024, ArcGatherParams.tile_config index) on this workload and makes the fastest the context's
  * default for tile_config = -1.  times_ms[num_shapes] (optional) receives each shape's time
  * (< 0 where it does not apply); *best the chosen index.  Waits for the stream; writes `out`. */
 int32_t arc_bruteforce_num_tile_shapes(void);

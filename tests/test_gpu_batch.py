@@ -153,3 +153,24 @@ def test_autotuner_picks_a_shape_and_makes_it_the_default(ctx, views):
     L.check(ctx.lib.arc_context_set_tile_config(ctx.handle, -1), "set_tile_config")  # back to the built-in one
     assert np.array_equal(imgs[-1], imgs[best])  # the tuned shape was the default
     assert H.rel_rmse(imgs[0], imgs[best]) < 2e-5
+
+
+def test_autotuner_cache_applies_a_stored_shape_without_timing(ctx, views, tmp_path):
+    v = views[0]
+    gp = api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
+    out = api.Outputs(v["w"], v["h"])
+    cache = api.TuningCache(str(tmp_path / "autotune.json"))
+    best, times = api.autotune_bruteforce(ctx, v["avpls"], v["gb"], v["cam"], gp, out, cache=cache)
+    assert ctx.synchronize() == 0
+    cache.save()
+    L.check(ctx.lib.arc_context_set_tile_config(ctx.handle, -1), "set_tile_config")
+    again = api.TuningCache(cache.path)
+    best2, times2 = api.autotune_bruteforce(ctx, v["avpls"], v["gb"], v["cam"], gp, out, cache=again)
+    assert best2 == best and len(times2) == len(times)
+    o1, o2 = api.Outputs(v["w"], v["h"]), api.Outputs(v["w"], v["h"])
+    api.gather_bruteforce(ctx, v["avpls"], v["gb"], v["cam"], gp, o1)  # the cached shape is the default
+    api.gather_bruteforce(ctx, v["avpls"], v["gb"], v["cam"], api.gather_params(L.ARC_AR_CONE, 30.0, 0.01,
+                                                                               tile_config=best), o2)
+    assert ctx.synchronize() == 0
+    assert np.array_equal(o1.result64.cpu().numpy(), o2.result64.cpu().numpy())
+    L.check(ctx.lib.arc_context_set_tile_config(ctx.handle, -1), "set_tile_config")
