@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(256) cut_solid_angle_kernel(SolidArgs a) {
     const int64_t o = (int64_t)y * a.opitch + x;
     float s[3] = {0, 0, 0}, c[3] = {0, 0, 0};
     bool error = false;
+    if (mat != 0 && !(mat > 0 && mat < a.num_mats)) set_error(a.err, ARC_DEVERR_BAD_MATERIAL);
     if (mat > 0 && mat < a.num_mats) {
         const float3 p = f3(gp.x, gp.y, gp.z);
         const float3 nraw = f3(gn.x, gn.y, gn.z);
@@ -214,6 +215,7 @@ struct TileArgs {
     float clamp2;
     int tiles_x, tiles_y;
     float4* info;  // [tiles][4]
+    uint32_t* err;
 };
 
 __device__ __forceinline__ float coarse_g(float px, float py, float pz, float nx, float ny, float nz, const float4 q0,
@@ -250,6 +252,7 @@ __global__ void __launch_bounds__(32 * kSelWarps) cut_tile_setup(TileArgs a) {
             gn = a.gnrm[(int64_t)y * a.gpitch + x];
             const int m = (int)gn.w;
             v = m > 0 && m < a.num_mats;
+            if (!v && m != 0) set_error(a.err, ARC_DEVERR_BAD_MATERIAL);  // gathers 0, as brute force does
             if (v) {
                 const float4 d = a.mats[m].diffuse_exp;
                 skd[warp][i][0] = rn_mul(kOneOverPi, d.x);
@@ -721,21 +724,22 @@ __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
             const uint64_t r = f2(rsqrtf(l2a), rsqrtf(l2b));
             const uint64_t c1 = f2_mul(f2_fma(NZ, dz, f2_fma(NY, dy, f2_mul(NX, dx))), r);
             const uint64_t c2n = f2_mul(f2_fma(f45.y, dz, f2_fma(f45.x, dy, f2_mul(f23.y, dx))), r);  // -c2
-            float c1a, c1b, c2a, c2b, rra, rrb;
+            float c1a, c1b, c2a, c2b, rra, rrb, ia, ib;
             f2_split(c1, c1a, c1b);
             f2_split(c2n, c2a, c2b);
             f2_split(f2_mul(r, r), rra, rrb);
             const uint64_t inv = f2(fminf(rra, inv_clamp2), fminf(rrb, inv_clamp2));
-            const uint64_t g = f2_mul(f2(fmaxf(c1a, 0.0f) * fmaxf(-c2a, 0.0f), fmaxf(c1b, 0.0f) * fmaxf(-c2b, 0.0f)), inv);
+            // c1 / max(d^2, clamp^2): the radiance term's receiver factor and the cone term itself
+            f2_split(f2_mul(c1, inv), ia, ib);
+            const uint64_t g = f2_mul(f2(fmaxf(ia, 0.0f), fmaxf(ib, 0.0f)), f2(fmaxf(-c2a, 0.0f), fmaxf(-c2b, 0.0f)));
             R0 = f2_fma(f89.y, g, R0);
             R1 = f2_fma(f1011.x, g, R1);
             R2 = f2_fma(f1011.y, g, R2);
             if (AR == ARC_AR_CONE) {
                 const ulonglong2 f1213 = s2[6], f1415 = s2[7];
                 const uint64_t wdr = f2_mul(f2_fma(f89.x, dz, f2_fma(f67.y, dy, f2_mul(f67.x, dx))), r);  // -cw
-                float wa, wb, ia, ib;
+                float wa, wb;
                 f2_split(wdr, wa, wb);
-                f2_split(f2_mul(c1, inv), ia, ib);
                 const uint64_t ga = f2((-wa > cos_thr && c1a > eps) ? ia : 0.0f, (-wb > cos_thr && c1b > eps) ? ib : 0.0f);
                 A0 = f2_fma(f1213.x, ga, A0);
                 A1 = f2_fma(f1213.y, ga, A1);
@@ -815,6 +819,7 @@ arc_status launch_tile_setup(arc_context* ctx, const arc_lbvh* bvh, const ArcGBu
     ta.tiles_x = tiles_x;
     ta.tiles_y = tiles_y;
     ta.info = info;
+    ta.err = ctx->d_error;
     float4* extra = nullptr;
     ARC_TRY(ctx->arena.get("node_extra", (size_t)(bvh->n - 1) * 2 * sizeof(float4), reinterpret_cast<void**>(&extra)));
     stage_begin(ctx, "cut_setup");

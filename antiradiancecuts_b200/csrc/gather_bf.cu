@@ -471,22 +471,22 @@ __global__ void __launch_bounds__(kThreads) gather_bf_packed_kernel(BfArgs k) {
                     const uint64_t r = f2(rsqrtf(l2a), rsqrtf(l2b));
                     const uint64_t c1 = f2_mul(f2_fma(NZc[j], dz, f2_fma(NYc[j], dy, f2_mul(NXc[j], dx))), r);
                     const uint64_t c2n = f2_mul(f2_fma(f45.y, dz, f2_fma(f45.x, dy, f2_mul(f23.y, dx))), r);
-                    float c1a, c1b, c2a, c2b, rra, rrb;
+                    float c1a, c1b, c2a, c2b, rra, rrb, ia, ib;
                     f2_split(c1, c1a, c1b);
                     f2_split(c2n, c2a, c2b);
                     f2_split(f2_mul(r, r), rra, rrb);
                     const uint64_t inv = f2(fminf(rra, inv_clamp2), fminf(rrb, inv_clamp2));
-                    const uint64_t g =
-                        f2_mul(f2(fmaxf(c1a, 0.0f) * fmaxf(-c2a, 0.0f), fmaxf(c1b, 0.0f) * fmaxf(-c2b, 0.0f)), inv);
+                    // c1 / max(d^2, clamp^2): the radiance term's receiver factor and the cone term itself
+                    f2_split(f2_mul(c1, inv), ia, ib);
+                    const uint64_t g = f2_mul(f2(fmaxf(ia, 0.0f), fmaxf(ib, 0.0f)), f2(fmaxf(-c2a, 0.0f), fmaxf(-c2b, 0.0f)));
                     acc[j][0] = f2_fma(f89.y, g, acc[j][0]);
                     acc[j][1] = f2_fma(f1011.x, g, acc[j][1]);
                     acc[j][2] = f2_fma(f1011.y, g, acc[j][2]);
                     if (AR == ARC_AR_CONE) {
                         const ulonglong2 f67 = s2[3], f1213 = s2[6], f1415 = s2[7];
                         const uint64_t wdr = f2_mul(f2_fma(f89.x, dz, f2_fma(f67.y, dy, f2_mul(f67.x, dx))), r);
-                        float wa, wb, ia, ib;
+                        float wa, wb;
                         f2_split(wdr, wa, wb);
-                        f2_split(f2_mul(c1, inv), ia, ib);
                         const uint64_t ga = f2((-wa > cos_thr && c1a > eps) ? ia : 0.0f,
                                                (-wb > cos_thr && c1b > eps) ? ib : 0.0f);
                         acc[j][3] = f2_fma(f1213.x, ga, acc[j][3]);

@@ -134,3 +134,21 @@ def test_clustered_edge_cases(ctx, w, h, z_near, theta):
     assert H.rel_rmse(a, b) < 1e-5
     if z_near < 1e-3:
         assert tc.max() > 64  # many clusters in a tile
+
+
+def test_clustered_antiradiance_matches_the_oracle(case):
+    """Against the oracle's restatement of the whole path (oracle_clustered_disk_ar: the same
+    screen clusters, light lists by the slab test, FP64 disk terms over each list): the number of
+    clusters and list entries to 1% (a pixel on a depth-slice boundary may fall on the other side
+    of it in FP64), the image to 1e-5 relative RMSE (FP32 terms on the GPU)."""
+    from oracle import oracle as O
+
+    d, _, _, _, r, out, info, h = case
+    op = O.params(1, 30.0, 0.0, disk_radius=r)
+    ref, nclusters, entries = O.clustered_disk_ar(d["pos"], d["nrm"], d["avpls"], d["dif"], d["spe"], d["ex"],
+                                                  d["cam"], 0.1, math.radians(0.5 * d["desc"].camera_fov_deg), op)
+    assert abs(int(h["tile_count"].sum()) - nclusters) <= 0.01 * nclusters
+    assert abs(int(info.list_entries) - entries) <= 0.01 * entries
+    a = out.antiradiance.cpu().numpy()[..., :3].reshape(-1, 3)
+    assert np.abs(ref).max() > 0
+    assert H.rel_rmse(a, ref) < 1e-5
