@@ -629,54 +629,58 @@ __global__ void __launch_bounds__(64) cut_eval_kernel(EvalArgs a) {
 // two cut nodes per step with f32x2 arithmetic.  The records are staged 128 nodes at a time,
 // interleaved by node pair: float pair * 32 + 2 f + h holds field f (0..15 of the packed record)
 // of node 2 pair + h, so one 16-byte shared load brings two fields of both nodes.  Staging is
-// double-buffered with 4-byte cp.async copies straight into that layout: the copies of the next
-// 128 nodes (and the load of the node ids after them) are in flight while the current 128 are
-// evaluated.  An odd count is padded with a zero record, which contributes exactly 0.  Same terms
-// as pair_terms; the even and odd nodes' partial sums are added before each chunk's Kahan step.
+// asynchronous and double-buffered: a warp copies a whole pair block per instruction, lane t
+// moving float t (field t / 2 of node 2 pair + t % 2) with a 4-byte cp.async -- the 32 lanes read
+// the two 64-byte records (4 sectors) and write 32 consecutive banks.  The node ids of each stage
+// arrive in shared memory one stage ahead with the copies before it, so the copies of stage s + 1
+// are issued from shared memory and fly while stage s is evaluated.  An odd count is padded with
+// a zero record, which contributes exactly 0.  Same terms as pair_terms; the even and odd nodes'
+// partial sums are added before each stage's Kahan step.
 template <int AR>
 __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
     constexpr int kSub = 128;  // nodes per stage; divides kChunkSize, so a stage never straddles two pool chunks
     __shared__ __align__(16) float srec[2][kSub * 16];
+    __shared__ int32_t sids[2][kSub];
     const int tile = a.order[blockIdx.x];
-    const int i = threadIdx.x;
+    const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
     const int x = (tile % a.tiles_x) * kTile + i % kTile, y = (tile / a.tiles_x) * kTile + i / kTile;
     const int count = a.pool.counts[tile];
     const int nsub = (count + kSub - 1) / kSub;
     const int32_t* table = a.pool.tables + (size_t)tile * a.pool.max_chunks;
-    // this thread's two slots (i, i + 64) of stage s: node ids, or -1 past the end
-    auto ids_of = [&](int s, int& id0, int& id1) {
+    const float* recf = reinterpret_cast<const float*>(a.records);
+    // node ids of stage s into sids[s & 1]: two per thread
+    auto copy_ids = [&](int s) {
         const int base = s * kSub;
         const int cnt = min(kSub, count - base);
         const int32_t* nodes = a.pool.entries + (size_t)table[base / kChunkSize] * kChunkSize + base % kChunkSize;
-        id0 = i < cnt ? nodes[i] : -1;
-        id1 = i + 64 < cnt ? nodes[i + 64] : -1;
+        if (i < cnt) cp_async4(&sids[s & 1][i], nodes + i);
+        if (i + 64 < cnt) cp_async4(&sids[s & 1][i + 64], nodes + i + 64);
     };
-    // copies of stage s into buffer s & 1 (one cp.async group per thread); the pad slot of an odd
-    // count gets zeros
-    auto stage = [&](int s, int id0, int id1) {
+    // records of stage s (ids already in sids[s & 1]) into srec[s & 1]: warp w copies pairs
+    // w, w + 2, ...; the pad half of an odd count's last pair gets a zero
+    auto copy_records = [&](int s) {
         const int cnt = min(kSub, count - s * kSub);
+        const int pairs = (cnt + 1) >> 1;
         float* buf = srec[s & 1];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int nl = i + 64 * h, id = h ? id1 : id0;
-            float* d = buf + (nl >> 1) * 32 + (nl & 1);
-            if (id >= 0) {
-                const float* src = reinterpret_cast<const float*>(a.records + 4 * (size_t)id);
-#pragma unroll
-                for (int f = 0; f < 16; ++f) cp_async4(d + 2 * f, src + f);
-            } else if (nl == cnt && (cnt & 1)) {
-#pragma unroll
-                for (int f = 0; f < 16; ++f) d[2 * f] = 0.0f;
-            }
+        const int h = lane & 1, f = lane >> 1;
+        for (int pr = warp; pr < pairs; pr += 2) {
+            const int nl = 2 * pr + h;
+            if (nl < cnt)
+                cp_async4(buf + pr * 32 + lane, recf + 16 * (size_t)sids[s & 1][nl] + f);
+            else
+                buf[pr * 32 + lane] = 0.0f;
         }
-        cp_async_commit();
     };
-    int nid0 = -1, nid1 = -1;
     if (nsub > 0) {
-        ids_of(0, nid0, nid1);
-        stage(0, nid0, nid1);
+        copy_ids(0);
+        cp_async_commit();
+        if (nsub > 1) copy_ids(1);
+        cp_async_commit();
+        cp_async_wait<1>();  // this thread's ids of stage 0
+        __syncthreads();     // everyone's
+        copy_records(0);
+        cp_async_commit();
     }
-    if (nsub > 1) ids_of(1, nid0, nid1);
 
     bool valid = x < a.width && y < a.height;
     float4 gp = make_float4(0, 0, 0, 0), gn = make_float4(0, 0, 0, 0);
@@ -701,14 +705,13 @@ __global__ void __launch_bounds__(64) cut_eval_packed_kernel(EvalArgs a) {
     const uint64_t kTiny2 = f2(1e-30f, 1e-30f);
     float ss[6] = {0, 0, 0, 0, 0, 0}, sc[6] = {0, 0, 0, 0, 0, 0};
     for (int s = 0; s < nsub; ++s) {
-        // stage s has landed for every thread, and every thread is done with stage s - 1, whose
-        // buffer the next copies overwrite
+        // stage s's records and stage s + 1's ids have landed for every thread, and every thread
+        // is done with stage s - 1, whose buffers the next copies overwrite
         cp_async_wait<0>();
         __syncthreads();
-        if (s + 1 < nsub) {
-            stage(s + 1, nid0, nid1);
-            if (s + 2 < nsub) ids_of(s + 2, nid0, nid1);
-        }
+        if (s + 1 < nsub) copy_records(s + 1);
+        if (s + 2 < nsub) copy_ids(s + 2);
+        cp_async_commit();
         const int cnt = min(kSub, count - s * kSub);
         const int pairs = (cnt + 1) >> 1;
         const float* srs = srec[s & 1];

@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 }
             }
             float y = 0.0f;
-            if (!mlp::infer_tiles<kLevelTiles, true>(c, fX, t, &y)) {
+            if (!mlp::infer_tiles<kLevelTiles>(c, fX, t, &y)) {
                 ok = false;
                 mma_gave_up = true;
                 break;

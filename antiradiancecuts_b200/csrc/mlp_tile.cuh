@@ -4,10 +4,10 @@
 //
 // Activation: GELU in its tanh form (Hendrycks & Gimpel 2016),
 //     gelu(x) = x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))),
-// with the hardware tanh (tanh.approx.f32).  Training, the stand-alone inference and the FP64 oracle
-// use this same function, so the network is trained for the activation it is evaluated with; the
-// learned cut's selection evaluates the tanh in BF16 pairs (tanh2_bf16), within the rounding its
-// BF16 activations carry anyway.
+// with the hardware tanh (tanh.approx.f32).  Training, inference and the FP64 oracle use this same
+// function, so the network is trained for the activation it is evaluated with.  (A BF16-pair tanh,
+// tanh.approx.bf16x2, was measured in the selection's epilogue: the packing and unpacking it needs
+// cost more issue slots than the special-function work it saves.)
 #ifndef ARC_MLP_TILE_CUH_
 #define ARC_MLP_TILE_CUH_
 
@@ -56,32 +56,6 @@ __device__ __forceinline__ uint64_t gelu2(uint64_t z, uint64_t b) {
     const uint64_t th = f2(tanh_hw(u0), tanh_hw(u1));
     const uint64_t hx = f2_mul(x, f2(0.5f, 0.5f));
     return f2_fma(hx, th, hx);
-}
-
-// tanh of a pair with one half-precision hardware tanh (tanh.approx.bf16x2): the pair is rounded
-// to BF16 on the way in and the results carry BF16's 8-bit precision (about the rounding the
-// hidden activations get anyway), at half the special-function-unit issues of two tanh.approx.f32.
-__device__ __forceinline__ uint64_t tanh2_bf16(uint64_t u) {
-    float u0, u1;
-    f2_split(u, u0, u1);
-    uint32_t p, t;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(p) : "f"(u1), "f"(u0));  // u1 in the upper half
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(p));
-    return f2(__uint_as_float(t << 16), __uint_as_float(t & 0xffff0000u));
-}
-
-// gelu of z + b for a pair with the BF16 tanh (inference of the learned cut's selection)
-__device__ __forceinline__ uint64_t gelu2_bf16tanh(uint64_t z, uint64_t b) {
-    const uint64_t x = f2_add(z, b);
-    const uint64_t u = f2_mul(x, f2_fma(f2(kGeluB, kGeluB), f2_mul(x, x), f2(kGeluA, kGeluA)));
-    const uint64_t th = tanh2_bf16(u);
-    const uint64_t hx = f2_mul(x, f2(0.5f, 0.5f));
-    return f2_fma(hx, th, hx);
-}
-
-template <bool HalfTanh>
-__device__ __forceinline__ uint64_t gelu2_t(uint64_t z, uint64_t b) {
-    return HalfTanh ? gelu2_bf16tanh(z, b) : gelu2(z, b);
 }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -155,7 +129,6 @@ __device__ __forceinline__ uint32_t row_tmem(const InferCta& c, int t) {
 
 // Hidden layer epilogue for this thread's row: 16 columns at a time from TMEM, + bias, GELU,
 // BF16 into the K-major hidden buffer (rows of all tiles, 64 columns).
-template <bool HalfTanh = false>
 __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const float* bias) {
     const uint32_t taddr = row_tmem(c, t);
 #pragma unroll
@@ -167,7 +140,7 @@ __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const 
         for (int j = 0; j < 8; ++j) {
             const float2 bb = *reinterpret_cast<const float2*>(bias + 16 * q + 2 * j);
             float g0, g1;
-            f2_split(gelu2_t<HalfTanh>(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), g0, g1);
+            f2_split(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), g0, g1);
             u[j] = pack2(g0, g1);
         }
         *reinterpret_cast<uint4*>(c.sm + c.h + tc::kmajor_offset(t, 16 * q, 64)) = make_uint4(u[0], u[1], u[2], u[3]);
@@ -180,8 +153,8 @@ __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const 
 // rows at smem offset x (stride between 8-row groups: 256 bytes), hidden rows at c.h (1024 bytes
 // between 8-row groups), tile u's accumulator in TMEM columns 64 u .. 64 u + 63.  Called by all
 // 128 NT threads; returns false (every thread) if a tensor-core wait gave up, after which the
-// caller frees its TMEM and stops.  HalfTanh: the activations' tanh in BF16 pairs (tanh2_bf16).
-template <int NT, bool HalfTanh = false>
+// caller frees its TMEM and stops.
+template <int NT>
 __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, float* logit) {
     constexpr uint32_t id = tc::idesc_bf16(128, 64, false, false);
     // layer 1 (K = 16)
@@ -195,7 +168,7 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
         tc::commit(c.bar);
     }
     if (!wait_mma(c)) return false;
-    hidden_epilogue<HalfTanh>(c, t, c.vec);
+    hidden_epilogue(c, t, c.vec);
     // layers 2 and 3 (K = 64); layer 2 overwrites the hidden buffer it read once its MMAs are done
 #pragma unroll 1
     for (int l = 0; l < 2; ++l) {
@@ -212,7 +185,7 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
             tc::commit(c.bar);
         }
         if (!wait_mma(c)) return false;
-        if (l == 0) hidden_epilogue<HalfTanh>(c, t, c.vec + 64);
+        if (l == 0) hidden_epilogue(c, t, c.vec + 64);
     }
     // layer 3 epilogue and the 64 -> 1 output layer on the CUDA cores
     const uint32_t taddr = row_tmem(c, t);
@@ -227,7 +200,7 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
         for (int j = 0; j < 8; ++j) {
             const float2 bb = *reinterpret_cast<const float2*>(b3 + 16 * q + 2 * j);
             const float2 ww = *reinterpret_cast<const float2*>(w4 + 16 * q + 2 * j);
-            y2 = f2_fma(gelu2_t<HalfTanh>(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), f2(ww.x, ww.y), y2);
+            y2 = f2_fma(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), f2(ww.x, ww.y), y2);
         }
     }
     float y0, y1;

@@ -88,18 +88,11 @@ def bf16(x):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def gelu_half_tanh(x):
-    """GELU with its tanh taken in BF16: the argument and the tanh rounded to BF16 (the learned cut
-    selection's tanh.approx.bf16x2)."""
-    return 0.5 * x * (1.0 + bf16(np.tanh(bf16(_A * (x + _B * x ** 3)))))
-
-
-def forward_bf16(p, x, half_tanh=False):
+def forward_bf16(p, x):
     """The network with the tensor-core kernels' rounding points: BF16 inputs, weights W1..W3 and
-    hidden activations h1, h2; FP64 otherwise (accumulation, biases, GELU, the 64 -> 1 layer).
-    half_tanh: the activations' tanh in BF16, as the learned cut's selection evaluates it."""
+    hidden activations h1, h2; FP64 otherwise (accumulation, biases, GELU, the 64 -> 1 layer)."""
     P = unpack(p)
-    act = gelu_half_tanh if half_tanh else gelu
+    act = gelu
     h = bf16(x)
     z1 = h @ bf16(P["W1"]).T + P["b1"]
     h1 = bf16(act(z1))

@@ -370,8 +370,7 @@ def learned_cut(pos4, nrm4, tree, diffuse, params, eps_bound, ar_uncertain, band
                 cone_half_angle_deg, disk_radius=0.0, threads=0):
     """The learned cut selection, level by level: leaves and nodes whose bound is within tau are
     accepted, nodes above band * tau refined, the rest scored by the network (BF16 rounding points
-    of the tensor-core kernels and the selection's BF16 tanh, FP64 otherwise) and refined iff the
-    logit reaches thr_logit.
+    of the tensor-core kernels, FP64 otherwise) and refined iff the logit reaches thr_logit.
     -> (sorted node array per tile, scored (tile, node, logit) rows)."""
     from . import mlp_oracle
 
@@ -400,7 +399,7 @@ def learned_cut(pos4, nrm4, tree, diffuse, params, eps_bound, ar_uncertain, band
         refine = (M > band32 * tau) & ~accept
         score = ~accept & ~refine
         if score.any():
-            y = mlp_oracle.forward_bf16(params, F[score], half_tanh=True)
+            y = mlp_oracle.forward_bf16(params, F[score])
             refine[np.nonzero(score)[0][y >= thr_logit]] = True
             scored.append(np.stack([it[score], inn[score], y], 1))
         done = ~refine

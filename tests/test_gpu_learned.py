@@ -115,41 +115,29 @@ def torch_isfinite(t):
 
 
 @pytest.mark.skipif(not os.path.exists(learned.DEFAULT_MODEL), reason="no trained model")
-def test_trained_model_beats_analytic_cut_on_held_out_scene(ctx):
-    """Ablation at the evaluation scale (held-out variant seed 500, 1920x1080, 1,048,576 AVPLs): the
-    shipped network's cut against the analytic error-bound cut without it, both scored against the
-    all-FP64 GPU image (itself checked against the CPU oracle in test_gpu_bruteforce).  At the
-    bound where the analytic cut stays within 1% relative RMSE (eps 0.002), the learned cut must
-    also stay within 1% with at most 60% of the analytic cut's nodes."""
-    wl = scene.WORKLOADS["variant500_1080p_1m"]
-    desc, avpls, _, pos, nrm = wl.build()
-    mats, _, _, _ = scene.materials(desc)
-    cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
-    ctx.upload_materials(mats)
-    dv = ctx.upload_avpls(avpls)
-    bvh = api.AvplBvh(ctx)
-    bvh.build(dv)
-    gb = api.GBuffer(pos, nrm)
-    W, Hh = wl.width, wl.height
-    out64 = api.Outputs(W, Hh)
-    api.gather_bruteforce(ctx, dv, gb, cam, api.gather_params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp,
-                                                              precision=L.ARC_PREC_FP64), out64)
-    assert ctx.synchronize() == 0
-    exact = out64.result64.cpu().numpy().reshape(-1, 3)
-    prm = api.gather_params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
-    pool = ((W + 7) // 8) * ((Hh + 7) // 8) * 65536
+@pytest.mark.parametrize("seed", [500, 501, 502])
+def test_trained_model_beats_analytic_cut_on_held_out_scenes(ctx, seed):
+    """Ablation at the evaluation scale (room variants 1920x1080 with 1,048,576 AVPLs, seeds that
+    neither trained the network (100-163) nor chose its operating point (164-171)): the shipped
+    network's cut against the analytic error-bound cut without it, both scored against the scene's
+    all-FP64 GPU image (itself checked against the CPU oracle in test_gpu_bruteforce).  At the bound
+    where the analytic cut stays within 1% relative RMSE on the validation scenes, the learned cut
+    (its threshold also chosen there) must stay within 1% here, with at most 60% of the analytic
+    cut's nodes."""
+    import json
 
-    def run(cut):
-        out = api.Outputs(W, Hh)
-        api.gather_cut(ctx, bvh, None, gb, cam, prm, cut, out)
-        assert ctx.synchronize() == 0
-        return H.rel_rmse(out.result64.cpu().numpy().reshape(-1, 3), exact), int(api.cut_counts(ctx).sum())
-
+    eps = 0.002
+    cal = os.path.join(os.path.dirname(learned.DEFAULT_MODEL), "cutnet_calibration.json")
+    if os.path.exists(cal):
+        eps = json.load(open(cal))["analytic"]["chosen"] or eps
+    sc = learned.EvalScene(ctx, seed)
+    pool = sc.tiles * 65536
     model = learned.load_default_model(ctx)
-    ea, na = run(api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.002, cut_pool_entries=pool))
-    el, nl = run(learned.cut_params(model, cut_pool_entries=pool))
-    print(f"analytic: {na} nodes, rel RMSE {ea:.4f}; learned: {nl} nodes, rel RMSE {el:.4f}")
-    assert ea <= 0.01 and el <= 0.01
-    assert nl <= 0.6 * na
+    an = sc.cut(api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=eps, ar_uncertain_factor=learned.PREACCEPT_K,
+                               cut_pool_entries=pool), reps=1)
+    lc = sc.cut(learned.cut_params(model, cut_pool_entries=pool), reps=1)
+    print(f"seed {seed}: analytic {an}, learned {lc}")
+    assert lc["rel_rmse"] <= 0.01
+    assert lc["nodes_per_tile"] <= 0.6 * an["nodes_per_tile"]
     model.close()
-    bvh.close()
+    sc.close()

@@ -10,7 +10,9 @@ oracle's correctly rounded FP32 value by one BF16 step (2^-7 relative) plus 2e-3
 compared where the difference is at least 1e-3 of the sum of the magnitudes.  Labels agree except
 where the node's error lies within 1% of the threshold delta; errors agree to 1% + 2e-6 of the tile
 value.  A learned-cut tile may differ from the oracle's only if one of its scored nodes has a logit
-within 0.1 of the threshold."""
+within 0.1 of the threshold, the lists differ in at most 2% of their nodes, and the two cuts'
+images agree to 1e-3 relative RMSE (the hardware tanh and the features' approximate operations
+are restated only up to their rounding, so a near-threshold decision may flip)."""
 import ctypes as C
 
 import numpy as np
@@ -127,9 +129,17 @@ def test_learned_selection_matches_oracle(ctx, scene_):
     differ = [t for t in range(len(gcuts)) if not np.array_equal(gcuts[t], ocuts[t])]
     close = {int(t) for t, _, y in scored if abs(y - thr) < 0.1}
     assert set(differ) <= close, sorted(set(differ) - close)[:10]
-    assert len(differ) <= 0.05 * len(gcuts)
+    # a decision taken the other way swaps a node for its subtree's cut: the lists differ in few nodes
+    total = sum(len(g) for g in gcuts)
+    swapped = sum(len(np.setxor1d(g, o)) for g, o in zip(gcuts, ocuts))
+    assert swapped <= 0.02 * total, (swapped, total)
     # the image is the oracle's evaluation of the GPU's own lists
     _, _, ref = O.eval_cut(d["pos"], d["nrm"], tree, gcuts, d["dif"], 2, CONE, CLAMP)
-    assert H.rel_rmse(out.result64.cpu().numpy().reshape(-1, 3), ref) < 2e-5
-    print(f"{len(scored)} scored rows, {len(differ)} of {len(gcuts)} tiles differ (all near the threshold)")
+    img = out.result64.cpu().numpy().reshape(-1, 3)
+    assert H.rel_rmse(img, ref) < 2e-5
+    # and the oracle's own cut renders the same image up to those swaps
+    _, _, oimg = O.eval_cut(d["pos"], d["nrm"], tree, ocuts, d["dif"], 2, CONE, CLAMP)
+    assert H.rel_rmse(img, oimg) < 1e-3
+    print(f"{len(scored)} scored rows, {len(differ)} of {len(gcuts)} tiles differ (all near the threshold), "
+          f"{swapped} of {total} nodes swapped")
     model.close()

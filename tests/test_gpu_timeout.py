@@ -46,7 +46,7 @@ def test_sort_lookback_timeout_is_reported_and_the_context_recovers(ctx):
     # and a gather over it completes without a device error
     out = api.Outputs(64, 64)
     api.gather_cut(ctx, bvh, dv, api.GBuffer(d["pos"], d["nrm"]), d["cam"], api.gather_params(),
-                   api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01), out)
+                   api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.05, cut_pool_entries=1 << 26), out)
     assert ctx.synchronize() == 0
     assert np.isfinite(out.result64.cpu().numpy()).all()
     bvh.close()
