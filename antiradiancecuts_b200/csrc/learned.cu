@@ -212,8 +212,12 @@ constexpr int kLevelThreads = 256;
 
 // Accepts (tile, node) or pushes (tile, lc), (tile, rc) at depth + 1, per the thread's action;
 // one atomic per CTA and kind (the two global counters are shared by every CTA of the level, so
-// reservations are aggregated over the CTA's 8 warps).  Every thread of the CTA calls it (it
-// holds barriers); se: 2 * warps + 2 shared ints, not touched by anything else.
+// reservations are aggregated over the CTA's 8 warps).  The CTA's left children are written in
+// thread order, then its right children in the same order: a run of entries that share a node
+// (the same node for consecutive tiles) becomes two runs that share its children.  The initial
+// frontier holds the root for every tile, so every level stays grouped by node, and a warp's
+// loads of node data mostly touch one or two nodes.  Every thread of the CTA calls it (it holds
+// barriers); se: 2 * warps + 3 shared ints, not touched by anything else.
 __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, int tile, int node, int lc, int rc,
                                      int depth) {
     constexpr int kW = kLevelThreads / 32;
@@ -223,7 +227,7 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, in
     const unsigned pm = __ballot_sync(0xffffffffu, action == kRefine);
     if (lane == 0) {
         se[w] = __popc(am);
-        se[kW + w] = 2 * __popc(pm);
+        se[kW + w] = __popc(pm);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -236,9 +240,10 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, in
             sp += y;
         }
         const int ba = sa ? atomicAdd(a.acc_count, sa) : 0;
-        const int bp = sp ? atomicAdd(a.out_count, sp) : 0;
+        const int bp = sp ? atomicAdd(a.out_count, 2 * sp) : 0;
         se[2 * kW] = ba;
         se[2 * kW + 1] = bp;
+        se[2 * kW + 2] = sp;
     }
     __syncthreads();
     if (action == kAccept) {
@@ -253,14 +258,14 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, in
         const unsigned grp = __match_any_sync(am, ok ? tile : -1 - lane);
         if (ok && lane == __ffs(grp) - 1) atomicAdd(&a.tile_counts[tile], __popc(grp));
     } else if (action == kRefine) {
-        const int pos = se[2 * kW + 1] + se[kW + w] + 2 * __popc(pm & lt);
-        if ((unsigned)pos + 1u < (unsigned)a.capacity) {
-            a.out[pos] = entry(tile, lc, depth + 1);
-            a.out[pos + 1] = entry(tile, rc, depth + 1);
-        } else {
-            if ((unsigned)pos < (unsigned)a.capacity) a.out[pos] = make_int2(-1, -1);  // the next level skips it
-            set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
-        }
+        // every reserved slot below the capacity is written; the rest do not exist (the next level
+        // reads min(count, capacity) entries)
+        const int rank = se[kW + w] + __popc(pm & lt);
+        const int pl = se[2 * kW + 1] + rank, pr = pl + se[2 * kW + 2];
+        const bool okl = (unsigned)pl < (unsigned)a.capacity, okr = (unsigned)pr < (unsigned)a.capacity;
+        if (okl) a.out[pl] = entry(tile, lc, depth + 1);
+        if (okr) a.out[pr] = entry(tile, rc, depth + 1);
+        if (!okl || !okr) set_error(a.err, ARC_DEVERR_CUT_OVERFLOW);
     }
 }
 
@@ -283,7 +288,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     __shared__ __align__(8) uint64_t bar, wbar;
     __shared__ uint32_t tmem_base;
     __shared__ int s_chunk, s_staged;
-    __shared__ int s_emit[2 * (kLevelThreads / 32) + 2];
+    __shared__ int s_emit[2 * (kLevelThreads / 32) + 3];
     const int t = threadIdx.x, w = t >> 5;
     const int count = min(*a.in_count, a.capacity);
     if ((int64_t)blockIdx.x * kLevelThreads >= count) return;  // no chunk can be left for this CTA
@@ -349,8 +354,14 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                     float f[kFeat];
                     node_features(ti, mean, g, M, nc, wc, rec[0], rec[1], rec[2].x, ne.Ls, ne.As, a.records + 4 * (size_t)lc,
                                   a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
-                    // < kStageRows: fewer than kLevelThreads rows are left over from the last round
-                    const int slot = atomicAdd(&s_staged, 1);
+                    // < kStageRows: fewer than kLevelThreads rows are left over from the last round.
+                    // Slots in thread order within each group of converged lanes, so the staged rows
+                    // (and the children they push) keep the frontier's grouping by node.
+                    const unsigned sm_ = __activemask();
+                    const int ldr = __ffs(sm_) - 1, ln = threadIdx.x & 31;
+                    int slot = 0;
+                    if (ln == ldr) slot = atomicAdd(&s_staged, __popc(sm_));
+                    slot = __shfl_sync(sm_, slot, ldr) + __popc(sm_ & ((1u << ln) - 1u));
                     uint4 x0, x1;
                     x0.x = mlp::pack2(f[0], f[1]);
                     x0.y = mlp::pack2(f[2], f[3]);

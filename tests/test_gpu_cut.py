@@ -113,3 +113,43 @@ def test_cut_overflow_is_reported(ctx, boxes):
     assert ctx.synchronize() & L.ARC_DEVERR_CUT_OVERFLOW
     cl = api.last_cut(ctx)
     assert sum(len(c) for c in cl) <= 100 * 1024
+
+
+def test_error_bound_cut_lists_identical_at_configuration_size(ctx):
+    """The LBVH + error-bound cut configuration at its stated size: room + 2 boxes, 1280x720, 65,536
+    AVPLs, relative error bound 1%.  Every tile's cut list equals the oracle's (the oracle runs
+    strip by strip: a tile's cut depends only on its own pixels), and one strip's image equals the
+    FP64 evaluation of the GPU's lists."""
+    d = H.workload("boxes2_720p_64k")
+    w = d["w"]
+    Wf, Hf = w.width, w.height
+    assert (Wf, Hf, len(d["avpls"])) == (1280, 720, 65536)
+    ctx.upload_materials(d["mats"])
+    dv = ctx.upload_avpls(d["avpls"])
+    bvh = api.AvplBvh(ctx)
+    bvh.build(dv)
+    gb = api.GBuffer(d["pos"], d["nrm"])
+    prm = api.gather_params(L.ARC_AR_CONE, w.cone_half_angle_deg, w.dist_clamp)
+    out = api.Outputs(Wf, Hf)
+    api.gather_cut(ctx, bvh, None, gb, d["cam"], prm, api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01), out)
+    assert ctx.synchronize() == 0
+    gcuts = api.last_cut(ctx)
+    tree = bvh.host_arrays()
+    tx = Wf // 8
+    rows = 64  # strips of 8 tile rows
+    total = 0
+    for y0 in range(0, Hf, rows):
+        ocuts, _, ov = O.tile_cut(d["pos"][y0:y0 + rows], d["nrm"][y0:y0 + rows], tree, d["dif"], 0.01, w.dist_clamp,
+                                  2, w.cone_half_angle_deg, max_cut=65536)
+        assert ov == 0
+        first = (y0 // 8) * tx
+        bad = [t for t in range(len(ocuts)) if not np.array_equal(gcuts[first + t], ocuts[t])]
+        assert not bad, f"strip at row {y0}: {len(bad)} tiles differ, first {bad[:5]}"
+        total += sum(len(c) for c in ocuts)
+        if y0 == 320:
+            _, _, res = O.eval_cut(d["pos"][y0:y0 + rows], d["nrm"][y0:y0 + rows], tree,
+                                   gcuts[first:first + len(ocuts)], d["dif"], 2, w.cone_half_angle_deg, w.dist_clamp)
+            got = out.result64.cpu().numpy()[y0:y0 + rows].reshape(-1, 3)
+            assert H.rel_rmse(got, res) < 2e-5
+    assert total == sum(len(c) for c in gcuts)
+    bvh.close()
