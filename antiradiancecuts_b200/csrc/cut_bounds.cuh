@@ -65,11 +65,11 @@ __device__ __forceinline__ float cone_max_cos(float a1x, float a1y, float a1z, f
     if (c1 <= -1.0f || c2 <= -1.0f) return 1.0f;
     float cb = rn_dot(a1x, a1y, a1z, a2x, a2y, a2z);
     cb = fminf(fmaxf(cb, -1.0f), 1.0f);
-    const float sb = cone_sine(cb);
     const float cg = rn_sub(rn_mul(c1, c2), rn_mul(s1, s2));
     const float sg = rn_add(rn_mul(s1, c2), rn_mul(c1, s2));
     if (sg < 0.0f) return 1.0f;   // combined half-angles exceed pi
     if (cb >= cg) return 1.0f;    // axes closer than the combined half-angles
+    const float sb = cone_sine(cb);  // (only needed past the early returns)
     return rn_add(rn_mul(cb, cg), rn_mul(sb, sg));
 }
 
@@ -79,11 +79,11 @@ __device__ __forceinline__ float cone_min_cos(float a1x, float a1y, float a1z, f
     if (c1 <= -1.0f || c2 <= -1.0f) return -1.0f;
     float cb = rn_dot(a1x, a1y, a1z, a2x, a2y, a2z);
     cb = fminf(fmaxf(cb, -1.0f), 1.0f);
-    const float sb = cone_sine(cb);
     const float cg = rn_sub(rn_mul(c1, c2), rn_mul(s1, s2));
     const float sg = rn_add(rn_mul(s1, c2), rn_mul(c1, s2));
     if (sg < 0.0f) return -1.0f;
     if (cg < -cb) return -1.0f;
+    const float sb = cone_sine(cb);
     return rn_sub(rn_mul(cb, cg), rn_mul(sb, sg));
 }
 

@@ -137,11 +137,13 @@ __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const 
         tc::ld16(taddr + 16 * q, z);
         uint32_t u[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float2 bb = *reinterpret_cast<const float2*>(bias + 16 * q + 2 * j);
+        for (int j = 0; j < 8; j += 2) {  // biases four at a time (one broadcast 16-byte load)
+            const float4 bb = *reinterpret_cast<const float4*>(bias + 16 * q + 2 * j);
             float g0, g1;
             f2_split(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), g0, g1);
             u[j] = pack2(g0, g1);
+            f2_split(gelu2(f2(z[2 * j + 2], z[2 * j + 3]), f2(bb.z, bb.w)), g0, g1);
+            u[j + 1] = pack2(g0, g1);
         }
         *reinterpret_cast<uint4*>(c.sm + c.h + tc::kmajor_offset(t, 16 * q, 64)) = make_uint4(u[0], u[1], u[2], u[3]);
         *reinterpret_cast<uint4*>(c.sm + c.h + tc::kmajor_offset(t, 16 * q + 8, 64)) =
@@ -197,10 +199,11 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
         float z[16];
         tc::ld16(taddr + 16 * q, z);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float2 bb = *reinterpret_cast<const float2*>(b3 + 16 * q + 2 * j);
-            const float2 ww = *reinterpret_cast<const float2*>(w4 + 16 * q + 2 * j);
+        for (int j = 0; j < 8; j += 2) {
+            const float4 bb = *reinterpret_cast<const float4*>(b3 + 16 * q + 2 * j);
+            const float4 ww = *reinterpret_cast<const float4*>(w4 + 16 * q + 2 * j);
             y2 = f2_fma(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), f2(ww.x, ww.y), y2);
+            y2 = f2_fma(gelu2(f2(z[2 * j + 2], z[2 * j + 3]), f2(bb.z, bb.w)), f2(ww.z, ww.w), y2);
         }
     }
     float y0, y1;

@@ -409,11 +409,13 @@ def seeds_leg(ctx, model, error_bound: float, seeds) -> dict:
             "all_learned_within_1pct": all(r["learned"]["rel_rmse"] <= 0.01 for r in rows) if model else None}
 
 
-def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
+def batch_leg(ctx, api, scene, L, stream, num_views: int, model=None) -> dict:
     """Multi-view batch: views of the room + 2 boxes scene drawn with seed 4 (resolutions from
     {256^2, 512^2, 1280x720, 1920x1080}, 8,192 - 262,144 AVPLs each, log-uniform, camera inside the
     room), each with its own AVPL set; per view an LBVH build and an error-bound cut gather (eps
-    0.01).  Timed eagerly (host loop over views) and as one recorded CUDA graph launch."""
+    0.01).  Timed as the views one after another on the context's stream (serial), as a batch on
+    concurrent lanes (eager), and as one recorded CUDA graph launch; with a model, the learned cut's
+    batch recorded into a graph too."""
     import torch
 
     desc = scene.scene_desc(L.ARC_SCENE_ROOM_2BOXES, 2, 2)
@@ -433,11 +435,28 @@ def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
     views = api.Batch.views(items)
     lp, gp = api.lbvh_params(), api.gather_params(L.ARC_AR_CONE, 30.0, 0.01)
     cp = api.cut_params(L.ARC_CUT_ERROR_BOUND, error_bound=0.01)
-    b = api.Batch(ctx)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    # serial: one view after another on the context's stream
+    bvh = api.AvplBvh(ctx)
+
+    def serial():
+        for av, gbv, cam, out in items:
+            L.check(ctx.lib.arc_lbvh_build(bvh.handle, C.byref(av), C.byref(lp)), "arc_lbvh_build")
+            api.gather_cut(ctx, bvh, av, gbv, cam, gp, cp, out)
+
+    serial()
+    assert ctx.synchronize() == 0
+    e0.record(stream)
+    for _ in range(reps):
+        serial()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    serial_ms = e0.elapsed_time(e1) / reps
+    bvh.close()
+    b = api.Batch(ctx)
     b.render(views, lp, gp, cp)  # warm-up (sizes every buffer)
     assert ctx.synchronize() == 0
-    reps = 3
     e0.record(stream)
     for _ in range(reps):
         b.render(views, lp, gp, cp)
@@ -454,10 +473,25 @@ def batch_leg(ctx, api, scene, L, stream, num_views: int) -> dict:
     torch.cuda.synchronize()
     graph = e0.elapsed_time(e1) / reps
     assert ctx.synchronize() == 0
+    learned_graph = None
+    if model is not None:
+        from antiradiancecuts_b200 import learned
+
+        b.capture(views, lp, gp, learned.cut_params(model))
+        b.launch()
+        assert ctx.synchronize() == 0
+        e0.record(stream)
+        for _ in range(reps):
+            b.launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        learned_graph = e0.elapsed_time(e1) / reps
+        assert ctx.synchronize() == 0
     b.close()
-    return {"views": num_views, "pixels": pixels, "avpls": avpl_total, "ms_per_batch_eager": eager,
-            "ms_per_batch_graph": graph, "graph_launches_per_batch": 1, "cut": "error bound 0.01",
-            "views_per_s": num_views * 1000.0 / graph}
+    return {"views": num_views, "pixels": pixels, "avpls": avpl_total, "ms_per_batch_serial": serial_ms,
+            "ms_per_batch_eager": eager, "ms_per_batch_graph": graph, "graph_launches_per_batch": 1,
+            "lanes": 4, "cut": "error bound 0.01", "views_per_s": num_views * 1000.0 / graph,
+            "ms_per_batch_graph_learned": learned_graph}
 
 
 def run_reference(args):
@@ -765,7 +799,7 @@ def main():
         seeds = seeds_leg(ctx, model, args.error_bound, [int(x) for x in args.seeds.split(",")])
         ctx.upload_materials(mats)
     if not args.no_extras:
-        batch = batch_leg(ctx, api, scene, L, stream, args.batch_views)
+        batch = batch_leg(ctx, api, scene, L, stream, args.batch_views, model)
         gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
         post = post_leg(ctx, api, L, out, stream, lbvh_roof["peak"])
         clus = clustered_leg(ctx, api, scene, L, desc, mats, dv, gb, cam, stream)
