@@ -51,7 +51,8 @@ class Model:
     threshold recommended for it (probability for a classifier, relative error for a regressor)."""
 
     def __init__(self, ctx: api.Context, params: np.ndarray | None = None, seed: int = 1,
-                 loss: int = L.ARC_MLP_LOSS_BCE, threshold: float | None = None, band: float = PREACCEPT_BAND):
+                 loss: int = L.ARC_MLP_LOSS_BCE, threshold: float | None = None, band: float = PREACCEPT_BAND,
+                 eps: float = PREACCEPT_EPS):
         self.ctx = ctx
         h = C.c_void_p()
         L.check(ctx.lib.arc_mlp_create(ctx.handle, seed, C.byref(h)), "arc_mlp_create")
@@ -61,18 +62,20 @@ class Model:
         self.loss = int(loss)
         self.threshold = threshold if threshold is not None else (0.5 if loss == L.ARC_MLP_LOSS_BCE else 1e-4)
         self.band = float(band)  # the analytic refine band the network was trained within
+        self.eps = float(eps)    # the analytic pre-acceptance bound it was trained with
         if params is not None:
             self.set_params(params)
 
     def save(self, path: str) -> None:
         np.savez(path, params=self.params(), loss=np.int32(self.loss), threshold=np.float32(self.threshold),
-                 band=np.float32(self.band))
+                 band=np.float32(self.band), eps=np.float32(self.eps))
 
     @classmethod
     def load(cls, ctx: api.Context, path: str) -> "Model":
         z = np.load(path)
         return cls(ctx, z["params"], loss=int(z["loss"]), threshold=float(z["threshold"]),
-                   band=float(z["band"]) if "band" in z else PREACCEPT_BAND)
+                   band=float(z["band"]) if "band" in z else PREACCEPT_BAND,
+                   eps=float(z["eps"]) if "eps" in z else PREACCEPT_EPS)
 
     def set_params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, np.float32)
@@ -96,7 +99,7 @@ class Model:
 def cut_params(model: Model, threshold: float | None = None, **kw):
     """ArcCutParams of the learned cut with the pre-acceptance the model was trained with."""
     kw.setdefault("mlp_band", model.band)
-    return api.cut_params(L.ARC_CUT_LEARNED, error_bound=PREACCEPT_EPS, ar_uncertain_factor=PREACCEPT_K,
+    return api.cut_params(L.ARC_CUT_LEARNED, error_bound=model.eps, ar_uncertain_factor=PREACCEPT_K,
                           model=model.handle.value,
                           mlp_threshold=model.threshold if threshold is None else threshold, **kw)
 
@@ -355,7 +358,7 @@ def choose(values, results, target: float, larger_is_faster: bool = True):
 
 THRESHOLDS = (0.01, 0.02, 0.03, 0.05, 0.07, 0.1, 0.15, 0.2, 0.3)
 ANALYTIC_BOUNDS = (0.0015, 0.002, 0.0025, 0.003, 0.004)
-CALIBRATION_TARGET = 0.0095  # the worst validation scene's relative RMSE: 1% with a margin
+CALIBRATION_TARGET = 0.0099  # the worst validation scene's relative RMSE stays under 1%
 
 
 def calibrate(ctx: api.Context, model_paths, seeds=VALIDATION_SEEDS, target=CALIBRATION_TARGET, log=print) -> dict:
@@ -381,7 +384,8 @@ def calibrate(ctx: api.Context, model_paths, seeds=VALIDATION_SEEDS, target=CALI
         thr = choose(THRESHOLDS, res, target, larger_is_faster=True)
         worst = [max(x["rel_rmse"] for x in r) for r in res]
         mean_ms = [float(np.mean([x["ms"] for x in r])) for r in res]
-        cand = {"model": os.path.basename(path), "band": m.band, "threshold": thr, "worst_rel_rmse": worst,
+        cand = {"model": os.path.basename(path), "band": m.band, "eps": m.eps, "threshold": thr,
+                "worst_rel_rmse": worst,
                 "mean_ms": mean_ms, "thresholds": list(THRESHOLDS)}
         if thr is not None:
             cand["calibrated_mean_ms"] = mean_ms[THRESHOLDS.index(thr)]
@@ -407,6 +411,7 @@ def main(argv=None):
     tr.add_argument("--delta", type=float, default=LABEL_DELTA)
     tr.add_argument("--objective", choices=["regression", "classification"], default="classification")
     tr.add_argument("--band", type=float, default=PREACCEPT_BAND)
+    tr.add_argument("--eps", type=float, default=PREACCEPT_EPS, help="analytic pre-acceptance bound")
     tr.add_argument("--threshold", type=float, default=None, help="selection threshold stored with the model")
     tr.add_argument("--out", default=DEFAULT_MODEL)
     ca = sub.add_parser("calibrate", help="choose the operating point on the validation scenes")
@@ -442,7 +447,7 @@ def main(argv=None):
     t0 = time.time()
     seeds = list(TRAIN_SEEDS)[: a.scenes]
     for s in seeds:
-        f, l, e = scene_samples(ctx, s, capacity=24 * per_scene, delta=a.delta, band=a.band)
+        f, l, e = scene_samples(ctx, s, capacity=24 * per_scene, delta=a.delta, band=a.band, error_bound=a.eps)
         if regress:
             l = torch.log2(torch.clamp(e, min=2.0 ** LOG2_FLOOR))
         if f.shape[0] > per_scene:  # uniform subsample to the per-scene budget
@@ -462,6 +467,7 @@ def main(argv=None):
     loss = L.ARC_MLP_LOSS_SQUARED if regress else L.ARC_MLP_LOSS_BCE
     model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs, loss=loss)
     model.band = a.band
+    model.eps = a.eps
     # the shipped classifier refines at P(refine) >= 0.05: within 1% RMSE on the held-out scene
     model.threshold = a.threshold if a.threshold is not None else (0.05 if not regress else 1e-4)
     print("validation:", evaluate(ctx, model, feats[val].contiguous(), labels[val].contiguous(), a.delta), flush=True)
