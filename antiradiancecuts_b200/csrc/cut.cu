@@ -900,7 +900,7 @@ arc_status launch_gather_cut(arc_context* ctx, const arc_lbvh* bvh, const ArcAvp
     const int max_cut = cp->max_cut_nodes > 0 ? cp->max_cut_nodes : (1 << 20);
     CutPool pool;
     pool.max_chunks = (max_cut + kChunkSize - 1) / kChunkSize;
-    const int64_t pool_entries = cp->cut_pool_entries > 0 ? cp->cut_pool_entries : (int64_t)tiles * 65536;
+    const int64_t pool_entries = cp->cut_pool_entries > 0 ? cp->cut_pool_entries : (int64_t)tiles * 32768;
     pool.num_chunks = (int32_t)std::min<int64_t>((pool_entries + kChunkSize - 1) / kChunkSize, INT32_MAX / kChunkSize);
     ARC_TRY(ctx->arena.get("cut_pool", (size_t)pool.num_chunks * kChunkSize * sizeof(int32_t),
                            reinterpret_cast<void**>(&pool.entries)));

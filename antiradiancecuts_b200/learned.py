@@ -41,7 +41,7 @@ LOG2_FLOOR = -30.0  # regression targets: log2 of the relative error, at least t
 # PREACCEPT_EPS of the tile estimate (antiradiance-uncertain nodes weighted by PREACCEPT_K) are
 # accepted, nodes whose bound exceeds PREACCEPT_BAND times that are refined, both without the
 # network; the network decides the nodes in between (it prunes refinements of the analytic cut)
-PREACCEPT_EPS = 2e-3
+PREACCEPT_EPS = 1.5e-3
 PREACCEPT_K = 16.0
 PREACCEPT_BAND = 64.0
 

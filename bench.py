@@ -799,6 +799,7 @@ def main():
         seeds = seeds_leg(ctx, model, args.error_bound, [int(x) for x in args.seeds.split(",")])
         ctx.upload_materials(mats)
     if not args.no_extras:
+        torch.cuda.empty_cache()  # the per-scene leg's tensors: the batch's lanes allocate outside torch
         batch = batch_leg(ctx, api, scene, L, stream, args.batch_views, model)
         gen = scene_leg(ctx, api, scene, wl, desc, avpls, pos, nrm, stream)
         post = post_leg(ctx, api, L, out, stream, lbvh_roof["peak"])

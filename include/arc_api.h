@@ -355,7 +355,8 @@ typedef struct ArcCutParams {
     float ar_uncertain_factor;   /* antiradiance bound multiplier for nodes whose cone test may differ
                                     between pairs (default 16); 1 treats them like certain nodes */
     int32_t max_cut_nodes;       /* per-tile cut capacity, default 2^20 (ARC_DEVERR_CUT_OVERFLOW beyond it) */
-    int64_t cut_pool_entries;    /* total cut entries over all tiles; 0 = 65536 per tile */
+    int64_t cut_pool_entries;    /* total cut entries over all tiles; 0 = 32768 per tile (the learned cut also keeps
+                                  * an 8-byte accepted-pair list of the same capacity) */
     const arc_mlp* model;        /* LEARNED only */
     float mlp_threshold;         /* LEARNED: refine when the predicted probability >= this (BCE model), or
                                     when the predicted relative node error >= this (squared-loss model

@@ -29,19 +29,27 @@ def test_gradient_matches_finite_differences(loss):
 
 def test_shipped_model_archive():
     """The shipped cut network: the archive fields a C / C++ host reads, the parameter count the
-    library expects, finite weights, and finite logits through the FP64 network."""
+    library expects, finite weights, finite logits through the FP64 network, and the operating
+    point it ships with is the one its calibration report chose on the validation scenes."""
+    import json
+    import os
+
     from antiradiancecuts_b200 import _lib as L
     from antiradiancecuts_b200 import learned
 
     z = np.load(learned.DEFAULT_MODEL)
-    assert set(z.files) >= {"params", "loss", "threshold", "band"}
+    assert set(z.files) >= {"params", "loss", "threshold", "band", "eps"}
     p = z["params"]
     assert p.dtype == np.float32 and p.shape == (M.NUM_PARAMS,)
     assert L.load().arc_mlp_num_params() == M.NUM_PARAMS == learned.NUM_PARAMS
     assert np.all(np.isfinite(p)) and np.abs(p).max() > 0
     assert int(z["loss"]) == L.ARC_MLP_LOSS_BCE
-    assert float(z["threshold"]) == pytest.approx(0.05)
-    assert float(z["band"]) == learned.PREACCEPT_BAND
+    rep = json.load(open(os.path.join(os.path.dirname(learned.DEFAULT_MODEL), "cutnet_calibration.json")))
+    chosen = rep["chosen"]
+    assert float(z["threshold"]) == pytest.approx(chosen["threshold"])
+    assert float(z["band"]) == chosen["band"] and float(z["eps"]) == pytest.approx(chosen["eps"])
+    assert max(chosen["worst_rel_rmse"][chosen["thresholds"].index(chosen["threshold"])], 0) <= rep["target_rel_rmse"]
+    assert rep["seeds"] == list(learned.VALIDATION_SEEDS)
     x = np.random.default_rng(0).normal(0, 1, (256, 16))
     logits, _ = M.forward(p.astype(np.float64), x)
     assert np.all(np.isfinite(logits)) and np.std(logits) > 0
