@@ -2,12 +2,16 @@
 // activation, and the inference of one 128-row tile on the tensor cores, used by the stand-alone
 // forward kernel (mlp.cu) and by the fused level kernel of the learned cut (learned.cu).
 //
-// Activation: GELU in its tanh form (Hendrycks & Gimpel 2016),
-//     gelu(x) = x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))),
-// with the hardware tanh (tanh.approx.f32).  Training, inference and the FP64 oracle use this same
-// function, so the network is trained for the activation it is evaluated with.  (A BF16-pair tanh,
-// tanh.approx.bf16x2, was measured in the selection's epilogue: the packing and unpacking it needs
-// cost more issue slots than the special-function work it saves.)
+// Activation: GELU in its sigmoid form (Hendrycks & Gimpel 2016, x sigma(1.702 x)), written with
+// the hardware tanh (tanh.approx.f32):
+//     gelu(x) = x/2 (1 + tanh(s x)),   s = 1.702 / 2.
+// Training and the FP64 oracle use this function.  Inference folds its constants into the
+// parameters (load_weights): with z' = s z the activation is (1 / (2 s)) g(z'), g(z) = z + z tanh(z),
+// so layer 1 takes s W1, s b1, the next layers (s / (2 s)) W = W / 2 and s b, and the output layer
+// w4 / (2 s); the epilogue is then one add (bias), one tanh and one multiply-add per value.
+// (Two forms were measured and dropped: the tanh form of GELU, whose cubic argument costs three
+// more operations per value, and a BF16-pair tanh, tanh.approx.bf16x2, whose packing cost more
+// issue slots than the special-function work it saved.)
 #ifndef ARC_MLP_TILE_CUH_
 #define ARC_MLP_TILE_CUH_
 
@@ -25,8 +29,8 @@ constexpr int kIn = 16, kHid = 64, kRows = 128;
 constexpr int oW1 = 0, oB1 = oW1 + kHid * kIn, oW2 = oB1 + kHid, oB2 = oW2 + kHid * kHid, oW3 = oB2 + kHid,
               oB3 = oW3 + kHid * kHid, oW4 = oB3 + kHid, oB4 = oW4 + kHid, kParams = oB4 + 1;  // 9473
 
-constexpr float kGeluA = 0.7978845608f;           // sqrt(2 / pi)
-constexpr float kGeluB = 0.7978845608f * 0.044715f;
+constexpr float kGeluS = 0.851f;                   // 1.702 / 2
+constexpr float kGeluOut = 0.5f / 0.851f;          // 1 / (2 s): the folded activation's scale
 
 __device__ __forceinline__ float tanh_hw(float x) {
     float y;
@@ -35,27 +39,24 @@ __device__ __forceinline__ float tanh_hw(float x) {
 }
 
 __device__ __forceinline__ float gelu(float x) {
-    const float th = tanh_hw(x * fmaf(kGeluB, x * x, kGeluA));
+    const float th = tanh_hw(kGeluS * x);
     const float hx = 0.5f * x;
     return fmaf(hx, th, hx);
 }
 
-// d gelu / dx = (1 + th) / 2 + x/2 (1 - th^2) sqrt(2/pi) (1 + 3 * 0.044715 x^2)
+// d gelu / dx = (1 + th) / 2 + (x / 2) s (1 - th^2)
 __device__ __forceinline__ float gelu_grad(float x) {
-    const float x2 = x * x;
-    const float th = tanh_hw(x * fmaf(kGeluB, x2, kGeluA));
-    return fmaf(0.5f, th, 0.5f) + 0.5f * x * (1.0f - th * th) * fmaf(3.0f * kGeluB, x2, kGeluA);
+    const float th = tanh_hw(kGeluS * x);
+    return fmaf(0.5f, th, 0.5f) + 0.5f * x * kGeluS * (1.0f - th * th);
 }
 
-// gelu of z + b for a pair, the same operations as gelu()
-__device__ __forceinline__ uint64_t gelu2(uint64_t z, uint64_t b) {
+// The folded activation of inference for a pair: x = z + b (both already scaled by s), g(x) =
+// x + x tanh(x); the result is 2 s gelu of the unscaled value.
+__device__ __forceinline__ uint64_t act2(uint64_t z, uint64_t b) {
     const uint64_t x = f2_add(z, b);
-    const uint64_t u = f2_mul(x, f2_fma(f2(kGeluB, kGeluB), f2_mul(x, x), f2(kGeluA, kGeluA)));
-    float u0, u1;
-    f2_split(u, u0, u1);
-    const uint64_t th = f2(tanh_hw(u0), tanh_hw(u1));
-    const uint64_t hx = f2_mul(x, f2(0.5f, 0.5f));
-    return f2_fma(hx, th, hx);
+    float x0, x1;
+    f2_split(x, x0, x1);
+    return f2_fma(x, f2(tanh_hw(x0), tanh_hw(x1)), x);
 }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -72,22 +73,23 @@ constexpr uint32_t kImageBytes = kWeightBytes + kVecBytesInfer;
 static_assert(kImageBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // Every thread of the CTA (nthreads of them) helps load the weights (into shared memory, or into
-// a global image in the same layout).
+// a global image in the same layout), with the activation's constants folded in (see the top of
+// this file): s W1 | W2 / 2 | W3 / 2 in BF16, then s b1 | s b2 | s b3 | w4 / (2 s) | b4 in FP32.
 __device__ __forceinline__ void load_weights(unsigned char* w, float* vec, const float* params, int t, int nthreads) {
     for (int i = t; i < kHid * kIn; i += nthreads)
         *reinterpret_cast<__nv_bfloat16*>(w + kW1 + tc::kmajor_offset(i / kIn, i % kIn, kIn)) =
-            __float2bfloat16_rn(params[oW1 + i]);
+            __float2bfloat16_rn(kGeluS * params[oW1 + i]);
     for (int i = t; i < kHid * kHid; i += nthreads) {
         *reinterpret_cast<__nv_bfloat16*>(w + kW2 + tc::kmajor_offset(i / kHid, i % kHid, kHid)) =
-            __float2bfloat16_rn(params[oW2 + i]);
+            __float2bfloat16_rn(0.5f * params[oW2 + i]);
         *reinterpret_cast<__nv_bfloat16*>(w + kW3 + tc::kmajor_offset(i / kHid, i % kHid, kHid)) =
-            __float2bfloat16_rn(params[oW3 + i]);
+            __float2bfloat16_rn(0.5f * params[oW3 + i]);
     }
     for (int i = t; i < 64; i += nthreads) {
-        vec[i] = params[oB1 + i];
-        vec[64 + i] = params[oB2 + i];
-        vec[128 + i] = params[oB3 + i];
-        vec[192 + i] = params[oW4 + i];
+        vec[i] = kGeluS * params[oB1 + i];
+        vec[64 + i] = kGeluS * params[oB2 + i];
+        vec[128 + i] = kGeluS * params[oB3 + i];
+        vec[192 + i] = kGeluOut * params[oW4 + i];
     }
     if (t == 0) vec[256] = params[oB4];
 }
@@ -140,9 +142,9 @@ __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const 
         for (int j = 0; j < 8; j += 2) {  // biases four at a time (one broadcast 16-byte load)
             const float4 bb = *reinterpret_cast<const float4*>(bias + 16 * q + 2 * j);
             float g0, g1;
-            f2_split(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), g0, g1);
+            f2_split(act2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), g0, g1);
             u[j] = pack2(g0, g1);
-            f2_split(gelu2(f2(z[2 * j + 2], z[2 * j + 3]), f2(bb.z, bb.w)), g0, g1);
+            f2_split(act2(f2(z[2 * j + 2], z[2 * j + 3]), f2(bb.z, bb.w)), g0, g1);
             u[j + 1] = pack2(g0, g1);
         }
         *reinterpret_cast<uint4*>(c.sm + c.h + tc::kmajor_offset(t, 16 * q, 64)) = make_uint4(u[0], u[1], u[2], u[3]);
@@ -202,8 +204,8 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
         for (int j = 0; j < 8; j += 2) {
             const float4 bb = *reinterpret_cast<const float4*>(b3 + 16 * q + 2 * j);
             const float4 ww = *reinterpret_cast<const float4*>(w4 + 16 * q + 2 * j);
-            y2 = f2_fma(gelu2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), f2(ww.x, ww.y), y2);
-            y2 = f2_fma(gelu2(f2(z[2 * j + 2], z[2 * j + 3]), f2(bb.z, bb.w)), f2(ww.z, ww.w), y2);
+            y2 = f2_fma(act2(f2(z[2 * j], z[2 * j + 1]), f2(bb.x, bb.y)), f2(ww.x, ww.y), y2);
+            y2 = f2_fma(act2(f2(z[2 * j + 2], z[2 * j + 3]), f2(bb.z, bb.w)), f2(ww.z, ww.w), y2);
         }
     }
     float y0, y1;

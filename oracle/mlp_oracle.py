@@ -1,6 +1,7 @@
-"""FP64 NumPy restatement of the cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, GELU in its tanh
-form, Hendrycks & Gimpel 2016) with its weighted binary-cross-entropy gradient.  TEST INFRASTRUCTURE ONLY: the checker for the
-tensor-core kernels in antiradiancecuts_b200/csrc/mlp.cu; the product never imports it.
+"""FP64 NumPy restatement of the cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, GELU in its sigmoid
+form x sigma(1.702 x), Hendrycks & Gimpel 2016) with its weighted binary-cross-entropy gradient.
+TEST INFRASTRUCTURE ONLY: the checker for the tensor-core kernels in
+antiradiancecuts_b200/csrc/mlp.cu; the product never imports it.
 
 Parameter layout (FP32 master copy of the library): W1[64][16], b1[64], W2[64][64], b2[64],
 W3[64][64], b3[64], w4[64], b4.
@@ -29,18 +30,17 @@ def pack(d):
     return np.concatenate([np.asarray(d[name], np.float64).ravel() for name, _ in SIZES])
 
 
-_A = math.sqrt(2.0 / math.pi)
-_B = 0.044715
+_S = 0.851  # 1.702 / 2
 
 
 def gelu(x):
-    """x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))"""
-    return 0.5 * x * (1.0 + np.tanh(_A * (x + _B * x ** 3)))
+    """x/2 (1 + tanh(s x)) = x sigma(1.702 x)"""
+    return 0.5 * x * (1.0 + np.tanh(_S * x))
 
 
 def gelu_grad(x):
-    th = np.tanh(_A * (x + _B * x ** 3))
-    return 0.5 * (1.0 + th) + 0.5 * x * (1.0 - th * th) * _A * (1.0 + 3.0 * _B * x * x)
+    th = np.tanh(_S * x)
+    return 0.5 * (1.0 + th) + 0.5 * x * _S * (1.0 - th * th)
 
 
 def forward(p, x):
@@ -89,15 +89,27 @@ def bf16(x):
 
 
 def forward_bf16(p, x):
-    """The network with the tensor-core kernels' rounding points: BF16 inputs, weights W1..W3 and
-    hidden activations h1, h2; FP64 otherwise (accumulation, biases, GELU, the 64 -> 1 layer)."""
+    """The network as the tensor-core kernels evaluate it: the activation's constants folded into the
+    parameters (s W1, W2 / 2, W3 / 2 rounded to BF16 from FP32 products; s b in FP32; w4 / (2 s)),
+    the folded activation g(z) = z + z tanh(z), BF16 inputs and hidden activations h1, h2; FP64
+    otherwise (accumulation, biases, activation, the 64 -> 1 layer)."""
     P = unpack(p)
-    act = gelu
+    s32 = np.float32(_S)
+    out32 = np.float32(0.5) / s32
+
+    def f32(a):
+        return np.asarray(a, np.float32)
+
+    def g(z):
+        return z + z * np.tanh(z)
+
+    W1 = bf16(s32 * f32(P["W1"]))
+    W2 = bf16(np.float32(0.5) * f32(P["W2"]))
+    W3 = bf16(np.float32(0.5) * f32(P["W3"]))
+    b1, b2, b3 = (np.float64(s32 * f32(P[k])) for k in ("b1", "b2", "b3"))
+    w4 = np.float64(out32 * f32(P["w4"]))
     h = bf16(x)
-    z1 = h @ bf16(P["W1"]).T + P["b1"]
-    h1 = bf16(act(z1))
-    z2 = h1 @ bf16(P["W2"]).T + P["b2"]
-    h2 = bf16(act(z2))
-    z3 = h2 @ bf16(P["W3"]).T + P["b3"]
-    h3 = act(z3)
-    return h3 @ P["w4"] + P["b4"][0]
+    h1 = bf16(g(h @ W1.T + b1))
+    h2 = bf16(g(h1 @ W2.T + b2))
+    h3 = g(h2 @ W3.T + b3)
+    return h3 @ w4 + np.float64(np.float32(P["b4"][0]))

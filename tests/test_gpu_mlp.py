@@ -19,19 +19,22 @@ def _bf16(t):
 
 
 def _torch_forward(p, x):
-    """FP32 reference rounding weights, inputs and the hidden activations to BF16 where the kernel does."""
+    """FP32 reference of the kernels' inference: the activation's constants folded into the
+    parameters as the library's weight image holds them (s W1, W2 / 2, W3 / 2 in BF16, s b in FP32,
+    w4 / (2 s)), the folded activation z + z tanh(z), and BF16 inputs and hidden activations."""
     import torch
 
     P = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in M.unpack(p).items()}
-    gelu = lambda z: 0.5 * z * (1 + torch.tanh(np.sqrt(2.0 / np.pi) * (z + 0.044715 * z ** 3)))  # noqa: E731
+    s = torch.tensor(0.851, dtype=torch.float32)
+    g = lambda z: z + z * torch.tanh(z)  # noqa: E731
     h = _bf16(x)
-    z1 = h @ _bf16(P["W1"]).T + P["b1"]
-    h1 = _bf16(gelu(z1))
-    z2 = h1 @ _bf16(P["W2"]).T + P["b2"]
-    h2 = _bf16(gelu(z2))
-    z3 = h2 @ _bf16(P["W3"]).T + P["b3"]
-    h3 = gelu(z3)
-    return h3 @ P["w4"] + P["b4"][0]
+    z1 = h @ _bf16(s * P["W1"]).T + s * P["b1"]
+    h1 = _bf16(g(z1))
+    z2 = h1 @ _bf16(0.5 * P["W2"]).T + s * P["b2"]
+    h2 = _bf16(g(z2))
+    z3 = h2 @ _bf16(0.5 * P["W3"]).T + s * P["b3"]
+    h3 = g(z3)
+    return h3 @ ((torch.tensor(0.5, dtype=torch.float32) / s) * P["w4"]) + P["b4"][0]
 
 
 @pytest.fixture(scope="module")
