@@ -97,29 +97,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
-// Plain arrive on an mbarrier (release at CTA scope).
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// Named barrier `id` over `nthreads` threads (whole warps), for a group of warps that synchronises
-// without the rest of the CTA; and the same barrier returning the AND of `v` over the group.
-__device__ __forceinline__ void named_barrier(int id, int nthreads) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
-__device__ __forceinline__ bool named_barrier_and(int id, int nthreads, bool v) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.and.pred p, %2, %3, q;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)v), "r"(id), "r"(nthreads)
-        : "memory");
-    return r != 0;
-}
-
 // cp.async (global -> shared, 4 bytes, through L1): one thread's copies complete as a group.
 __device__ __forceinline__ void cp_async4(void* dst_smem, const void* src_gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst_smem)), "l"(src_gmem) : "memory");

@@ -211,19 +211,17 @@ enum Action : int { kNone = 0, kAccept = 1, kRefine = 2, kScore = 3 };
 constexpr int kLevelThreads = 256;
 
 // Accepts (tile, node) or pushes (tile, lc), (tile, rc) at depth + 1, per the thread's action;
-// one atomic per group and kind (the two global counters are shared by every CTA of the level, so
-// reservations are aggregated over the group's warps).  The group's left children are written in
+// one atomic per CTA and kind (the two global counters are shared by every CTA of the level, so
+// reservations are aggregated over the CTA's 8 warps).  The CTA's left children are written in
 // thread order, then its right children in the same order: a run of entries that share a node
 // (the same node for consecutive tiles) becomes two runs that share its children.  The initial
 // frontier holds the root for every tile, so every level stays grouped by node, and a warp's
-// loads of node data mostly touch one or two nodes.  Every thread of the group (NT threads, named
-// barrier BarId; gt = the thread's index in the group) calls it; se: 2 * NT / 32 + 3 shared ints,
-// not touched by anything else.
-template <int BarId, int NT>
-__device__ __forceinline__ void emit(const LevelArgs& a, int* se, int gt, int action, int tile, int node, int lc, int rc,
+// loads of node data mostly touch one or two nodes.  Every thread of the CTA calls it (it holds
+// barriers); se: 2 * warps + 3 shared ints, not touched by anything else.
+__device__ __forceinline__ void emit(const LevelArgs& a, int* se, int action, int tile, int node, int lc, int rc,
                                      int depth) {
-    constexpr int kW = NT / 32;
-    const int lane = gt & 31, w = gt >> 5;
+    constexpr int kW = kLevelThreads / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const unsigned am = __ballot_sync(0xffffffffu, action == kAccept);
     const unsigned pm = __ballot_sync(0xffffffffu, action == kRefine);
@@ -231,8 +229,8 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int gt, int ac
         se[w] = __popc(am);
         se[kW + w] = __popc(pm);
     }
-    named_barrier(BarId, NT);
-    if (gt == 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
         int sa = 0, sp = 0;
         for (int i = 0; i < kW; ++i) {
             const int x = se[i], y = se[kW + i];
@@ -247,7 +245,7 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int gt, int ac
         se[2 * kW + 1] = bp;
         se[2 * kW + 2] = sp;
     }
-    named_barrier(BarId, NT);
+    __syncthreads();
     if (action == kAccept) {
         // unsigned: the shared counter keeps counting past the capacity and may wrap past 2^31
         const int pos = se[2 * kW] + se[w] + __popc(am & lt);
@@ -271,224 +269,167 @@ __device__ __forceinline__ void emit(const LevelArgs& a, int* se, int gt, int ac
     }
 }
 
-// learned_level: a warp-specialised CTA of 384 threads.  The scan group (warps 0-7, 256 threads)
-// takes 256 frontier pairs at a time from the level's work counter, one per thread: it accepts or
-// refines by the analytic bound, and stages the features of every pair in the band as a BF16 row
-// in a ring of four 128-row slots.  The net group (warps 8-11, 128 threads, one row each) scores
-// full slots on the tensor cores (three layers, one 128-row tile, its accumulator in 64 TMEM
-// columns) and refines or accepts their pairs by the logit.  The two groups meet only at the
-// ring: a slot's `full` mbarrier completes when its 128th row is written (the writer that brings
-// its fill count to a multiple of 128 arrives), its `empty` mbarrier when the net group has read
-// it; each group's frontier pushes are aggregated on its own named barrier.  So the scan group
-// never waits for the network and the network never waits for a chunk's slowest thread.  At the
-// level's end the scan group pads the last partial slot with empty rows and publishes the row
-// total, after which the net group stops once it has scored every slot.  Every wait is bounded.
-// Shared memory: weights and vectors (the image built by weight_image) | ring rows (512, K-major,
-// K = 16) | hidden rows (128 x 64) | ring pairs {tile, node | depth}.
-constexpr int kScanThreads = kLevelThreads, kNetThreads = 128, kLevelBlock = kScanThreads + kNetThreads;
-constexpr int kRingSlots = 4, kRingRows = 128 * kRingSlots;
-constexpr int kScanBar = 1, kNetBar = 2;
+// learned_level: 256 threads, one pair per thread per chunk, rows scored two 128-row tiles at a
+// time.  Shared memory: weights and vectors (the image built by weight_image) | staged feature
+// rows (512, K-major, K = 16: fewer than 256 left over plus one chunk) | hidden rows (256 x 64)
+// | staged pairs {tile, node | depth}
+constexpr int kLevelTiles = kLevelThreads / 128, kStageRows = 2 * kLevelThreads;
 constexpr uint32_t fW = 0, fVec = mlp::kWeightBytes, fX = ((mlp::kImageBytes + 127) / 128) * 128,
-                   fH = fX + kRingRows * 32, fMeta = fH + 128 * 128, kLevelSmem = fMeta + kRingRows * 8;
-constexpr uint32_t kLevelTmemCols = 64;
+                   fH = fX + kStageRows * 32, fMeta = fH + kLevelThreads * 128, kLevelSmem = fMeta + kStageRows * 8;
+constexpr uint32_t kLevelTmemCols = 64 * kLevelTiles;
 
 // BF16 core-matrix weights + FP32 vectors, once per selection
 __global__ void weight_image(const float* params, unsigned char* img) {
     mlp::load_weights(img, reinterpret_cast<float*>(img + mlp::kWeightBytes), params, threadIdx.x, blockDim.x);
 }
 
-__global__ void __launch_bounds__(kLevelBlock, 2) learned_level(LevelArgs a) {
+__global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t bar, wbar, full[kRingSlots], empty[kRingSlots];
+    __shared__ __align__(8) uint64_t bar, wbar;
     __shared__ uint32_t tmem_base;
-    __shared__ int s_chunk, s_rows, s_end;
-    __shared__ int s_fill[kRingSlots];
-    __shared__ int s_emit_scan[2 * (kScanThreads / 32) + 3], s_emit_net[2 * (kNetThreads / 32) + 3];
+    __shared__ int s_chunk, s_staged;
+    __shared__ int s_emit[2 * (kLevelThreads / 32) + 3];
     const int t = threadIdx.x, w = t >> 5;
     const int count = min(*a.in_count, a.capacity);
-    if ((int64_t)blockIdx.x * kScanThreads >= count) return;  // no chunk can be left for this CTA
+    if ((int64_t)blockIdx.x * kLevelThreads >= count) return;  // no chunk can be left for this CTA
     float* vec = reinterpret_cast<float*>(sm + fVec);
     int2* meta = reinterpret_cast<int2*>(sm + fMeta);
     if (t == 0) {
         mbar_init(&bar, 1);
         mbar_init(&wbar, 1);
-        for (int i = 0; i < kRingSlots; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], 1);
-            s_fill[i] = 0;
-        }
         fence_mbar_init();
         mbar_arrive_expect_tx(&wbar, mlp::kImageBytes);
         bulk_g2s(sm + fW, a.weight_image, mlp::kImageBytes, &wbar);
-        s_rows = 0;
-        s_end = -1;
-        s_chunk = atomicAdd(a.work, 1);
+        s_staged = 0;
     }
-    if (w == kScanThreads / 32) tc::alloc(&tmem_base, kLevelTmemCols);  // the net group's first warp
+    for (int i = t; i < kStageRows * 2; i += kLevelThreads)  // rows past the staged ones stay finite
+        reinterpret_cast<uint4*>(sm + fX)[i] = make_uint4(0, 0, 0, 0);
+    if (w == 0) tc::alloc(&tmem_base, kLevelTmemCols);
     fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-
-    if (t < kScanThreads) {
-        // ------------------------------------------------------------------ scan group
-        bool ok = true;
-        // The next chunk's index and entries are fetched one chunk ahead, so that neither the work
-        // counter's round trip nor the entry load sits on the chain of dependent loads of a chunk.
-        int chunk = s_chunk;
-        int2 en_next = make_int2(0, 0);
-        if ((int64_t)chunk * kScanThreads + t < count) en_next = a.in[(int64_t)chunk * kScanThreads + t];
-        for (;;) {
-            // every scan thread has read s_chunk before it changes again
-            named_barrier(kScanBar, kScanThreads);
-            const int64_t first = (int64_t)chunk * kScanThreads;
-            const bool done = first >= count;
-            if (done) break;
-            const int64_t e = first + t;
-            int next = 0;
-            if (t == 0) next = atomicAdd(a.work, 1);
-            int action = kNone, tile = 0, node = 0, lc = 0, rc = 0, depth = 0;
-            if (e < count) {
-                const int2 en = en_next;
-                const bool good = valid_entry(en, a.tiles, a.n);
-                if (!good) set_error(a.err, en.x == -1 ? ARC_DEVERR_CUT_OVERFLOW : ARC_DEVERR_BAD_NODE);
-                tile = good ? en.x : 0;
-                node = good ? en.y & ((1 << kDepthShift) - 1) : 0;
-                depth = good ? en.y >> kDepthShift : 0;
-                action = good ? kAccept : kNone;
-                if (good && node >= a.n) {
-                    const int k = node - a.n;
-                    float mean;
-                    const TileInfo ti = load_tile_info(a.info, tile, &mean);
-                    const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
-                    const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
-                    const float4* rec = a.records + 4 * (size_t)node;
-                    const NodeExtra ne = load_node_extra(a.extra, k);
-                    const NodeGeom g = node_geom(ti, b0, b1, nc, wc, ne, a.bp);
-                    const float M = node_bound(ti, g, ne.Ls, ne.As, a.bp);
-                    lc = child_index(__float_as_int(b0.w), a.n);
-                    rc = child_index(__float_as_int(b1.w), a.n);
-                    if (M > ti.tau) action = M > a.band * ti.tau ? kRefine : kScore;
-                    if (action == kScore) {
-                        float f[kFeat];
-                        node_features(ti, mean, g, M, nc, wc, rec[0], rec[1], rec[2].x, ne.Ls, ne.As,
-                                      a.records + 4 * (size_t)lc, a.records + 4 * (size_t)rc, a.dirstat[node], depth,
-                                      a.clamp2, a.cos_thr, f);
-                        // a ring row: rows in lane order within each group of converged lanes, so
-                        // the staged rows (and the children they push) keep the grouping by node
-                        const unsigned am_ = __activemask();
-                        const int ldr = __ffs(am_) - 1, ln = t & 31;
-                        int r = 0;
-                        if (ln == ldr) r = atomicAdd(&s_rows, __popc(am_));
-                        r = __shfl_sync(am_, r, ldr) + __popc(am_ & ((1u << ln) - 1u));
-                        const int seq = r >> 7, slot = seq & (kRingSlots - 1), lap = seq / kRingSlots;
-                        // the slot's previous lap has been read by the net group
-                        if (ok) ok = mbar_wait_bounded(&empty[slot], (uint32_t)((lap & 1) ^ 1), a.err);
-                        if (ok) {
-                            const int rr = r & (kRingRows - 1);
-                            uint4 x0, x1;
-                            x0.x = mlp::pack2(f[0], f[1]);
-                            x0.y = mlp::pack2(f[2], f[3]);
-                            x0.z = mlp::pack2(f[4], f[5]);
-                            x0.w = mlp::pack2(f[6], f[7]);
-                            x1.x = mlp::pack2(f[8], f[9]);
-                            x1.y = mlp::pack2(f[10], f[11]);
-                            x1.z = mlp::pack2(f[12], f[13]);
-                            x1.w = mlp::pack2(f[14], f[15]);
-                            *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(rr, 0, kFeat)) = x0;
-                            *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(rr, 8, kFeat)) = x1;
-                            meta[rr] = make_int2(tile, node | (depth << kDepthShift));
-                            // the row reaches the tensor cores (async proxy) and the net group
-                            fence_proxy_async_smem();
-                            __threadfence_block();
-                            if (atomicAdd(&s_fill[slot], 1) == 128 * lap + 127) {
-                                __threadfence_block();
-                                mbar_arrive(&full[slot]);
-                            }
-                        }
-                    }
-                }
-            }
-            if (t == 0) s_chunk = next;
-            emit<kScanBar, kScanThreads>(a, s_emit_scan, t, action == kScore ? kNone : action, tile, node, lc, rc,
-                                         depth);
-            chunk = s_chunk;  // emit's barriers order the store before this read
-            const int64_t en = (int64_t)chunk * kScanThreads + t;
-            if (en < count) en_next = a.in[en];
-        }
-        // the level is exhausted: every row is written (the barrier above); pad the last partial
-        // slot with empty rows and publish the total
-        if (t == 0) {
-            const int total = s_rows;
-            const int padded = (total + 127) & ~127;
-            if (padded > total && ok) {
-                const int seq = total >> 7, slot = seq & (kRingSlots - 1), lap = seq / kRingSlots;
-                // (the slot's previous lap was awaited by the writers of its real rows)
-                for (int r = total; r < padded; ++r) {
-                    const int rr = r & (kRingRows - 1);
-                    *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(rr, 0, kFeat)) = make_uint4(0, 0, 0, 0);
-                    *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(rr, 8, kFeat)) = make_uint4(0, 0, 0, 0);
-                    meta[rr] = make_int2(-1, 0);
-                }
-                fence_proxy_async_smem();
-                __threadfence_block();
-                if (atomicAdd(&s_fill[slot], padded - total) + (padded - total) == 128 * (lap + 1)) {
-                    __threadfence_block();
-                    mbar_arrive(&full[slot]);
-                }
-            }
-            __threadfence_block();
-            *reinterpret_cast<volatile int*>(&s_end) = ok ? padded : 0;
-        }
-        return;
-    }
-
-    // ---------------------------------------------------------------------- net group
-    const int tn = t - kScanThreads;
-    bool ok = named_barrier_and(kNetBar, kNetThreads, mbar_wait_bounded(&wbar, 0, a.err));
+    bool ok = __syncthreads_and(mbar_wait_bounded(&wbar, 0, a.err)) != 0;
     bool mma_gave_up = false;  // a tensor-core wait gave up: its commit may still be in flight
     mlp::InferCta c{smem_u32(sm), fW, fH, sm, vec, tmem_base, &bar, 0u, a.err};
     unsigned long long scored = 0;
-    for (int seq = 0; ok; ++seq) {
-        const int slot = seq & (kRingSlots - 1), lap = seq / kRingSlots;
-        // wait for the slot to fill, or for the level to end before it (bounded)
-        bool got = false, end = false;
-        for (uint32_t i = 0; i < (1u << 24) && !got && !end; ++i) {
-            got = mbar_try_wait(&full[slot], (uint32_t)(lap & 1));
-            if (!got) {
-                const int e_ = *reinterpret_cast<volatile int*>(&s_end);
-                end = e_ >= 0 && seq * 128 >= e_;
+    // The next chunk's index and entries are fetched one chunk ahead, so that neither the work
+    // counter's round trip nor the entry load sits on the chain of dependent loads of a chunk.
+    if (t == 0) s_chunk = atomicAdd(a.work, 1);
+    __syncthreads();
+    int chunk = s_chunk;
+    int2 en_next = make_int2(0, 0);
+    if ((int64_t)chunk * kLevelThreads + t < count) en_next = a.in[(int64_t)chunk * kLevelThreads + t];
+    while (ok) {
+        // every thread has read s_chunk and s_staged before they change again
+        __syncthreads();
+        const int64_t first = (int64_t)chunk * kLevelThreads;
+        const bool done = first >= count;
+        const int64_t e = first + t;
+        int next = 0;
+        if (t == 0 && !done) next = atomicAdd(a.work, 1);
+        int action = kNone, tile = 0, node = 0, lc = 0, rc = 0, depth = 0;
+        if (!done && e < count) {
+            const int2 en = en_next;
+            const bool good = valid_entry(en, a.tiles, a.n);
+            if (!good) set_error(a.err, en.x == -1 ? ARC_DEVERR_CUT_OVERFLOW : ARC_DEVERR_BAD_NODE);
+            tile = good ? en.x : 0;
+            node = good ? en.y & ((1 << kDepthShift) - 1) : 0;
+            depth = good ? en.y >> kDepthShift : 0;
+            action = good ? kAccept : kNone;
+            if (good && node >= a.n) {
+                const int k = node - a.n;
+                float mean;
+                const TileInfo ti = load_tile_info(a.info, tile, &mean);
+                const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
+                const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
+                const float4* rec = a.records + 4 * (size_t)node;
+                const NodeExtra ne = load_node_extra(a.extra, k);
+                const NodeGeom g = node_geom(ti, b0, b1, nc, wc, ne, a.bp);
+                const float M = node_bound(ti, g, ne.Ls, ne.As, a.bp);
+                lc = child_index(__float_as_int(b0.w), a.n);
+                rc = child_index(__float_as_int(b1.w), a.n);
+                if (M > ti.tau) action = M > a.band * ti.tau ? kRefine : kScore;
+                if (action == kScore) {
+                    float f[kFeat];
+                    node_features(ti, mean, g, M, nc, wc, rec[0], rec[1], rec[2].x, ne.Ls, ne.As, a.records + 4 * (size_t)lc,
+                                  a.records + 4 * (size_t)rc, a.dirstat[node], depth, a.clamp2, a.cos_thr, f);
+                    // < kStageRows: fewer than kLevelThreads rows are left over from the last round.
+                    // Slots in thread order within each group of converged lanes, so the staged rows
+                    // (and the children they push) keep the frontier's grouping by node.
+                    const unsigned sm_ = __activemask();
+                    const int ldr = __ffs(sm_) - 1, ln = threadIdx.x & 31;
+                    int slot = 0;
+                    if (ln == ldr) slot = atomicAdd(&s_staged, __popc(sm_));
+                    slot = __shfl_sync(sm_, slot, ldr) + __popc(sm_ & ((1u << ln) - 1u));
+                    uint4 x0, x1;
+                    x0.x = mlp::pack2(f[0], f[1]);
+                    x0.y = mlp::pack2(f[2], f[3]);
+                    x0.z = mlp::pack2(f[4], f[5]);
+                    x0.w = mlp::pack2(f[6], f[7]);
+                    x1.x = mlp::pack2(f[8], f[9]);
+                    x1.y = mlp::pack2(f[10], f[11]);
+                    x1.z = mlp::pack2(f[12], f[13]);
+                    x1.w = mlp::pack2(f[14], f[15]);
+                    *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(slot, 0, kFeat)) = x0;
+                    *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(slot, 8, kFeat)) = x1;
+                    meta[slot] = make_int2(tile, node | (depth << kDepthShift));
+                }
             }
         }
-        if (!got && !end) set_error(a.err, ARC_DEVERR_TIMEOUT);
-        // every thread of the group sees the same outcome: a slot that filled completes for all
-        if (!named_barrier_and(kNetBar, kNetThreads, got)) break;
-        const int rr = seq * 128 + tn;
-        const int2 m = meta[rr & (kRingRows - 1)];
-        const bool valid = m.x >= 0;
-        const int mnode = m.y & ((1 << kDepthShift) - 1), mdepth = m.y >> kDepthShift;
-        // the children of the row's (inner) node are fetched while the network runs
-        int cl = 0, cr = 0;
-        if (valid && mnode >= a.n) {
-            const size_t k = (size_t)(mnode - a.n);
-            cl = __float_as_int(a.bounds[4 * k].w);
-            cr = __float_as_int(a.bounds[4 * k + 1].w);
+        if (t == 0 && !done) s_chunk = next;
+        // emit's barriers also order every staging of this chunk before s_staged is read
+        emit(a, s_emit, action, tile, node, lc, rc, depth);
+        if (!done) {
+            chunk = s_chunk;
+            const int64_t en = (int64_t)chunk * kLevelThreads + t;
+            if (en < count) en_next = a.in[en];
         }
-        float y = 0.0f;
-        if (!mlp::infer_tiles<1, kNetBar>(c, fX + (uint32_t)slot * 4096u, tn, &y)) {
-            ok = false;
-            mma_gave_up = true;
-            break;
+        int staged = s_staged;
+        // score full tiles now, and whatever is left once the level is exhausted
+        while (staged >= kLevelThreads || (done && staged > 0)) {
+            const int n_rows = min(staged, kLevelThreads);
+            // the children of every staged (inner) node are fetched while the network runs
+            int2 m = make_int2(0, 0);
+            int cl = 0, cr = 0;
+            if (t < n_rows) {
+                m = meta[t];
+                const int mn = m.y & ((1 << kDepthShift) - 1);
+                if (mn >= a.n) {
+                    const size_t k = (size_t)(mn - a.n);
+                    cl = __float_as_int(a.bounds[4 * k].w);
+                    cr = __float_as_int(a.bounds[4 * k + 1].w);
+                }
+            }
+            float y = 0.0f;
+            if (!mlp::infer_tiles<kLevelTiles>(c, fX, t, &y)) {
+                ok = false;
+                mma_gave_up = true;
+                break;
+            }
+            scored += n_rows;
+            const int act = t < n_rows ? (y >= a.thr_logit ? kRefine : kAccept) : kNone;
+            const int mnode = m.y & ((1 << kDepthShift) - 1), mdepth = m.y >> kDepthShift;
+            const int mlc = child_index(cl, a.n), mrc = child_index(cr, a.n);
+            // after emit's barriers every thread has read its pair: the rows can be moved
+            emit(a, s_emit, act, m.x, mnode, mlc, mrc, mdepth);
+            const int rest = staged - n_rows;
+            if (t < rest) {
+                const int r = kLevelThreads + t;
+                *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(t, 0, kFeat)) =
+                    *reinterpret_cast<const uint4*>(sm + fX + tc::kmajor_offset(r, 0, kFeat));
+                *reinterpret_cast<uint4*>(sm + fX + tc::kmajor_offset(t, 8, kFeat)) =
+                    *reinterpret_cast<const uint4*>(sm + fX + tc::kmajor_offset(r, 8, kFeat));
+                meta[t] = meta[r];
+            }
+            if (t == 0) s_staged = rest;
+            // the next round's first barrier (in infer_tiles) or the next chunk's orders these moves
+            staged = rest;
         }
-        scored += valid ? 1 : 0;
-        const int act = valid ? (y >= a.thr_logit ? kRefine : kAccept) : kNone;
-        emit<kNetBar, kNetThreads>(a, s_emit_net, tn, act, m.x, mnode, child_index(cl, a.n), child_index(cr, a.n),
-                                   mdepth);
-        // emit's barriers: every net thread has read its row and pair; the slot goes back to the scan group
-        if (tn == 0) mbar_arrive(&empty[slot]);
+        if (!ok || done) break;
     }
-    if (scored) atomicAdd(a.rows_scored, scored);
-    if (!ok && tn == 0) {
+    if (t == 0 && scored) atomicAdd(a.rows_scored, scored);
+    if (!ok && t == 0) {
         // a bounded wait gave up (the error word says so): before this CTA's shared memory and
         // TMEM are released, give its weight copy and its last tensor-core commit a second
         // bounded wait (the failed wait has already flipped the phase)
@@ -496,8 +437,8 @@ __global__ void __launch_bounds__(kLevelBlock, 2) learned_level(LevelArgs a) {
         if (mma_gave_up) mbar_wait_bounded(&bar, c.phase ^ 1u, a.err);
     }
     tc::fence_before_sync();
-    named_barrier(kNetBar, kNetThreads);
-    if (w == kScanThreads / 32) tc::dealloc(tmem_base, kLevelTmemCols);
+    __syncthreads();
+    if (w == 0) tc::dealloc(tmem_base, kLevelTmemCols);
 }
 
 // Past the last level the host runs: every pair still in the frontier is accepted.
@@ -926,7 +867,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     int smem_sm = 0;
     ARC_TRY_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
     // (1 KB per CTA reserved by the system, plus the kernel's static shared variables)
-    const int per_sm = std::max(1, std::min(2, std::min(512 / (int)kLevelTmemCols, smem_sm / (int)(kLevelSmem + 1280))));
+    const int per_sm = std::max(1, std::min(512 / (int)kLevelTmemCols, smem_sm / (int)(kLevelSmem + 1280)));
     ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmem));
     ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));
@@ -947,7 +888,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
         la.work = counters + 8 + 4 * level + 2;
         la.out = nxt;
         la.out_count = counters + 8 + 4 * (level + 1);
-        learned_level<<<ctx->sm_count * per_sm, kLevelBlock, kLevelSmem, st>>>(la);
+        learned_level<<<ctx->sm_count * per_sm, kLevelThreads, kLevelSmem, st>>>(la);
         ++kernels;
         std::swap(cur, nxt);
     }

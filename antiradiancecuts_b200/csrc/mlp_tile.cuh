@@ -108,36 +108,19 @@ struct InferCta {
     uint32_t* err;
 };
 
-// The threads that run the inference synchronise either as the whole CTA (BarId < 0) or as a group
-// of NT threads on named barrier BarId (a warp-specialised CTA whose other warps do other work).
-template <int BarId, int NT>
-__device__ __forceinline__ void group_sync() {
-    if (BarId < 0)
-        __syncthreads();
-    else
-        named_barrier(BarId, NT);
-}
-template <int BarId, int NT>
-__device__ __forceinline__ bool group_and(bool v) {
-    if (BarId < 0) return __syncthreads_and(v) != 0;
-    return named_barrier_and(BarId, NT, v);
-}
-
 // Waits for the MMAs committed on the barrier; every thread learns whether all threads got there.
-template <int BarId = -1, int NT = 0>
 __device__ __forceinline__ bool wait_mma(InferCta& c) {
     const bool ok = mbar_wait_bounded(c.bar, c.phase, c.err);
     c.phase ^= 1u;
     tc::fence_after_sync();
-    return group_and<BarId, NT>(ok);
+    return __syncthreads_and(ok) != 0;
 }
 
 // Makes this thread's generic-proxy smem writes visible to the tensor cores, then barrier.
-template <int BarId = -1, int NT = 0>
 __device__ __forceinline__ void publish_smem() {
     fence_proxy_async_smem();
     tc::fence_before_sync();
-    group_sync<BarId, NT>();
+    __syncthreads();
 }
 
 // TMEM address of thread t's row: tile t / 128 owns accumulator columns 64 (t / 128) ..+63, and a
@@ -170,18 +153,16 @@ __device__ __forceinline__ void hidden_epilogue(const InferCta& c, int t, const 
     }
 }
 
-// Logits of NT 128-row tiles: row t (of 128 NT, one per thread of the group) of the K-major input
+// Logits of NT 128-row tiles: row t (of 128 NT, one per thread of the CTA) of the K-major input
 // rows at smem offset x (stride between 8-row groups: 256 bytes), hidden rows at c.h (1024 bytes
 // between 8-row groups), tile u's accumulator in TMEM columns 64 u .. 64 u + 63.  Called by all
-// 128 NT threads of the group (the CTA, or named barrier BarId); returns false (every thread) if a
-// tensor-core wait gave up, after which the caller frees its TMEM and stops.  The group's warps
-// must be aligned to TMEM lane quarters: row t is read by warp (t / 32) % 4 of its group.
-template <int NT, int BarId = -1>
+// 128 NT threads; returns false (every thread) if a tensor-core wait gave up, after which the
+// caller frees its TMEM and stops.
+template <int NT>
 __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, float* logit) {
     constexpr uint32_t id = tc::idesc_bf16(128, 64, false, false);
-    constexpr int kThreads = 128 * NT;
     // layer 1 (K = 16)
-    publish_smem<BarId, kThreads>();
+    publish_smem();
     if (t == 0) {
         tc::fence_after_sync();
 #pragma unroll
@@ -190,12 +171,12 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
                     tc::smem_desc(c.base + c.w + kW1, 128, 256), id, false);
         tc::commit(c.bar);
     }
-    if (!wait_mma<BarId, kThreads>(c)) return false;
+    if (!wait_mma(c)) return false;
     hidden_epilogue(c, t, c.vec);
     // layers 2 and 3 (K = 64); layer 2 overwrites the hidden buffer it read once its MMAs are done
 #pragma unroll 1
     for (int l = 0; l < 2; ++l) {
-        publish_smem<BarId, kThreads>();
+        publish_smem();
         if (t == 0) {
             tc::fence_after_sync();
             const uint32_t wb = c.w + (l == 0 ? kW2 : kW3);
@@ -207,7 +188,7 @@ __device__ __forceinline__ bool infer_tiles(InferCta& c, uint32_t x, int t, floa
                             tc::smem_desc(c.base + wb + 256 * s, 128, 1024), id, s > 0);
             tc::commit(c.bar);
         }
-        if (!wait_mma<BarId, kThreads>(c)) return false;
+        if (!wait_mma(c)) return false;
         if (l == 0) hidden_epilogue(c, t, c.vec + 64);
     }
     // layer 3 epilogue and the 64 -> 1 output layer on the CUDA cores
