@@ -159,22 +159,31 @@ def max_over_ranks(world, x: float) -> float:
     return float(t.item())
 
 
+def host_threads() -> int:
+    """The host cores this process may run on (its affinity mask, not the machine's count)."""
+    try:
+        return len(os.sched_getaffinity(0)) or 1
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s: float, threads: int):
     """Runs the scalar FP32 CPU gather over chunks of the pixel list `order` until target_s seconds
     of gather time are spent (or the list is done) -> (pixels gathered, seconds).  Every chunk is a
     multiple of `threads` pixels and the gather hands out one pixel at a time, so no thread idles
     while another still has pixels; after the first chunk each is sized to about a quarter of the
     remaining time at the rate measured so far."""
-    k, dt, chunk = 0, 0.0, threads
+    k, dt, cpu, chunk = 0, 0.0, 0.0, threads
     while k < len(order) and dt < target_s:
         part = order[k:k + chunk]
-        t0 = time.perf_counter()
+        t0, c0 = time.perf_counter(), time.process_time()
         O.gather_fp32(pos, nrm, part, avpls, dif, spe, ex, cam, prm, threads=threads)
         dt += time.perf_counter() - t0
+        cpu += time.process_time() - c0
         k += len(part)
         want = (k / max(dt, 1e-6)) * max(target_s - dt, 0.0) / 4
         chunk = max(threads, int(want // threads) * threads)
-    return k, dt
+    return k, dt, cpu
 
 
 def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, threads: int, ref64=None,
@@ -188,13 +197,13 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
     prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
     valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
     order = np.random.default_rng(7).permutation(valid)
-    k, dt = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s, threads)
+    k, dt, cpu = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s, threads)
     # every pixel costs the same (all AVPLs); background pixels cost nothing, so extrapolate over
     # the valid pixels
     ms_frame = dt * 1e3 * len(valid) / max(k, 1)
     single = None
     if single_s > 0:
-        k1, dt1 = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, single_s, 1)
+        k1, dt1, _ = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, single_s, 1)
         single = {"value": dt1 * 1e3 * len(valid) / max(k1, 1), "unit": UNIT, "cores": 1,
                   "sample": f"{k1} random surface pixels x {len(avpls)} AVPLs, {dt1:.1f} s"}
     sample = order[:k]
@@ -206,7 +215,10 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
         check = float(np.max(np.sqrt(np.mean(d ** 2, 0)) / (np.sqrt(np.mean(o64 ** 2, 0)) + 1e-300)))
     out = {"value": ms_frame, "unit": UNIT, "cores": threads, "kind": "port",
            "sample": f"{k} random surface pixels x {len(avpls)} AVPLs (scalar FP32 C, -O3, {threads} threads, "
-                     f"one pixel per work item), {dt:.1f} s, extrapolated to {len(valid)} surface pixels"}
+                     f"one pixel per work item), {dt:.1f} s, extrapolated to {len(valid)} surface pixels",
+           # the host is shared with other jobs: the cores the gather actually got (process CPU time
+           # over wall time) and the load average when it ran
+           "cpu_seconds_per_second": cpu / max(dt, 1e-9), "loadavg_1min": os.getloadavg()[0]}
     if single is not None:
         out["single_thread"] = single
     if ref64 is not None:
@@ -511,15 +523,18 @@ def run_reference(args):
     desc, avpls, paths, pos, nrm = wl.build(lib=L.load_scene_library(O.INPUTS_LIB))
     _, dif, spe, ex = scene.materials(desc)
     cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
-    vals = []
+    vals, cores = [], []
     for i in range(args.warmup + args.steps):
         b = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, per, threads)
         if i >= args.warmup:
             vals.append(b["value"])
+            cores.append(b["cpu_seconds_per_second"])
     v = float(np.median(vals))
     b["value"] = v
+    b["per_step_values"] = [round(x, 1) for x in vals]
+    b["per_step_cpu_seconds_per_second"] = [round(x, 2) for x in cores]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -790,7 +805,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_extras:
-        cpu = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, args.cpu_seconds, os.cpu_count() or 1,
+        cpu = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, args.cpu_seconds, host_threads(),
                            ref64=ref64, single_s=args.cpu_single_seconds)
         result["fp64_image_vs_cpu_oracle_rel_rmse"] = cpu.pop("fp64_image_vs_oracle_rel_rmse")
 
