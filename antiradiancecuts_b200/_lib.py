@@ -38,6 +38,7 @@ ARC_PREC_KAHAN, ARC_PREC_KAHAN_STRICT, ARC_PREC_NAIVE, ARC_PREC_FP64 = 0, 1, 2, 
 ARC_BBOX_SCENE, ARC_BBOX_AVPL_REFERENCE = 0, 1
 ARC_CUT_SOLID_ANGLE, ARC_CUT_ERROR_BOUND, ARC_CUT_LEARNED = 0, 1, 2
 ARC_MLP_LOSS_BCE, ARC_MLP_LOSS_SQUARED = 0, 1
+ARC_MLP_ACT_GELU, ARC_MLP_ACT_RELU = 0, 1
 ARC_SCENE_ROOM, ARC_SCENE_ROOM_2BOXES, ARC_SCENE_ROOM_RANDOM, ARC_SCENE_TRAIN_VARIANT = 0, 1, 2, 3
 
 
@@ -213,6 +214,8 @@ SIGNATURES = {
     "arc_mlp_train_step": (_st, [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float, _vp]),
     "arc_mlp_set_loss": (_st, [_vp, C.c_int32]),
     "arc_mlp_get_loss": (C.c_int32, [_vp]),
+    "arc_mlp_set_activation": (_st, [_vp, C.c_int32]),
+    "arc_mlp_get_activation": (C.c_int32, [_vp]),
     "arc_cut_training_samples": (_st, [_vp, _vp, P(ArcGBufferView), ArcFloat3, P(ArcGatherParams), P(ArcCutParams),
                                        C.c_float, _vp, _vp, _vp, _vp, C.c_int32, P(C.c_int32)]),
     "arc_run": (_st, [_vp, P(ArcAvplHost), C.c_int32, ArcFloat3, C.c_float, P(ArcRunConfig), P(ArcGBufferView),

@@ -44,6 +44,7 @@ namespace arc {
 
 const float* mlp_params(const arc_mlp* m);
 int32_t mlp_loss_kind(const arc_mlp* m);
+int32_t mlp_activation(const arc_mlp* m);
 
 namespace {
 
@@ -279,10 +280,12 @@ constexpr uint32_t fW = 0, fVec = mlp::kWeightBytes, fX = ((mlp::kImageBytes + 1
 constexpr uint32_t kLevelTmemCols = 64 * kLevelTiles;
 
 // BF16 core-matrix weights + FP32 vectors, once per selection
+template <int ACT>
 __global__ void weight_image(const float* params, unsigned char* img) {
-    mlp::load_weights(img, reinterpret_cast<float*>(img + mlp::kWeightBytes), params, threadIdx.x, blockDim.x);
+    mlp::load_weights<ACT>(img, reinterpret_cast<float*>(img + mlp::kWeightBytes), params, threadIdx.x, blockDim.x);
 }
 
+template <int ACT>
 __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar, wbar;
@@ -402,7 +405,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
                 }
             }
             float y = 0.0f;
-            if (!mlp::infer_tiles<kLevelTiles>(c, fX, t, &y)) {
+            if (!mlp::infer_tiles<kLevelTiles, ACT>(c, fX, t, &y)) {
                 ok = false;
                 mma_gave_up = true;
                 break;
@@ -563,6 +566,47 @@ __global__ void scatter_nodes(ScatterArgs s) {
         const int id = s.chunk_base[p.x] + pos / kChunk;
         if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p.x])
             s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p.y;
+    }
+}
+
+// The same scatter with the per-tile slot reservations binned in shared memory, for frames whose
+// tile counters fit there (tiles * 4 bytes of dynamic shared memory).  A CTA takes segments of
+// kBinSegment accepted pairs: it counts the segment's pairs per tile with shared-memory atomics,
+// reserves each tile's run with one global atomic per tile present, then reads the segment again
+// and hands out the slots of each run.  The accepted list comes grouped by node, so a warp's 32
+// pairs mostly name 32 different tiles: reserving per pair (scatter_nodes) costs one global atomic
+// each, and binning a large segment cuts that to one per (segment, tile).
+constexpr int kBinSegment = 1 << 19;
+
+__global__ void __launch_bounds__(1024) scatter_nodes_binned(ScatterArgs s, int tiles) {
+    extern __shared__ int bins[];  // [tiles]: counts, then each tile's next slot
+    const int count = (int)min((unsigned)*s.acc_count, (unsigned)s.acc_capacity);
+    for (int64_t seg = (int64_t)blockIdx.x * kBinSegment; seg < count; seg += (int64_t)gridDim.x * kBinSegment) {
+        const int end = (int)(seg + kBinSegment < (int64_t)count ? seg + kBinSegment : (int64_t)count);
+        for (int t = threadIdx.x; t < tiles; t += blockDim.x) bins[t] = 0;
+        __syncthreads();
+        for (int e = (int)seg + threadIdx.x; e < end; e += blockDim.x) {
+            const int tile = s.accepted[e].x;
+            if ((unsigned)tile < (unsigned)tiles) atomicAdd(&bins[tile], 1);
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
+            const int c = bins[t];
+            if (c) bins[t] = atomicAdd(&s.fill[t], c);
+        }
+        __syncthreads();
+        for (int e = (int)seg + threadIdx.x; e < end; e += blockDim.x) {
+            const int2 p = s.accepted[e];
+            if ((unsigned)p.x >= (unsigned)tiles) {
+                set_error(s.err, ARC_DEVERR_BAD_NODE);
+                continue;
+            }
+            const int pos = atomicAdd(&bins[p.x], 1);
+            const int id = s.chunk_base[p.x] + pos / kChunk;
+            if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p.x])
+                s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p.y;
+        }
+        __syncthreads();  // the bins are zeroed for the next segment only after every thread is done
     }
 }
 
@@ -868,13 +912,18 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     ARC_TRY_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
     // (1 KB per CTA reserved by the system, plus the kernel's static shared variables)
     const int per_sm = std::max(1, std::min(512 / (int)kLevelTmemCols, smem_sm / (int)(kLevelSmem + 1280)));
-    ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmem));
-    ARC_TRY_CUDA(cudaFuncSetAttribute(learned_level, cudaFuncAttributePreferredSharedMemoryCarveout,
+    const bool relu = mlp_activation(cp->model) == ARC_MLP_ACT_RELU;
+    auto* level_kernel = relu ? learned_level<mlp::kActRelu> : learned_level<mlp::kActGelu>;
+    ARC_TRY_CUDA(cudaFuncSetAttribute(level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmem));
+    ARC_TRY_CUDA(cudaFuncSetAttribute(level_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));
     stage_begin(ctx, "cut_learned");
     int kernels = 0;
     const int grid = ctx->sm_count * 8;
-    weight_image<<<1, 256, 0, st>>>(mlp_params(cp->model), img);
+    if (relu)
+        weight_image<mlp::kActRelu><<<1, 256, 0, st>>>(mlp_params(cp->model), img);
+    else
+        weight_image<mlp::kActGelu><<<1, 256, 0, st>>>(mlp_params(cp->model), img);
     init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, counters + 8, info, tiles, n);
     kernels += 2;
     int2 *cur = fa, *nxt = fb;
@@ -888,7 +937,7 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
         la.work = counters + 8 + 4 * level + 2;
         la.out = nxt;
         la.out_count = counters + 8 + 4 * (level + 1);
-        learned_level<<<ctx->sm_count * per_sm, kLevelThreads, kLevelSmem, st>>>(la);
+        level_kernel<<<ctx->sm_count * per_sm, kLevelThreads, kLevelSmem, st>>>(la);
         ++kernels;
         std::swap(cur, nxt);
     }
@@ -908,7 +957,19 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     sa.err = ctx->d_error;
     tile_chunk_scan<<<1, 1024, 0, st>>>(tile_counts, tiles, chunk_base, counters + 4, pool.max_chunks, ctx->d_error);
     scatter_tables<<<(tiles + 255) / 256, 256, 0, st>>>(sa, tiles);
-    scatter_nodes<<<grid, 256, 0, st>>>(sa);
+    // binned in shared memory when the tile counters fit (1080p: 32,400 tiles, 130 KB)
+    int smem_optin = 0;
+    ARC_TRY_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const size_t bin_bytes = sizeof(int) * (size_t)tiles;
+    if (bin_bytes <= (size_t)smem_optin) {
+        // the device's full opt-in size, never lowered: graphs recorded for other frame sizes keep
+        // their launches valid
+        ARC_TRY_CUDA(cudaFuncSetAttribute(scatter_nodes_binned, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          smem_optin));
+        scatter_nodes_binned<<<ctx->sm_count, 1024, bin_bytes, st>>>(sa, tiles);
+    } else {
+        scatter_nodes<<<grid, 256, 0, st>>>(sa);
+    }
     kernels += 3;
     ARC_TRY_CUDA(cudaMemcpyAsync(pool.next, counters + 4, sizeof(int), cudaMemcpyDeviceToDevice, st));
     stage_end(ctx, kernels);

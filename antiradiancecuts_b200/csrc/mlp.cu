@@ -1,9 +1,9 @@
-// The cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, GELU, BF16 weights, FP32 accumulation) on
+// The cut-refinement MLP (16 -> 64 -> 64 -> 64 -> 1, GELU or ReLU, BF16 weights, FP32 accumulation) on
 // the 5th-generation tensor cores.  No counterpart in the reference: it predicts, for an 8x8 pixel
 // tile and a tree node, whether the cut must refine the node.
 //
 // Two kernels.  Each 128-thread CTA walks 128-row tiles of the input (thread t owns row t):
-//   forward   X[128x16] -> tcgen05.mma -> TMEM -> +b, GELU -> BF16 core-matrix smem -> next layer;
+//   forward   X[128x16] -> tcgen05.mma -> TMEM -> +b, activation -> BF16 core-matrix smem -> next layer;
 //             the 64 -> 1 output layer runs on the CUDA cores from registers (mlp_tile.cuh, shared
 //             with the fused level kernel of the learned cut).
 //   training  the forward pass, then BCE gradient, and the backward pass:
@@ -105,13 +105,14 @@ __device__ __forceinline__ void accumulate_columns(const float* v, float* g, int
 }
 
 // Forward over every row of the input: persistent CTAs, one 128-row tile at a time.
+template <int ACT>
 __global__ void __launch_bounds__(128) mlp_infer_kernel(Args a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_base;
     const int t = threadIdx.x, w = t >> 5;
     float* vec = reinterpret_cast<float*>(sm + sInVec);
-    load_weights(sm, vec, a.params, t, 128);
+    load_weights<ACT>(sm, vec, a.params, t, 128);
     if (w == 0) tc::alloc(&tmem_base, 64);
     if (t == 0) {
         mbar_init(&bar, 1);
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(Args a) {
         *reinterpret_cast<uint4*>(sm + sInX + tc::kmajor_offset(t, 0, kIn)) = x0;
         *reinterpret_cast<uint4*>(sm + sInX + tc::kmajor_offset(t, 8, kIn)) = x1;
         float y;
-        if (!infer_tile(c, sInX, t, &y)) {
+        if (!infer_tile<ACT>(c, sInX, t, &y)) {
             // the wait gave up (the error word says so): its commit gets a second bounded wait
             // before the TMEM and shared memory are released (the failed wait flipped the phase)
             if (t == 0) mbar_wait_bounded(&bar, c.phase ^ 1u, a.err);
@@ -149,6 +150,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(Args a) {
 }
 
 // Forward + backward with weight-gradient accumulation in TMEM (training).
+template <int ACT>
 __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -258,7 +260,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
 #pragma unroll
         for (int j = 0; j < 64; ++j) {
             z[j] += b1[j];
-            h[j] = gelu(z[j]);
+            h[j] = act<ACT>(z[j]);
         }
         store_row64(sm + sH1, t, h);
         store_row64(sm + sZ1, t, z);
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
 #pragma unroll
         for (int j = 0; j < 64; ++j) {
             z[j] += b2[j];
-            h[j] = gelu(z[j]);
+            h[j] = act<ACT>(z[j]);
         }
         store_row64(sm + sH2, t, h);
         store_row64(sm + sZ2, t, z);
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
 #pragma unroll
         for (int j = 0; j < 64; ++j) {
             z[j] += b3[j];
-            h[j] = gelu(z[j]);
+            h[j] = act<ACT>(z[j]);
         }
         // ---- output layer on the CUDA cores ----
         float y = b4;
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         for (int j = 0; j < 64; ++j) g[j] = dy * h[j];
         accumulate_columns(g, gw4, lane);
 #pragma unroll
-        for (int j = 0; j < 64; ++j) g[j] = dy * w4[j] * gelu_grad(z[j]);  // dZ3
+        for (int j = 0; j < 64; ++j) g[j] = dy * w4[j] * act_grad<ACT>(z[j]);  // dZ3
         accumulate_columns(g, gb3, lane);
         store_row64(sm + sDZ, t, g);
         // dW3 += dZ3^T H2 ; dH2 = dZ3 W3
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         load_tmem64(tmem + lane_off, g);  // dH2
         load_row64(sm + sZ2, t, z);
 #pragma unroll
-        for (int j = 0; j < 64; ++j) g[j] *= gelu_grad(z[j]);  // dZ2
+        for (int j = 0; j < 64; ++j) g[j] *= act_grad<ACT>(z[j]);  // dZ2
         accumulate_columns(g, gb2, lane);
         store_row64(sm + sDZ, t, g);
         // dW2 += dZ2^T H1 ; dH1 = dZ2 W2
@@ -358,7 +360,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(Args a) {
         load_tmem64(tmem + lane_off, g);  // dH1
         load_row64(sm + sZ1, t, z);
 #pragma unroll
-        for (int j = 0; j < 64; ++j) g[j] *= gelu_grad(z[j]);  // dZ1
+        for (int j = 0; j < 64; ++j) g[j] *= act_grad<ACT>(z[j]);  // dZ1
         accumulate_columns(g, gb1, lane);
         store_row64(sm + sDZ, t, g);
         // dW1 += dZ1^T X  (N = 16)
@@ -436,6 +438,7 @@ struct arc_mlp {
     float* loss = nullptr;
     int64_t step = 0;
     int32_t loss_kind = ARC_MLP_LOSS_BCE;
+    int32_t activation = ARC_MLP_ACT_GELU;
 };
 
 namespace {
@@ -459,19 +462,20 @@ arc_status mlp_launch(arc_mlp* m, bool train, const void* x, int64_t rows, float
     if (tiles == 0) return ARC_OK;
     // the shared-memory limit is a per-device attribute of the kernel: set it on every call (a
     // host-side call), not once per process, so contexts on other devices get it too
+    const bool relu = m->activation == ARC_MLP_ACT_RELU;
     if (train) {
-        ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)mlp::kSmemTrain));
+        auto* k = relu ? mlp::mlp_train_kernel<mlp::kActRelu> : mlp::mlp_train_kernel<mlp::kActGelu>;
+        ARC_TRY_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp::kSmemTrain));
         const int grid = (int)std::min<int64_t>(tiles, ctx->sm_count);
         stage_begin(ctx, "mlp_train");
-        mlp::mlp_train_kernel<<<grid, 128, mlp::kSmemTrain, ctx->stream>>>(a);
+        k<<<grid, 128, mlp::kSmemTrain, ctx->stream>>>(a);
         stage_end(ctx, 1);
     } else {
-        ARC_TRY_CUDA(cudaFuncSetAttribute(mlp::mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)mlp::kSmemInfer));
+        auto* k = relu ? mlp::mlp_infer_kernel<mlp::kActRelu> : mlp::mlp_infer_kernel<mlp::kActGelu>;
+        ARC_TRY_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp::kSmemInfer));
         const int grid = (int)std::min<int64_t>(tiles, (int64_t)ctx->sm_count * 4);
         stage_begin(ctx, "mlp_forward");
-        mlp::mlp_infer_kernel<<<grid, 128, mlp::kSmemInfer, ctx->stream>>>(a);
+        k<<<grid, 128, mlp::kSmemInfer, ctx->stream>>>(a);
         stage_end(ctx, 1);
     }
     ARC_TRY_CUDA(cudaGetLastError());
@@ -483,6 +487,7 @@ arc_status mlp_launch(arc_mlp* m, bool train, const void* x, int64_t rows, float
 namespace arc {
 const float* mlp_params(const arc_mlp* m) { return m->params; }
 int32_t mlp_loss_kind(const arc_mlp* m) { return m->loss_kind; }
+int32_t mlp_activation(const arc_mlp* m) { return m->activation; }
 arc_status mlp_forward_device(arc_mlp* m, const void* x, int64_t rows, float* logits) {
     return mlp_launch(m, false, x, rows, logits, nullptr, nullptr, 0.0f);
 }
@@ -599,6 +604,15 @@ arc_status arc_mlp_set_loss(arc_mlp* m, int32_t kind) {
 }
 
 int32_t arc_mlp_get_loss(const arc_mlp* m) { return m ? m->loss_kind : -1; }
+
+arc_status arc_mlp_set_activation(arc_mlp* m, int32_t kind) {
+    ARC_CHECK_ARG(m, "NULL model");
+    ARC_CHECK_ARG(kind == ARC_MLP_ACT_GELU || kind == ARC_MLP_ACT_RELU, "unknown activation");
+    m->activation = kind;
+    return ARC_OK;
+}
+
+int32_t arc_mlp_get_activation(const arc_mlp* m) { return m ? m->activation : -1; }
 
 arc_status arc_mlp_train_step(arc_mlp* m, const void* features_bf16, const float* labels, const float* weights,
                               int64_t rows, float weight_sum, float lr, float* device_loss_accum) {

@@ -47,19 +47,22 @@ PREACCEPT_BAND = 64.0
 
 
 class Model:
-    """An arc_mlp handle with its parameters, its loss (L.ARC_MLP_LOSS_*) and the selection
-    threshold recommended for it (probability for a classifier, relative error for a regressor)."""
+    """An arc_mlp handle with its parameters, its loss (L.ARC_MLP_LOSS_*), its hidden activation
+    (L.ARC_MLP_ACT_*) and the selection threshold recommended for it (probability for a classifier,
+    relative error for a regressor)."""
 
     def __init__(self, ctx: api.Context, params: np.ndarray | None = None, seed: int = 1,
                  loss: int = L.ARC_MLP_LOSS_BCE, threshold: float | None = None, band: float = PREACCEPT_BAND,
-                 eps: float = PREACCEPT_EPS):
+                 eps: float = PREACCEPT_EPS, act: int = L.ARC_MLP_ACT_GELU):
         self.ctx = ctx
         h = C.c_void_p()
         L.check(ctx.lib.arc_mlp_create(ctx.handle, seed, C.byref(h)), "arc_mlp_create")
         self.handle = h
         ctx._children.add(self)
         L.check(ctx.lib.arc_mlp_set_loss(h, int(loss)), "arc_mlp_set_loss")
+        L.check(ctx.lib.arc_mlp_set_activation(h, int(act)), "arc_mlp_set_activation")
         self.loss = int(loss)
+        self.act = int(act)
         self.threshold = threshold if threshold is not None else (0.5 if loss == L.ARC_MLP_LOSS_BCE else 1e-4)
         self.band = float(band)  # the analytic refine band the network was trained within
         self.eps = float(eps)    # the analytic pre-acceptance bound it was trained with
@@ -68,14 +71,15 @@ class Model:
 
     def save(self, path: str) -> None:
         np.savez(path, params=self.params(), loss=np.int32(self.loss), threshold=np.float32(self.threshold),
-                 band=np.float32(self.band), eps=np.float32(self.eps))
+                 band=np.float32(self.band), eps=np.float32(self.eps), act=np.int32(self.act))
 
     @classmethod
     def load(cls, ctx: api.Context, path: str) -> "Model":
         z = np.load(path)
         return cls(ctx, z["params"], loss=int(z["loss"]), threshold=float(z["threshold"]),
                    band=float(z["band"]) if "band" in z else PREACCEPT_BAND,
-                   eps=float(z["eps"]) if "eps" in z else PREACCEPT_EPS)
+                   eps=float(z["eps"]) if "eps" in z else PREACCEPT_EPS,
+                   act=int(z["act"]) if "act" in z else L.ARC_MLP_ACT_GELU)
 
     def set_params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, np.float32)
@@ -162,12 +166,13 @@ def scene_samples(ctx: api.Context, seed: int, capacity: int, width=TRAIN_W, hei
 
 
 def train(ctx: api.Context, feats, labels, epochs: float = 3.0, batch: int = 8192, lr: float = 2e-3,
-          pos_weight: float = 2.0, seed: int = 1, log=print, loss: int = L.ARC_MLP_LOSS_BCE) -> Model:
+          pos_weight: float = 2.0, seed: int = 1, log=print, loss: int = L.ARC_MLP_LOSS_BCE,
+          act: int = L.ARC_MLP_ACT_GELU) -> Model:
     """Adam with a cosine learning rate on the weighted BCE of 0/1 labels (refine samples weighted
     pos_weight), or on the squared error of real-valued labels."""
     import torch
 
-    model = Model(ctx, seed=seed, loss=loss)
+    model = Model(ctx, seed=seed, loss=loss, act=act)
     n = feats.shape[0]
     steps = max(1, int(epochs * n / batch))
     g = torch.Generator(device="cuda").manual_seed(seed)
@@ -384,7 +389,7 @@ def calibrate(ctx: api.Context, model_paths, seeds=VALIDATION_SEEDS, target=CALI
         thr = choose(THRESHOLDS, res, target, larger_is_faster=True)
         worst = [max(x["rel_rmse"] for x in r) for r in res]
         mean_ms = [float(np.mean([x["ms"] for x in r])) for r in res]
-        cand = {"model": os.path.basename(path), "band": m.band, "eps": m.eps, "threshold": thr,
+        cand = {"model": os.path.basename(path), "band": m.band, "eps": m.eps, "act": m.act, "threshold": thr,
                 "worst_rel_rmse": worst,
                 "mean_ms": mean_ms, "thresholds": list(THRESHOLDS)}
         if thr is not None:
@@ -413,6 +418,7 @@ def main(argv=None):
     tr.add_argument("--band", type=float, default=PREACCEPT_BAND)
     tr.add_argument("--eps", type=float, default=PREACCEPT_EPS, help="analytic pre-acceptance bound")
     tr.add_argument("--threshold", type=float, default=None, help="selection threshold stored with the model")
+    tr.add_argument("--act", choices=["gelu", "relu"], default="gelu", help="hidden-layer activation")
     tr.add_argument("--out", default=DEFAULT_MODEL)
     ca = sub.add_parser("calibrate", help="choose the operating point on the validation scenes")
     ca.add_argument("models", nargs="+", help="candidate model archives (band and delta differ)")
@@ -465,7 +471,8 @@ def main(argv=None):
     nv = max(1, n // 50)
     val, trn = perm[:nv], perm[nv:]
     loss = L.ARC_MLP_LOSS_SQUARED if regress else L.ARC_MLP_LOSS_BCE
-    model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs, loss=loss)
+    act = L.ARC_MLP_ACT_RELU if a.act == "relu" else L.ARC_MLP_ACT_GELU
+    model = train(ctx, feats[trn].contiguous(), labels[trn].contiguous(), epochs=a.epochs, loss=loss, act=act)
     model.band = a.band
     model.eps = a.eps
     # the shipped classifier refines at P(refine) >= 0.05: within 1% RMSE on the held-out scene

@@ -167,6 +167,39 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def cgroup_cpu() -> dict:
+    """This process's cgroup CPU bandwidth limit (quota / period in cores, None = unlimited) and the
+    throttling counters so far (cgroup v2 cpu.max / cpu.stat, else v1 cpu.cfs_* / cpu.stat)."""
+    out = {"quota_cores": None, "throttled_s": None, "nr_throttled": None}
+
+    def read(path):
+        try:
+            with open(path) as f:
+                return f.read().split()
+        except OSError:
+            return None
+
+    v2 = read("/sys/fs/cgroup/cpu.max")
+    if v2 and len(v2) == 2:
+        if v2[0] != "max":
+            out["quota_cores"] = int(v2[0]) / max(1, int(v2[1]))
+        st = read("/sys/fs/cgroup/cpu.stat") or []
+        kv = dict(zip(st[0::2], st[1::2]))
+        if "throttled_usec" in kv:
+            out["throttled_s"] = int(kv["throttled_usec"]) * 1e-6
+            out["nr_throttled"] = int(kv.get("nr_throttled", 0))
+        return out
+    q, per = read("/sys/fs/cgroup/cpu/cpu.cfs_quota_us"), read("/sys/fs/cgroup/cpu/cpu.cfs_period_us")
+    if q and per and int(q[0]) > 0:
+        out["quota_cores"] = int(q[0]) / max(1, int(per[0]))
+    st = read("/sys/fs/cgroup/cpu/cpu.stat") or []
+    kv = dict(zip(st[0::2], st[1::2]))
+    if "throttled_time" in kv:
+        out["throttled_s"] = int(kv["throttled_time"]) * 1e-9
+        out["nr_throttled"] = int(kv.get("nr_throttled", 0))
+    return out
+
+
 def _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s: float, threads: int):
     """Runs the scalar FP32 CPU gather over chunks of the pixel list `order` until target_s seconds
     of gather time are spent (or the list is done) -> (pixels gathered, seconds).  Every chunk is a
@@ -197,7 +230,9 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
     prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
     valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
     order = np.random.default_rng(7).permutation(valid)
+    cg0 = cgroup_cpu()
     k, dt, cpu = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s, threads)
+    cg1 = cgroup_cpu()
     # every pixel costs the same (all AVPLs); background pixels cost nothing, so extrapolate over
     # the valid pixels
     ms_frame = dt * 1e3 * len(valid) / max(k, 1)
@@ -218,7 +253,11 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
                      f"one pixel per work item), {dt:.1f} s, extrapolated to {len(valid)} surface pixels",
            # the host is shared with other jobs: the cores the gather actually got (process CPU time
            # over wall time) and the load average when it ran
-           "cpu_seconds_per_second": cpu / max(dt, 1e-9), "loadavg_1min": os.getloadavg()[0]}
+           "cpu_seconds_per_second": cpu / max(dt, 1e-9), "loadavg_1min": os.getloadavg()[0],
+           # a CPU bandwidth limit on the process's cgroup, and how long it held the gather back
+           "cgroup_quota_cores": cg1["quota_cores"],
+           "cgroup_throttled_s": (cg1["throttled_s"] - cg0["throttled_s"]) if cg0["throttled_s"] is not None else None,
+           "cgroup_nr_throttled": (cg1["nr_throttled"] - cg0["nr_throttled"]) if cg0["nr_throttled"] is not None else None}
     if single is not None:
         out["single_thread"] = single
     if ref64 is not None:
@@ -525,16 +564,18 @@ def run_reference(args):
     cam = (desc.camera_position.x, desc.camera_position.y, desc.camera_position.z)
     threads = host_threads()
     per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
-    vals, cores = [], []
+    vals, cores, thr = [], [], []
     for i in range(args.warmup + args.steps):
         b = cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, per, threads)
         if i >= args.warmup:
             vals.append(b["value"])
             cores.append(b["cpu_seconds_per_second"])
+            thr.append(b["cgroup_throttled_s"])
     v = float(np.median(vals))
     b["value"] = v
     b["per_step_values"] = [round(x, 1) for x in vals]
     b["per_step_cpu_seconds_per_second"] = [round(x, 2) for x in cores]
+    b["per_step_cgroup_throttled_s"] = [None if x is None else round(x, 2) for x in thr]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -395,8 +395,9 @@ arc_status arc_last_cut(arc_context* ctx, ArcCutLists* out);
 /* Cut-refinement MLP (no counterpart in the reference)                                      */
 /* ---------------------------------------------------------------------------------------- */
 
-/* 16 -> 64 -> 64 -> 64 -> 1 multilayer perceptron with GELU activations: BF16 weights and
- * activations on the tensor cores (tcgen05), FP32 accumulation, FP32 master parameters
+/* 16 -> 64 -> 64 -> 64 -> 1 multilayer perceptron (GELU or ReLU activations, a property of the
+ * model): BF16 weights and activations on the tensor cores (tcgen05), FP32 accumulation, FP32
+ * master parameters
  * (layout: W1[64][16], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4).  Features
  * are BF16 rows of 16 values (16-byte aligned).  What the output means follows the model's loss:
  * ARC_MLP_LOSS_BCE (default): the logit of "refine this node" (labels 0 / 1);
@@ -421,6 +422,14 @@ arc_status arc_mlp_gradients(arc_mlp* mlp, const void* features_bf16, const floa
 /* Loss used by arc_mlp_gradients / arc_mlp_train_step, and the meaning of the output (above). */
 arc_status arc_mlp_set_loss(arc_mlp* mlp, int32_t kind);
 int32_t arc_mlp_get_loss(const arc_mlp* mlp);
+/* Hidden-layer activation of the model (default GELU); applies to forward, gradients, training
+ * and the learned cut's selection alike. */
+typedef enum arc_mlp_activation {
+    ARC_MLP_ACT_GELU = 0, /* x sigma(1.702 x) = x/2 (1 + tanh(0.851 x)) (sigmoid form of GELU) */
+    ARC_MLP_ACT_RELU = 1  /* max(x, 0) */
+} arc_mlp_activation;
+arc_status arc_mlp_set_activation(arc_mlp* mlp, int32_t kind);
+int32_t arc_mlp_get_activation(const arc_mlp* mlp);
 /* One Adam step (beta 0.9 / 0.999) on the batch's gradient; device_loss_accum (optional, device
  * float) accumulates the batch loss.  Enqueued only. */
 arc_status arc_mlp_train_step(arc_mlp* mlp, const void* features_bf16, const float* labels, const float* weights,

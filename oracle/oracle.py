@@ -367,10 +367,11 @@ def training_samples(pos4, nrm4, tree, diffuse, eps_bound, dist_clamp, ar_kind, 
 
 
 def learned_cut(pos4, nrm4, tree, diffuse, params, eps_bound, ar_uncertain, band, thr_logit, dist_clamp, ar_kind,
-                cone_half_angle_deg, disk_radius=0.0, threads=0):
+                cone_half_angle_deg, disk_radius=0.0, threads=0, act="gelu"):
     """The learned cut selection, level by level: leaves and nodes whose bound is within tau are
-    accepted, nodes above band * tau refined, the rest scored by the network (BF16 rounding points
-    of the tensor-core kernels, FP64 otherwise) and refined iff the logit reaches thr_logit.
+    accepted, nodes above band * tau refined, the rest scored by the network (hidden activation
+    `act`; BF16 rounding points of the tensor-core kernels, FP64 otherwise) and refined iff the
+    logit reaches thr_logit.
     -> (sorted node array per tile, scored (tile, node, logit) rows)."""
     from . import mlp_oracle
 
@@ -399,7 +400,7 @@ def learned_cut(pos4, nrm4, tree, diffuse, params, eps_bound, ar_uncertain, band
         refine = (M > band32 * tau) & ~accept
         score = ~accept & ~refine
         if score.any():
-            y = mlp_oracle.forward_bf16(params, F[score])
+            y = mlp_oracle.forward_bf16(params, F[score], act)
             refine[np.nonzero(score)[0][y >= thr_logit]] = True
             scored.append(np.stack([it[score], inn[score], y], 1))
         done = ~refine

@@ -124,7 +124,7 @@ def test_learned_selection_matches_oracle(ctx, scene_):
     assert ctx.synchronize() == 0
     gcuts = api.last_cut(ctx)
     ocuts, scored = O.learned_cut(d["pos"], d["nrm"], tree, d["dif"], params, model.eps, K, model.band, thr, CLAMP,
-                                  2, CONE)
+                                  2, CONE, act=model.act)
     assert len(scored) > 1000
     differ = [t for t in range(len(gcuts)) if not np.array_equal(gcuts[t], ocuts[t])]
     close = {int(t) for t, _, y in scored if abs(y - thr) < 0.1}

@@ -18,13 +18,22 @@ def _bf16(t):
     return t.to(torch.bfloat16).to(torch.float32)
 
 
-def _torch_forward(p, x):
-    """FP32 reference of the kernels' inference: the activation's constants folded into the
+ACTS = {"gelu": L.ARC_MLP_ACT_GELU, "relu": L.ARC_MLP_ACT_RELU}
+
+
+def _torch_forward(p, x, act="gelu"):
+    """FP32 reference of the kernels' inference.  GELU: the activation's constants folded into the
     parameters as the library's weight image holds them (s W1, W2 / 2, W3 / 2 in BF16, s b in FP32,
-    w4 / (2 s)), the folded activation z + z tanh(z), and BF16 inputs and hidden activations."""
+    w4 / (2 s)), the folded activation z + z tanh(z).  ReLU: the parameters as stored, W in BF16.
+    Both: BF16 inputs and hidden activations."""
     import torch
 
     P = {k: torch.tensor(v, dtype=torch.float32, device="cuda") for k, v in M.unpack(p).items()}
+    if act == "relu":
+        h = _bf16(x)
+        h1 = _bf16(torch.relu(h @ _bf16(P["W1"]).T + P["b1"]))
+        h2 = _bf16(torch.relu(h1 @ _bf16(P["W2"]).T + P["b2"]))
+        return torch.relu(h2 @ _bf16(P["W3"]).T + P["b3"]) @ P["w4"] + P["b4"][0]
     s = torch.tensor(0.851, dtype=torch.float32)
     g = lambda z: z + z * torch.tanh(z)  # noqa: E731
     h = _bf16(x)
@@ -51,26 +60,33 @@ def _params(ctx, h):
     return p
 
 
+@pytest.mark.parametrize("act", ["gelu", "relu"])
 @pytest.mark.parametrize("rows", [1, 127, 128, 1000, 70000])
-def test_forward_matches_torch_and_oracle(ctx, mlp, rows):
+def test_forward_matches_torch_and_oracle(ctx, mlp, rows, act):
     import torch
 
+    L.check(ctx.lib.arc_mlp_set_activation(mlp, ACTS[act]), "set_activation")
+    assert ctx.lib.arc_mlp_get_activation(mlp) == ACTS[act]
     g = torch.Generator(device="cuda").manual_seed(rows)
     x = torch.randn(rows, 16, device="cuda", generator=g).to(torch.bfloat16).contiguous()
     out = torch.empty(rows, device="cuda")
     L.check(ctx.lib.arc_mlp_forward(mlp, C.c_void_p(x.data_ptr()), rows, C.c_void_p(out.data_ptr())), "forward")
     assert ctx.synchronize() == 0
+    L.check(ctx.lib.arc_mlp_set_activation(mlp, L.ARC_MLP_ACT_GELU), "set_activation")
     p = _params(ctx, mlp)
-    ref = _torch_forward(p, x.float())
+    ref = _torch_forward(p, x.float(), act)
     err = (out - ref).abs().max().item()
     assert err <= 2e-3 * max(1.0, ref.abs().max().item()), err
     if rows <= 1000:
-        y64, _ = M.forward(p.astype(np.float64), x.float().cpu().numpy())
+        y64, _ = M.forward(p.astype(np.float64), x.float().cpu().numpy(), act)
         assert np.max(np.abs(out.cpu().numpy() - y64)) <= 3e-2 * max(1.0, np.abs(y64).max())
+        yb = M.forward_bf16(p, x.float().cpu().numpy(), act)
+        assert np.max(np.abs(out.cpu().numpy() - yb)) <= 2e-3 * max(1.0, np.abs(yb).max())
 
 
+@pytest.mark.parametrize("act", ["gelu", "relu"])
 @pytest.mark.parametrize("loss", ["bce", "squared"])
-def test_gradients_match_torch_and_oracle(ctx, mlp, loss):
+def test_gradients_match_torch_and_oracle(ctx, mlp, loss, act):
     import torch
 
     rows = 1000
@@ -83,6 +99,7 @@ def test_gradients_match_torch_and_oracle(ctx, mlp, loss):
     wts = torch.rand(rows, device="cuda", generator=g) + 0.5
     kind = L.ARC_MLP_LOSS_BCE if loss == "bce" else L.ARC_MLP_LOSS_SQUARED
     L.check(ctx.lib.arc_mlp_set_loss(mlp, kind), "set_loss")
+    L.check(ctx.lib.arc_mlp_set_activation(mlp, ACTS[act]), "set_activation")
     assert ctx.lib.arc_mlp_get_loss(mlp) == kind
     grads = np.zeros(M.NUM_PARAMS, np.float32)
     loss_v = C.c_float()
@@ -91,19 +108,23 @@ def test_gradients_match_torch_and_oracle(ctx, mlp, loss):
                                       grads.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss_v)), "gradients")
     p = _params(ctx, mlp)
     L.check(ctx.lib.arc_mlp_set_loss(mlp, L.ARC_MLP_LOSS_BCE), "set_loss")
+    L.check(ctx.lib.arc_mlp_set_activation(mlp, L.ARC_MLP_ACT_GELU), "set_activation")
     l64, g64 = M.loss_and_grad(p.astype(np.float64), x.float().cpu().numpy(), lab.cpu().numpy(), wts.cpu().numpy(),
-                               loss=loss)
+                               loss=loss, act=act)
     assert abs(loss_v.value - l64) <= 1e-2 * abs(l64)
     # torch autograd with the kernel's rounding points (straight-through in the backward)
     P = {k: torch.tensor(v, dtype=torch.float32, device="cuda", requires_grad=True) for k, v in M.unpack(p).items()}
-    gelu = lambda z: 0.5 * z * (1 + torch.tanh(np.sqrt(2.0 / np.pi) * (z + 0.044715 * z ** 3)))  # noqa: E731
+    if act == "relu":
+        f = torch.relu
+    else:
+        f = lambda z: 0.5 * z * (1 + torch.tanh(0.851 * z))  # noqa: E731  (x sigma(1.702 x))
     st = lambda t: t + (_bf16(t) - t).detach()  # noqa: E731
     z1 = st(x.float()) @ st(P["W1"]).T + P["b1"]
-    h1 = st(gelu(z1))
+    h1 = st(f(z1))
     z2 = h1 @ st(P["W2"]).T + P["b2"]
-    h2 = st(gelu(z2))
+    h2 = st(f(z2))
     z3 = h2 @ st(P["W3"]).T + P["b3"]
-    y = gelu(z3) @ P["w4"] + P["b4"][0]
+    y = f(z3) @ P["w4"] + P["b4"][0]
     if loss == "bce":
         per = torch.nn.functional.binary_cross_entropy_with_logits(y, lab, reduction="none")
     else:
@@ -118,11 +139,13 @@ def test_gradients_match_torch_and_oracle(ctx, mlp, loss):
         assert cos > 0.998
 
 
-def test_training_learns_a_separable_rule(ctx):
+@pytest.mark.parametrize("act", ["gelu", "relu"])
+def test_training_learns_a_separable_rule(ctx, act):
     import torch
 
     h = C.c_void_p()
     L.check(ctx.lib.arc_mlp_create(ctx.handle, 1, C.byref(h)), "create")
+    L.check(ctx.lib.arc_mlp_set_activation(h, ACTS[act]), "set_activation")
     g = torch.Generator(device="cuda").manual_seed(5)
     n = 65536
     x = torch.randn(n, 16, device="cuda", generator=g)
