@@ -945,6 +945,10 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.in_count = counters + 8 + 4 * kMaxLevels;
     accept_frontier<<<grid, 256, 0, st>>>(la);
     ++kernels;
+    stage_end(ctx, kernels);
+    // the accepted pairs grouped by tile into the cut pool, timed as a stage of its own
+    stage_begin(ctx, "cut_lists");
+    kernels = 0;
     ScatterArgs sa;
     sa.accepted = accepted;
     sa.acc_count = counters + 3;

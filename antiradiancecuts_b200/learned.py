@@ -361,7 +361,7 @@ def choose(values, results, target: float, larger_is_faster: bool = True):
     return max(ok, key=lambda vr: vr[0])[0] if larger_is_faster else min(ok, key=lambda vr: vr[0])[0]
 
 
-THRESHOLDS = (0.01, 0.015, 0.02, 0.025, 0.03, 0.04, 0.05, 0.07, 0.1, 0.15, 0.2)
+THRESHOLDS = (0.01, 0.015, 0.02, 0.025, 0.03, 0.04, 0.05, 0.06, 0.07, 0.08, 0.09, 0.1, 0.12, 0.15, 0.2, 0.25, 0.3)
 ANALYTIC_BOUNDS = (0.0015, 0.002, 0.0025, 0.003, 0.004)
 CALIBRATION_TARGET = 0.0099  # the worst validation scene's relative RMSE stays under 1%
 

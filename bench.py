@@ -40,6 +40,10 @@ UNIT = "ms/frame"
 FLOP_PER_PAIR = {0: 30, 1: 54, 2: 43}
 # MLP forward per scored row: 2 * (16*64 + 64*64 + 64*64 + 64) multiply-adds
 FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64)
+# DRAM bytes (read + write) of all learned_level launches of a frame per scored row: one ncu capture
+# of the 96 level launches of a 640x360 / 262,144-AVPL frame
+# (profiles/learned_level_dram_640x360_262k.md), scaled to the frame by its scored rows
+LEARNED_LEVEL_DRAM_BYTES_PER_ROW = 33.16
 
 
 CALIBRATION = os.path.join(ROOT, "antiradiancecuts_b200", "models", "cutnet_calibration.json")
@@ -732,7 +736,11 @@ def main():
         bf16 = peaks.get("bf16_tflops", 1590.0)
         ach = rows_per_frame * FLOP_PER_ROW / (per_stage[dom] * 1e-3) / 1e12
         roof = {"kernel": "learned_level", "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-                "frac": ach / bf16, "traffic": None, "rows_per_frame": rows_per_frame,
+                "frac": ach / bf16, "traffic": LEARNED_LEVEL_DRAM_BYTES_PER_ROW * rows_per_frame,
+                "traffic_scope": "bytes of the frame's 96 level launches (the unit `achieved` is taken over): "
+                                 f"{LEARNED_LEVEL_DRAM_BYTES_PER_ROW} B per scored row from a 640x360 capture "
+                                 "x rows_per_frame",
+                "rows_per_frame": rows_per_frame,
                 "flop_per_row": FLOP_PER_ROW, "ms": per_stage[dom],
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if "bf16_tflops" in peaks else "fallback"}
     elif dom.startswith("lbvh"):
