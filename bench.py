@@ -204,6 +204,19 @@ def cgroup_cpu() -> dict:
     return out
 
 
+def host_cpu_times():
+    """(busy, steal, total) jiffies over all CPUs of the host (/proc/stat), or None."""
+    try:
+        with open("/proc/stat") as f:
+            v = [int(x) for x in f.readline().split()[1:]]
+    except (OSError, ValueError):
+        return None
+    idle = v[3] + (v[4] if len(v) > 4 else 0)
+    steal = v[7] if len(v) > 7 else 0
+    total = sum(v[:8])
+    return total - idle - steal, steal, total
+
+
 def _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s: float, threads: int):
     """Runs the scalar FP32 CPU gather over chunks of the pixel list `order` until target_s seconds
     of gather time are spent (or the list is done) -> (pixels gathered, seconds).  Every chunk is a
@@ -234,9 +247,16 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
     prm = O.params(wl.ar_kind, wl.cone_half_angle_deg, wl.dist_clamp)
     valid = np.nonzero(nrm.reshape(-1, 4)[:, 3] > 0)[0]
     order = np.random.default_rng(7).permutation(valid)
-    cg0 = cgroup_cpu()
+    import resource
+
+    cg0, hs0, ru0 = cgroup_cpu(), host_cpu_times(), resource.getrusage(resource.RUSAGE_SELF)
     k, dt, cpu = _cpu_gather_sample(O, pos, nrm, order, avpls, dif, spe, ex, cam, prm, target_s, threads)
-    cg1 = cgroup_cpu()
+    cg1, hs1, ru1 = cgroup_cpu(), host_cpu_times(), resource.getrusage(resource.RUSAGE_SELF)
+    host = None
+    if hs0 and hs1 and hs1[2] > hs0[2]:
+        tot = hs1[2] - hs0[2]
+        # busy and steal shares of every CPU of the host, this process's threads included
+        host = {"busy": (hs1[0] - hs0[0]) / tot, "steal": (hs1[1] - hs0[1]) / tot, "cpus": os.cpu_count()}
     # every pixel costs the same (all AVPLs); background pixels cost nothing, so extrapolate over
     # the valid pixels
     ms_frame = dt * 1e3 * len(valid) / max(k, 1)
@@ -261,7 +281,11 @@ def cpu_baseline(wl, desc, avpls, pos, nrm, dif, spe, ex, cam, target_s: float, 
            # a CPU bandwidth limit on the process's cgroup, and how long it held the gather back
            "cgroup_quota_cores": cg1["quota_cores"],
            "cgroup_throttled_s": (cg1["throttled_s"] - cg0["throttled_s"]) if cg0["throttled_s"] is not None else None,
-           "cgroup_nr_throttled": (cg1["nr_throttled"] - cg0["nr_throttled"]) if cg0["nr_throttled"] is not None else None}
+           "cgroup_nr_throttled": (cg1["nr_throttled"] - cg0["nr_throttled"]) if cg0["nr_throttled"] is not None else None,
+           # the host's CPUs during the sample, and how often the kernel took a core from a gather
+           # thread (involuntary) or a thread gave it up (voluntary)
+           "host_cpu": host,
+           "context_switches": {"involuntary": ru1.ru_nivcsw - ru0.ru_nivcsw, "voluntary": ru1.ru_nvcsw - ru0.ru_nvcsw}}
     if single is not None:
         out["single_thread"] = single
     if ref64 is not None:

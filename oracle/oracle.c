@@ -172,10 +172,14 @@ OR_EXPORT void oracle_gather_fp64(const float* gb_pos, const float* gb_nrm, int3
                                   const float* diffuse, const float* specular, const float* exponent,
                                   int32_t num_materials, const float* cam, const oracle_params* P, double* out_rad,
                                   double* out_ar, double* out_res, int32_t num_threads) {
-    oracle_materials M = {diffuse, specular, exponent, num_materials};
-    d3 c = d3load(cam);
     (void)width;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads > 0 ? num_threads : 1)
+    /* thread-private copies of the call's constants, as in oracle_gather_fp32 */
+#pragma omp parallel num_threads(num_threads > 0 ? num_threads : 1)
+    {
+    const oracle_params Pl = *P;
+    const oracle_materials M = {diffuse, specular, exponent, num_materials};
+    const d3 c = d3load(cam);
+#pragma omp for schedule(dynamic, 1)
     for (int32_t k = 0; k < num_pixels; ++k) {
         const int64_t px = pixels[k];
         const float* gp = gb_pos + 4 * px;
@@ -186,16 +190,17 @@ OR_EXPORT void oracle_gather_fp64(const float* gb_pos, const float* gb_nrm, int3
             d3 pos = d3load(gp), n = d3load(gn);
             for (int32_t i = 0; i < num_avpls; ++i) {
                 d3 pa = d3load(a_pos + 3 * i), na = d3load(a_nrm + 3 * i), wa = d3load(a_w + 3 * i);
-                rad = d3add(rad, radiance_term(pos, n, mat, pa, na, wa, d3load(a_L + 3 * i), a_mat[i], c, &M, P));
-                if (P->ar_kind == 1)
-                    ar = d3add(ar, antiradiance_disk(pos, n, mat, pa, na, wa, d3load(a_A + 3 * i), c, &M, P));
-                else if (P->ar_kind == 2)
-                    ar = d3add(ar, antiradiance_cone(pos, n, mat, pa, wa, d3load(a_A + 3 * i), c, &M, P));
+                rad = d3add(rad, radiance_term(pos, n, mat, pa, na, wa, d3load(a_L + 3 * i), a_mat[i], c, &M, &Pl));
+                if (Pl.ar_kind == 1)
+                    ar = d3add(ar, antiradiance_disk(pos, n, mat, pa, na, wa, d3load(a_A + 3 * i), c, &M, &Pl));
+                else if (Pl.ar_kind == 2)
+                    ar = d3add(ar, antiradiance_cone(pos, n, mat, pa, wa, d3load(a_A + 3 * i), c, &M, &Pl));
             }
         }
         out_rad[3 * k + 0] = rad.x; out_rad[3 * k + 1] = rad.y; out_rad[3 * k + 2] = rad.z;
         out_ar[3 * k + 0] = ar.x; out_ar[3 * k + 1] = ar.y; out_ar[3 * k + 2] = ar.z;
         out_res[3 * k + 0] = rad.x - ar.x; out_res[3 * k + 1] = rad.y - ar.y; out_res[3 * k + 2] = rad.z - ar.z;
+    }
     }
 }
 
@@ -337,13 +342,19 @@ OR_EXPORT void oracle_gather_fp32(const float* gb_pos, const float* gb_nrm, int3
                                   const float* diffuse, const float* specular, const float* exponent,
                                   int32_t num_materials, const float* cam, const oracle_params* P, float* out_res,
                                   int32_t num_threads) {
-    oracle_materials M = {diffuse, specular, exponent, num_materials};
+    (void)width;
+    /* Every thread keeps its own copy of the call's constants: read through the calling thread's
+     * stack frame, they share cache lines with what that thread writes while it gathers, and the
+     * team then runs little faster than one thread. */
+#pragma omp parallel num_threads(num_threads > 0 ? num_threads : 1)
+    {
+    const oracle_params Pl = *P;
+    const oracle_materials M = {diffuse, specular, exponent, num_materials};
     const f3 c = f3load(cam);
     const float eps = 0.001f;
-    const float cos_half = cosf(P->cone_half_angle);
-    const float clamp2 = P->dist_clamp * P->dist_clamp;
-    (void)width;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads > 0 ? num_threads : 1)
+    const float cos_half = cosf(Pl.cone_half_angle);
+    const float clamp2 = Pl.dist_clamp * Pl.dist_clamp;
+#pragma omp for schedule(dynamic, 1)
     for (int32_t k = 0; k < num_pixels; ++k) {
         const int64_t px = pixels[k];
         const int mat = (int)gb_nrm[4 * px + 3];
@@ -365,24 +376,24 @@ OR_EXPORT void oracle_gather_fp32(const float* gb_pos, const float* gb_nrm, int3
                 const float c2 = clampf(-f3dot(na, w), 0.0f, 1.0f);
                 const float l2c = (clamp2 > 0.0f && l2 < clamp2) ? clamp2 : l2;
                 float g = c1 * c2 / l2c;
-                if (P->geo_limit_radiance > 0.0f) g = clampf(g, 0.0f, P->geo_limit_radiance);
+                if (Pl.geo_limit_radiance > 0.0f) g = clampf(g, 0.0f, Pl.geo_limit_radiance);
                 rad = f3add(rad, f3s(g, f3mul(f3mul(f3load(a_L + 3 * i), brdf_light), brdf)));
                 /* antiradiance */
-                if (P->ar_kind == 2) {
+                if (Pl.ar_kind == 2) {
                     const float cw = -f3dot(w, wa);
                     if (cw > eps && c1 > eps && cw > cos_half) {
                         float ga = f3dot(n, w) / l2c;
-                        if (P->geo_limit_antiradiance > 0.0f) ga = clampf(ga, 0.0f, P->geo_limit_antiradiance);
+                        if (Pl.geo_limit_antiradiance > 0.0f) ga = clampf(ga, 0.0f, Pl.geo_limit_antiradiance);
                         ar = f3add(ar, f3s(ga, f3mul(f3load(a_A + 3 * i), brdf)));
                     }
-                } else if (P->ar_kind == 1) {
+                } else if (Pl.ar_kind == 1) {
                     const float denom = f3dot(wa, n);
                     if (denom != 0.0f) {
                         const float t = f3dot(f3s(-1.0f, v), n) / denom;
                         const f3 wn = f3norm(wa);
                         const f3 h = f3add(pa, f3s(t, wn));
                         const f3 hp = f3sub(h, pos);
-                        const float r = P->disk_radius;
+                        const float r = Pl.disk_radius;
                         if (t > 0.0f && sqrtf(f3dot(hp, hp)) < r && f3dot(f3norm(f3sub(h, pa)), wa) > 0.0f &&
                             denom < 0.0f && -f3dot(w, na) < 0.0f)
                             ar = f3add(ar, f3s(1.0f / (3.14159265f * r * r), f3mul(f3load(a_A + 3 * i), brdf)));
@@ -393,6 +404,7 @@ OR_EXPORT void oracle_gather_fp32(const float* gb_pos, const float* gb_nrm, int3
         out_res[3 * k + 0] = rad.x - ar.x;
         out_res[3 * k + 1] = rad.y - ar.y;
         out_res[3 * k + 2] = rad.z - ar.z;
+    }
     }
 }
 
