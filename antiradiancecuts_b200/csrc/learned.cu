@@ -575,19 +575,42 @@ __global__ void scatter_nodes(ScatterArgs s) {
 // reserves each tile's run with one global atomic per tile present, then reads the segment again
 // and hands out the slots of each run.  The accepted list comes grouped by node, so a warp's 32
 // pairs mostly name 32 different tiles: reserving per pair (scatter_nodes) costs one global atomic
-// each, and binning a large segment cuts that to one per (segment, tile).
+// each, and binning a large segment cuts that to one per (segment, tile).  Each thread reads
+// kBinPer consecutive pairs with 16-byte loads before it uses any of them, so that enough bytes
+// are in flight to cover the memory latency with one 1024-thread CTA per SM.
 constexpr int kBinSegment = 1 << 19;
+constexpr int kBinPer = 8;
+
+// pairs b .. b + kBinPer - 1 (tile -1 past end); b is even, so the 16-byte loads are aligned
+__device__ __forceinline__ void load_pairs(const int2* acc, int64_t b, int64_t end, int2* p) {
+    if (b + kBinPer <= end) {
+        const int4* q = reinterpret_cast<const int4*>(acc + b);
+#pragma unroll
+        for (int j = 0; j < kBinPer / 2; ++j) {
+            const int4 v = __ldg(q + j);
+            p[2 * j] = make_int2(v.x, v.y);
+            p[2 * j + 1] = make_int2(v.z, v.w);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kBinPer; ++j) p[j] = b + j < end ? acc[b + j] : make_int2(-1, 0);
+    }
+}
 
 __global__ void __launch_bounds__(1024) scatter_nodes_binned(ScatterArgs s, int tiles) {
     extern __shared__ int bins[];  // [tiles]: counts, then each tile's next slot
     const int count = (int)min((unsigned)*s.acc_count, (unsigned)s.acc_capacity);
+    const int64_t stride = (int64_t)blockDim.x * kBinPer;
     for (int64_t seg = (int64_t)blockIdx.x * kBinSegment; seg < count; seg += (int64_t)gridDim.x * kBinSegment) {
-        const int end = (int)(seg + kBinSegment < (int64_t)count ? seg + kBinSegment : (int64_t)count);
+        const int64_t end = seg + kBinSegment < (int64_t)count ? seg + kBinSegment : (int64_t)count;
         for (int t = threadIdx.x; t < tiles; t += blockDim.x) bins[t] = 0;
         __syncthreads();
-        for (int e = (int)seg + threadIdx.x; e < end; e += blockDim.x) {
-            const int tile = s.accepted[e].x;
-            if ((unsigned)tile < (unsigned)tiles) atomicAdd(&bins[tile], 1);
+        for (int64_t b = seg + (int64_t)threadIdx.x * kBinPer; b < end; b += stride) {
+            int2 p[kBinPer];
+            load_pairs(s.accepted, b, end, p);
+#pragma unroll
+            for (int j = 0; j < kBinPer; ++j)
+                if ((unsigned)p[j].x < (unsigned)tiles) atomicAdd(&bins[p[j].x], 1);
         }
         __syncthreads();
         for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
@@ -595,16 +618,25 @@ __global__ void __launch_bounds__(1024) scatter_nodes_binned(ScatterArgs s, int 
             if (c) bins[t] = atomicAdd(&s.fill[t], c);
         }
         __syncthreads();
-        for (int e = (int)seg + threadIdx.x; e < end; e += blockDim.x) {
-            const int2 p = s.accepted[e];
-            if ((unsigned)p.x >= (unsigned)tiles) {
-                set_error(s.err, ARC_DEVERR_BAD_NODE);
-                continue;
+        for (int64_t b = seg + (int64_t)threadIdx.x * kBinPer; b < end; b += stride) {
+            int2 p[kBinPer];
+            load_pairs(s.accepted, b, end, p);
+            int pos[kBinPer];
+#pragma unroll
+            for (int j = 0; j < kBinPer; ++j) {
+                pos[j] = -1;
+                if ((unsigned)p[j].x < (unsigned)tiles)
+                    pos[j] = atomicAdd(&bins[p[j].x], 1);
+                else if (b + j < end)
+                    set_error(s.err, ARC_DEVERR_BAD_NODE);
             }
-            const int pos = atomicAdd(&bins[p.x], 1);
-            const int id = s.chunk_base[p.x] + pos / kChunk;
-            if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p.x])
-                s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p.y;
+#pragma unroll
+            for (int j = 0; j < kBinPer; ++j) {
+                if (pos[j] < 0) continue;
+                const int id = s.chunk_base[p[j].x] + pos[j] / kChunk;
+                if (pos[j] / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos[j] < s.pool.counts[p[j].x])
+                    s.pool.entries[(size_t)id * kChunk + pos[j] % kChunk] = p[j].y;
+            }
         }
         __syncthreads();  // the bins are zeroed for the next segment only after every thread is done
     }
