@@ -824,13 +824,16 @@ OR_EXPORT void oracle_cut_solid_angle(const float* gb_pos, const float* gb_nrm, 
                                       const float* specular, const float* exponent, int32_t num_materials,
                                       const float* cam, float thresh, float dist_clamp, int32_t stack_cap,
                                       double* out_rad, int32_t* err, int32_t num_threads) {
-    oracle_materials M = {diffuse, specular, exponent, num_materials};
+    /* thread-private copies of the call's constants, as in oracle_gather_fp32 */
+#pragma omp parallel num_threads(num_threads > 0 ? num_threads : 1)
+    {
+    const oracle_materials M = {diffuse, specular, exponent, num_materials};
     oracle_params P;
     memset(&P, 0, sizeof(P));
     P.dist_clamp = dist_clamp;
-    d3 c = d3load(cam);
+    const d3 c = d3load(cam);
     const float two_pi = 2.0f * kPiF;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads > 0 ? num_threads : 1)
+#pragma omp for schedule(dynamic, 1)
     for (int32_t q = 0; q < num_pixels; ++q) {
         const int64_t px = pixels[q];
         const float* gp = gb_pos + 4 * px;
@@ -882,6 +885,7 @@ OR_EXPORT void oracle_cut_solid_angle(const float* gb_pos, const float* gb_nrm, 
         out_rad[3 * q + 1] = rad.y;
         out_rad[3 * q + 2] = rad.z;
         err[q] = error;
+    }
     }
 }
 
