@@ -522,7 +522,8 @@ struct ScatterArgs {
     int acc_capacity;
     const int* tile_counts;
     const int* chunk_base;
-    int* fill;
+    int* fill;              // per-tile slot counters, spread: tile t at fill_index(t, fill_stride)
+    int fill_stride;
     CutPool pool;
     const int* total_chunks;
     uint32_t* err;
@@ -546,99 +547,52 @@ __global__ void scatter_tables(ScatterArgs s, int tiles) {
     s.pool.counts[t] = cnt;
 }
 
-// (blockDim a multiple of 32: every lane of a warp takes the same loop trips)
+// The accepted list is grouped by node, so a warp's 32 pairs name consecutive tiles; their slot
+// counters are spread so that consecutive tiles sit fill_stride ints apart (fill_stride >= 32,
+// one 128-byte line or more), and the warp's reservations go to 32 lines instead of one or two.
+__host__ __device__ __forceinline__ int fill_index(int tile, int stride) { return (tile & 31) * stride + (tile >> 5); }
+
+__host__ __device__ __forceinline__ int fill_stride_of(int tiles) { return ((tiles + 31) / 32 + 31) / 32 * 32; }
+
+// Each thread takes kScatterIlp pairs per trip (a warp reads 32 consecutive pairs for each), and
+// all their loads, then all their slot reservations, are issued before any result is used, so
+// that several global atomics per thread are in flight.  (blockDim a multiple of 32: every lane
+// of a warp takes the same loop trips.)
+constexpr int kScatterIlp = 4;
+
 __global__ void scatter_nodes(ScatterArgs s) {
     // every reserved slot below the capacity was written; the counter may have wrapped past 2^31
     const int count = (int)min((unsigned)*s.acc_count, (unsigned)s.acc_capacity);
     const int lane = threadIdx.x & 31;
-    for (int b = blockIdx.x * blockDim.x; b < count; b += gridDim.x * blockDim.x) {
-        const int e = b + threadIdx.x;
-        const bool valid = e < count;
-        const int2 p = valid ? s.accepted[e] : make_int2(-1 - lane, 0);
+    const int64_t trip = (int64_t)blockDim.x * kScatterIlp;
+    for (int64_t b = (int64_t)blockIdx.x * trip; b < count; b += (int64_t)gridDim.x * trip) {
+        int2 p[kScatterIlp];
+        bool valid[kScatterIlp];
+#pragma unroll
+        for (int u = 0; u < kScatterIlp; ++u) {
+            const int64_t e = b + (int64_t)u * blockDim.x + threadIdx.x;
+            valid[u] = e < count;
+            p[u] = valid[u] ? s.accepted[e] : make_int2(-1 - lane, 0);
+        }
         // lanes with the same tile take consecutive slots with one atomic
-        const unsigned grp = __match_any_sync(0xffffffffu, p.x);
-        const int leader = __ffs(grp) - 1;
-        int base = 0;
-        if (valid && lane == leader) base = atomicAdd(&s.fill[p.x], __popc(grp));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (!valid) continue;
-        const int pos = base + __popc(grp & ((1u << lane) - 1u));
-        const int id = s.chunk_base[p.x] + pos / kChunk;
-        if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p.x])
-            s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p.y;
-    }
-}
-
-// The same scatter with the per-tile slot reservations binned in shared memory, for frames whose
-// tile counters fit there (tiles * 4 bytes of dynamic shared memory).  A CTA takes segments of
-// kBinSegment accepted pairs: it counts the segment's pairs per tile with shared-memory atomics,
-// reserves each tile's run with one global atomic per tile present, then reads the segment again
-// and hands out the slots of each run.  The accepted list comes grouped by node, so a warp's 32
-// pairs mostly name 32 different tiles: reserving per pair (scatter_nodes) costs one global atomic
-// each, and binning a large segment cuts that to one per (segment, tile).  Each thread reads
-// kBinPer consecutive pairs with 16-byte loads before it uses any of them, so that enough bytes
-// are in flight to cover the memory latency with one 1024-thread CTA per SM.
-constexpr int kBinSegment = 1 << 19;
-constexpr int kBinPer = 8;
-
-// pairs b .. b + kBinPer - 1 (tile -1 past end); b is even, so the 16-byte loads are aligned
-__device__ __forceinline__ void load_pairs(const int2* acc, int64_t b, int64_t end, int2* p) {
-    if (b + kBinPer <= end) {
-        const int4* q = reinterpret_cast<const int4*>(acc + b);
+        unsigned grp[kScatterIlp];
+        int base[kScatterIlp];
 #pragma unroll
-        for (int j = 0; j < kBinPer / 2; ++j) {
-            const int4 v = __ldg(q + j);
-            p[2 * j] = make_int2(v.x, v.y);
-            p[2 * j + 1] = make_int2(v.z, v.w);
+        for (int u = 0; u < kScatterIlp; ++u) {
+            grp[u] = __match_any_sync(0xffffffffu, p[u].x);
+            base[u] = 0;
+            if (valid[u] && lane == __ffs(grp[u]) - 1)
+                base[u] = atomicAdd(&s.fill[fill_index(p[u].x, s.fill_stride)], __popc(grp[u]));
         }
-    } else {
 #pragma unroll
-        for (int j = 0; j < kBinPer; ++j) p[j] = b + j < end ? acc[b + j] : make_int2(-1, 0);
-    }
-}
-
-__global__ void __launch_bounds__(1024) scatter_nodes_binned(ScatterArgs s, int tiles) {
-    extern __shared__ int bins[];  // [tiles]: counts, then each tile's next slot
-    const int count = (int)min((unsigned)*s.acc_count, (unsigned)s.acc_capacity);
-    const int64_t stride = (int64_t)blockDim.x * kBinPer;
-    for (int64_t seg = (int64_t)blockIdx.x * kBinSegment; seg < count; seg += (int64_t)gridDim.x * kBinSegment) {
-        const int64_t end = seg + kBinSegment < (int64_t)count ? seg + kBinSegment : (int64_t)count;
-        for (int t = threadIdx.x; t < tiles; t += blockDim.x) bins[t] = 0;
-        __syncthreads();
-        for (int64_t b = seg + (int64_t)threadIdx.x * kBinPer; b < end; b += stride) {
-            int2 p[kBinPer];
-            load_pairs(s.accepted, b, end, p);
-#pragma unroll
-            for (int j = 0; j < kBinPer; ++j)
-                if ((unsigned)p[j].x < (unsigned)tiles) atomicAdd(&bins[p[j].x], 1);
+        for (int u = 0; u < kScatterIlp; ++u) {
+            base[u] = __shfl_sync(0xffffffffu, base[u], __ffs(grp[u]) - 1);
+            if (!valid[u]) continue;
+            const int pos = base[u] + __popc(grp[u] & ((1u << lane) - 1u));
+            const int id = s.chunk_base[p[u].x] + pos / kChunk;
+            if (pos / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos < s.pool.counts[p[u].x])
+                s.pool.entries[(size_t)id * kChunk + pos % kChunk] = p[u].y;
         }
-        __syncthreads();
-        for (int t = threadIdx.x; t < tiles; t += blockDim.x) {
-            const int c = bins[t];
-            if (c) bins[t] = atomicAdd(&s.fill[t], c);
-        }
-        __syncthreads();
-        for (int64_t b = seg + (int64_t)threadIdx.x * kBinPer; b < end; b += stride) {
-            int2 p[kBinPer];
-            load_pairs(s.accepted, b, end, p);
-            int pos[kBinPer];
-#pragma unroll
-            for (int j = 0; j < kBinPer; ++j) {
-                pos[j] = -1;
-                if ((unsigned)p[j].x < (unsigned)tiles)
-                    pos[j] = atomicAdd(&bins[p[j].x], 1);
-                else if (b + j < end)
-                    set_error(s.err, ARC_DEVERR_BAD_NODE);
-            }
-#pragma unroll
-            for (int j = 0; j < kBinPer; ++j) {
-                if (pos[j] < 0) continue;
-                const int id = s.chunk_base[p[j].x] + pos[j] / kChunk;
-                if (pos[j] / kChunk < s.pool.max_chunks && id < s.pool.num_chunks && pos[j] < s.pool.counts[p[j].x])
-                    s.pool.entries[(size_t)id * kChunk + pos[j] % kChunk] = p[j].y;
-            }
-        }
-        __syncthreads();  // the bins are zeroed for the next segment only after every thread is done
     }
 }
 
@@ -905,10 +859,11 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     ARC_TRY(arena_get(ctx, "lc_counters", kSlots, &counters));
     ARC_TRY(arena_get(ctx, "lc_tile_counts", tiles, &tile_counts));
     ARC_TRY(arena_get(ctx, "lc_chunk_base", tiles, &chunk_base));
-    ARC_TRY(arena_get(ctx, "lc_fill", tiles, &fill));
+    const int fill_stride = fill_stride_of(tiles);
+    ARC_TRY(arena_get(ctx, "lc_fill", 32 * fill_stride, &fill));
     ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * kSlots, st));
     ARC_TRY_CUDA(cudaMemsetAsync(tile_counts, 0, sizeof(int) * tiles, st));
-    ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * tiles, st));
+    ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * 32 * (size_t)fill_stride, st));
 
     const float p = cp->mlp_threshold;
     LevelArgs la{};
@@ -988,24 +943,13 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     sa.tile_counts = tile_counts;
     sa.chunk_base = chunk_base;
     sa.fill = fill;
+    sa.fill_stride = fill_stride;
     sa.pool = pool;
     sa.total_chunks = counters + 4;
     sa.err = ctx->d_error;
     tile_chunk_scan<<<1, 1024, 0, st>>>(tile_counts, tiles, chunk_base, counters + 4, pool.max_chunks, ctx->d_error);
     scatter_tables<<<(tiles + 255) / 256, 256, 0, st>>>(sa, tiles);
-    // binned in shared memory when the tile counters fit (1080p: 32,400 tiles, 130 KB)
-    int smem_optin = 0;
-    ARC_TRY_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const size_t bin_bytes = sizeof(int) * (size_t)tiles;
-    if (bin_bytes <= (size_t)smem_optin) {
-        // the device's full opt-in size, never lowered: graphs recorded for other frame sizes keep
-        // their launches valid
-        ARC_TRY_CUDA(cudaFuncSetAttribute(scatter_nodes_binned, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          smem_optin));
-        scatter_nodes_binned<<<ctx->sm_count, 1024, bin_bytes, st>>>(sa, tiles);
-    } else {
-        scatter_nodes<<<grid, 256, 0, st>>>(sa);
-    }
+    scatter_nodes<<<grid, 256, 0, st>>>(sa);
     kernels += 3;
     ARC_TRY_CUDA(cudaMemcpyAsync(pool.next, counters + 4, sizeof(int), cudaMemcpyDeviceToDevice, st));
     stage_end(ctx, kernels);
