@@ -522,8 +522,7 @@ struct ScatterArgs {
     int acc_capacity;
     const int* tile_counts;
     const int* chunk_base;
-    int* fill;              // per-tile slot counters, spread: tile t at fill_index(t, fill_stride)
-    int fill_stride;
+    int* fill;
     CutPool pool;
     const int* total_chunks;
     uint32_t* err;
@@ -546,13 +545,6 @@ __global__ void scatter_tables(ScatterArgs s, int tiles) {
     }
     s.pool.counts[t] = cnt;
 }
-
-// The accepted list is grouped by node, so a warp's 32 pairs name consecutive tiles; their slot
-// counters are spread so that consecutive tiles sit fill_stride ints apart (fill_stride >= 32,
-// one 128-byte line or more), and the warp's reservations go to 32 lines instead of one or two.
-__host__ __device__ __forceinline__ int fill_index(int tile, int stride) { return (tile & 31) * stride + (tile >> 5); }
-
-__host__ __device__ __forceinline__ int fill_stride_of(int tiles) { return ((tiles + 31) / 32 + 31) / 32 * 32; }
 
 // Each thread takes kScatterIlp pairs per trip (a warp reads 32 consecutive pairs for each), and
 // all their loads, then all their slot reservations, are issued before any result is used, so
@@ -581,8 +573,7 @@ __global__ void scatter_nodes(ScatterArgs s) {
         for (int u = 0; u < kScatterIlp; ++u) {
             grp[u] = __match_any_sync(0xffffffffu, p[u].x);
             base[u] = 0;
-            if (valid[u] && lane == __ffs(grp[u]) - 1)
-                base[u] = atomicAdd(&s.fill[fill_index(p[u].x, s.fill_stride)], __popc(grp[u]));
+            if (valid[u] && lane == __ffs(grp[u]) - 1) base[u] = atomicAdd(&s.fill[p[u].x], __popc(grp[u]));
         }
 #pragma unroll
         for (int u = 0; u < kScatterIlp; ++u) {
@@ -859,11 +850,10 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     ARC_TRY(arena_get(ctx, "lc_counters", kSlots, &counters));
     ARC_TRY(arena_get(ctx, "lc_tile_counts", tiles, &tile_counts));
     ARC_TRY(arena_get(ctx, "lc_chunk_base", tiles, &chunk_base));
-    const int fill_stride = fill_stride_of(tiles);
-    ARC_TRY(arena_get(ctx, "lc_fill", 32 * fill_stride, &fill));
+    ARC_TRY(arena_get(ctx, "lc_fill", tiles, &fill));
     ARC_TRY_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * kSlots, st));
     ARC_TRY_CUDA(cudaMemsetAsync(tile_counts, 0, sizeof(int) * tiles, st));
-    ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * 32 * (size_t)fill_stride, st));
+    ARC_TRY_CUDA(cudaMemsetAsync(fill, 0, sizeof(int) * tiles, st));
 
     const float p = cp->mlp_threshold;
     LevelArgs la{};
@@ -943,7 +933,6 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     sa.tile_counts = tile_counts;
     sa.chunk_base = chunk_base;
     sa.fill = fill;
-    sa.fill_stride = fill_stride;
     sa.pool = pool;
     sa.total_chunks = counters + 4;
     sa.err = ctx->d_error;
