@@ -418,7 +418,7 @@ def main(argv=None):
     tr.add_argument("--band", type=float, default=PREACCEPT_BAND)
     tr.add_argument("--eps", type=float, default=PREACCEPT_EPS, help="analytic pre-acceptance bound")
     tr.add_argument("--threshold", type=float, default=None, help="selection threshold stored with the model")
-    tr.add_argument("--act", choices=["gelu", "relu"], default="gelu", help="hidden-layer activation")
+    tr.add_argument("--act", choices=["gelu", "relu"], default="relu", help="hidden-layer activation")
     tr.add_argument("--out", default=DEFAULT_MODEL)
     ca = sub.add_parser("calibrate", help="choose the operating point on the validation scenes")
     ca.add_argument("models", nargs="+", help="candidate model archives (band and delta differ)")
