@@ -66,6 +66,30 @@ __device__ __forceinline__ TileInfo load_tile_info(const float4* info, int tile,
     return t;
 }
 
+// The same record from the field-major copy the selection reads (info_t[k * tiles + tile] =
+// info[4 * tile + k], tile_info_transpose): a warp whose lanes hold consecutive tiles loads each
+// float4 of 32 tiles from 512 contiguous bytes instead of 32 lines 64 bytes apart.
+__device__ __forceinline__ TileInfo load_tile_info_t(const float4* info_t, int tiles, int tile, float* mean) {
+    const float4 i0 = info_t[tile], i1 = info_t[(size_t)tiles + tile], i2 = info_t[2 * (size_t)tiles + tile],
+                 i3 = info_t[3 * (size_t)tiles + tile];
+    TileInfo t;
+    t.tmin[0] = i0.x; t.tmin[1] = i0.y; t.tmin[2] = i0.z; t.kdl = i0.w;
+    t.tmax[0] = i1.x; t.tmax[1] = i1.y; t.tmax[2] = i1.z; t.tau = i1.w;
+    t.ncone = i2;
+    t.valid = __float_as_int(i3.x);
+    *mean = i3.y;
+    t.rt = i3.z;
+    t.sn = i3.w;
+    return t;
+}
+
+__global__ void tile_info_transpose(const float4* info, float4* info_t, int tiles) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tiles) return;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) info_t[(size_t)k * tiles + t] = info[4 * (size_t)t + k];
+}
+
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
 // features are coarse network inputs: fast hardware log2 / division / square root
@@ -173,7 +197,7 @@ struct LevelArgs {
     const float4* bounds;
     const float4* records;
     const float4* dirstat;
-    const float4* info;
+    const float4* info;     // tile records, field-major (load_tile_info_t)
     const float4* extra;    // NodeExtra per inner node
     BoundParams bp;
     const int2* in;         // {tile, node | depth << 26}
@@ -343,7 +367,7 @@ __global__ void __launch_bounds__(kLevelThreads) learned_level(LevelArgs a) {
             if (good && node >= a.n) {
                 const int k = node - a.n;
                 float mean;
-                const TileInfo ti = load_tile_info(a.info, tile, &mean);
+                const TileInfo ti = load_tile_info_t(a.info, a.tiles, tile, &mean);
                 const float4 b0 = a.bounds[4 * (size_t)k], b1 = a.bounds[4 * (size_t)k + 1];
                 const float4 nc = a.bounds[4 * (size_t)k + 2], wc = a.bounds[4 * (size_t)k + 3];
                 const float4* rec = a.records + 4 * (size_t)node;
@@ -862,7 +886,9 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     la.bounds = reinterpret_cast<const float4*>(bvh->view.bounds);
     la.records = reinterpret_cast<const float4*>(bvh->view.records);
     la.dirstat = reinterpret_cast<const float4*>(bvh->view.dirstat);
-    la.info = info;
+    float4* info_t;
+    ARC_TRY(arena_get(ctx, "lc_info_t", 4 * (size_t)tiles, &info_t));
+    la.info = info_t;
     la.extra = extra;
     la.bp = bound_params(gp, cp);
     la.capacity = cap;
@@ -902,7 +928,8 @@ arc_status launch_cut_select_learned(arc_context* ctx, const arc_lbvh* bvh, cons
     else
         weight_image<mlp::kActGelu><<<1, 256, 0, st>>>(mlp_params(cp->model), img);
     init_frontier<<<(tiles + 255) / 256, 256, 0, st>>>(fa, counters + 8, info, tiles, n);
-    kernels += 2;
+    tile_info_transpose<<<(tiles + 255) / 256, 256, 0, st>>>(info, info_t, tiles);
+    kernels += 3;
     int2 *cur = fa, *nxt = fb;
     // Every level up to kMaxLevels is launched without reading anything back: a launch past the
     // tree's last level finds an empty frontier and returns at once, so the selection holds no
