@@ -43,7 +43,7 @@ FLOP_PER_ROW = 2 * (16 * 64 + 64 * 64 + 64 * 64 + 64)
 # DRAM bytes (read + write) of all learned_level launches of a frame per scored row: one ncu capture
 # of the 96 level launches of a 640x360 / 262,144-AVPL frame
 # (profiles/learned_level_dram_640x360_262k.md), scaled to the frame by its scored rows
-LEARNED_LEVEL_DRAM_BYTES_PER_ROW = 33.0
+LEARNED_LEVEL_DRAM_BYTES_PER_ROW = 33.1
 
 
 CALIBRATION = os.path.join(ROOT, "antiradiancecuts_b200", "models", "cutnet_calibration.json")
