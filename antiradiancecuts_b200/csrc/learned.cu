@@ -12,10 +12,10 @@
 //     cores (mlp_tile.cuh) and their pairs are refined or accepted by the logit, in the same
 //     launch.
 // Persistent CTAs take 256 pairs at a time from a per-level work counter (the next chunk fetched
-// one ahead); pushes and accepts reserve their slots with one atomic per CTA and kind.  The host
-// checks the frontier size only every few levels.  Accepted
-// pairs are finally grouped by tile into the chunked cut pool (count, scan, scatter), which the
-// shared cut evaluation reads.
+// one ahead); pushes and accepts reserve their slots with one atomic per CTA and kind.  The walk
+// reads nothing back on the host: it launches a fixed number of levels, and a launch past the
+// deepest frontier returns at once.  Accepted pairs are finally grouped by tile into the chunked
+// cut pool (count, scan, scatter), which the shared cut evaluation reads.
 //
 // Training data (arc_cut_training_samples): for a batch of tiles, label_prefix computes, per
 // pixel, the FP64 prefix sums over the sorted leaves of the luminance of each leaf's signed
