@@ -92,6 +92,28 @@ def test_reference_arm_prints_the_contract_line():
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == "room_256_4k"
+    # what the gather got from the host, per step
+    assert len(b["per_step_values"]) == 2 and len(b["per_step_cpu_seconds_per_second"]) == 2
+    assert 0 < b["cpu_seconds_per_second"] <= b["cores"] + 1
+    assert set(b["context_switches"]) == {"involuntary", "voluntary"}
+    if b["host_cpu"] is not None:
+        assert 0 <= b["host_cpu"]["busy"] <= 1 and 0 <= b["host_cpu"]["steal"] <= 1
+
+
+def test_host_cpu_readers():
+    """The host and cgroup CPU readers the baseline records: well-formed on this machine, whatever
+    its cgroup version."""
+    import bench
+
+    h = bench.host_cpu_times()
+    if h is not None:
+        busy, steal, total = h
+        assert 0 <= busy <= total and 0 <= steal <= total
+    cg = bench.cgroup_cpu()
+    assert set(cg) == {"quota_cores", "throttled_s", "nr_throttled"}
+    assert cg["quota_cores"] is None or cg["quota_cores"] > 0
+    assert cg["throttled_s"] is None or cg["throttled_s"] >= 0
+    assert bench.host_threads() >= 1
 
 
 def test_reference_arm_loads_no_gpu_library():
