@@ -1188,10 +1188,13 @@ OR_EXPORT void oracle_eval_cut(const float* gb_pos, const float* gb_nrm, int32_t
                                int32_t num_materials, int32_t ar_kind, float cone_half_angle, float dist_clamp,
                                float disk_radius, double* out_rad, double* out_ar, double* out_res,
                                int32_t num_threads) {
+    /* thread-private copies of the call's constants, as in oracle_gather_fp32 */
+#pragma omp parallel num_threads(num_threads > 0 ? num_threads : 1)
+    {
     const int tx_n = (W + 7) / 8;
     const double cos_thr = fmax(cos((double)cone_half_angle), 0.001);
     const double c2 = (double)dist_clamp * dist_clamp;
-#pragma omp parallel for schedule(dynamic, 64) num_threads(num_threads > 0 ? num_threads : 1)
+#pragma omp for schedule(dynamic, 64)
     for (int64_t px = 0; px < (int64_t)W * H; ++px) {
         const int x = (int)(px % W), y = (int)(px / W);
         const int tile = (y / 8) * tx_n + x / 8;
@@ -1241,6 +1244,7 @@ OR_EXPORT void oracle_eval_cut(const float* gb_pos, const float* gb_nrm, int32_t
             out_ar[3 * px + k] = a[k];
             out_res[3 * px + k] = r[k] - a[k];
         }
+    }
     }
 }
 
