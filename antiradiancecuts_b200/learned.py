@@ -1,15 +1,18 @@
 """The learned cut: training data, training and loading of the cut-refinement MLP.
 
-    python -m antiradiancecuts_b200.learned train [--scenes 64] [--samples 20000000] [--out PATH]
+    python -m antiradiancecuts_b200.learned train [--act relu] [--band 64] [--delta 5e-5] [--eps 0.0015]
+                                                  [--scenes 64] [--samples 20000000] [--out PATH]
+    python -m antiradiancecuts_b200.learned calibrate ARCHIVE... [--install PATH] [--report PATH]
 
 Training data come from the exact gather itself: for each training scene (room variants with
 seeds 100..163: 0-16 random boxes, random light position and wall albedo) rendered at the
 evaluation scale (1920x1080 G-buffer, 1,048,576 AVPLs), the GPU walks the trees of the 8x8 tiles in
-a few seeded 64x64-pixel windows with the exact refine/accept decision and records the features,
+16 seeded 32x32-pixel windows with the exact refine/accept decision and records the features,
 label and error of every node the selection would score (arc_cut_training_samples).  The network
-is then trained on the GPU by the library's own tensor-core forward/backward kernels
-(arc_mlp_train_step, Adam) as a classifier of the 0/1 labels (weighted binary cross-entropy); the
-selection refines a node when the predicted probability reaches the threshold.  A regression of
+(ReLU or GELU hidden layers) is then trained on the GPU by the library's own tensor-core
+forward/backward kernels (arc_mlp_train_step, Adam) as a classifier of the 0/1 labels (weighted
+binary cross-entropy); the selection refines a node when the predicted probability reaches the
+threshold, which `calibrate` chooses on the validation scenes (seeds 164..171).  A regression of
 log2 of each node's exact relative error (squared loss; refine when the predicted error reaches
 the threshold) is the alternative objective.
 """
@@ -35,7 +38,7 @@ NUM_PARAMS = 9473
 TRAIN_SEEDS = range(100, 164)
 TRAIN_W, TRAIN_H, TRAIN_AVPLS = 1920, 1080, 1 << 20
 TRAIN_CROPS, TRAIN_CROP = 16, 32  # windows per scene and their size in pixels
-LABEL_DELTA = 1e-4  # label: refine when the node's true error exceeds this fraction of the tile value
+LABEL_DELTA = 5e-5  # label: refine when the node's true error exceeds this fraction of the tile value
 LOG2_FLOOR = -30.0  # regression targets: log2 of the relative error, at least this
 # analytic pre-acceptance shared by labelling and selection: nodes whose error bound is within
 # PREACCEPT_EPS of the tile estimate (antiradiance-uncertain nodes weighted by PREACCEPT_K) are

@@ -45,7 +45,7 @@ def scene_(ctx):
     return d, bvh, tree, api.GBuffer(d["pos"], d["nrm"])
 
 
-def _gpu_samples(ctx, bvh, gb, d, capacity=400000):
+def _gpu_samples(ctx, bvh, gb, d, capacity=2_000_000):
     import torch
 
     prm = api.gather_params(L.ARC_AR_CONE, CONE, CLAMP)
@@ -76,7 +76,8 @@ def test_training_features_and_labels_match_oracle(ctx, scene_):
     d, bvh, tree, gb = scene_
     gk, gf, gl, ge = _gpu_samples(ctx, bvh, gb, d)
     ok, of, ol, oe = O.training_samples(d["pos"], d["nrm"], tree, d["dif"], EPS, CLAMP, 2, CONE, BAND, DELTA,
-                                        ar_uncertain=K)
+                                        ar_uncertain=K, capacity=1 << 22)
+    assert len(ok) < 1 << 22
     gi, oi = _index(gk), _index(ok)
     assert len(gi) == len(gk) and len(oi) == len(ok), "a (tile, node) pair was sampled twice"
     common = sorted(set(gi) & set(oi))
